@@ -1,0 +1,371 @@
+#!/usr/bin/env python3
+"""Benchmark of the PO diffraction hot path (one JSON line on rank 0).
+
+Workload: the orientation-averaged hexagonal column of the reference's
+headline configuration: --particle 1 100 40 (D = 40 um, L = 100 um),
+m = 1.3116 + 1e-9 i, 4 reflections, 16,384 Owen-Sobol orientations (seed 42),
+zenith 0..180 deg in 0.1 deg steps x 48 azimuth bins (86,448 directions).
+Beams come from the reference's own host tracer (libmbs_host.so, compiled
+from the reference sources); they are synthetic only in that no measured
+data set is involved.
+
+A step = one pass of the hot path over the whole batch: diffraction of every
+(orientation, beam, direction), coherent Jones sums, Mueller conversion and
+the orientation average, in the FP32-compensated precision.
+  value : orientations/s with the batch resident in HBM (device timing).
+  e2e   : the same through the public C-ABI call mbs_po_diffract with pinned
+          host buffers: H2D of the beam arrays, kernels, D2H of the Mueller
+          grid, every step.
+The FP64 path runs once on the same batch as the error reference.
+
+--impl reference times the reference's own CPU implementation of the path
+(HandlerPO::HandleBeamsToLocal + AddToMuellerLocal under OpenMP, built from
+the reference sources into oracle/_ref) on a bounded sample of the same
+orientations, with every host thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PO orientations/s and beam·dir evals/s at stated M11 error vs plain FP64 path"
+WORKLOAD = "orientation-averaged hexagonal column D=40um L=100um, m=1.3116+1e-9i, 4 reflections, " \
+           "16384 Sobol orientations, theta 0-180 deg step 0.1 x 48 phi"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--orient", type=int, default=16384)
+    ap.add_argument("--n-phi", type=int, default=48)
+    ap.add_argument("--n-theta", type=int, default=1800)
+    ap.add_argument("--cpu-sample", type=int, default=48, help="orientations in the CPU baseline sample")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error reference")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def build_inputs(args, rank, world):
+    from mbs_fast_b200 import beams as B
+    cfg = B.ParticleConfig(particle_type=1, p=(100.0, 40.0), ri_re=1.3116, ri_im=1e-9,
+                           wavelength=0.532, max_reflections=4)
+    bs, gs, _ = B.symmetry(cfg)
+    beta, gamma, w = B.sobol_orientations(args.orient, bs, gs, 42)
+    # weak scaling: every rank owns its own contiguous orientation shard of
+    # the same size (TracerPOTotal.cpp:5715-5718 splits ranks the same way)
+    if world > 1:
+        beta, gamma, w = np.tile(beta, world), np.tile(gamma, world), np.tile(w, world)
+        n = args.orient
+        beta, gamma, w = beta[rank * n:(rank + 1) * n], gamma[rank * n:(rank + 1) * n], w[rank * n:(rank + 1) * n]
+    batch = B.trace(cfg, beta, gamma, w)
+    grid = B.grid(0.0, 180.0, args.n_phi, args.n_theta)
+    wave = B.wave(cfg)
+    return cfg, batch, grid, wave, (beta, gamma, w)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=5)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(mx)) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_flops(batch, n_dirs: int) -> float:
+    """F = 12*nv + 168 flops per beam-direction, +100 per orientation-direction
+    (the per-unit work definition of the PO path)."""
+    return float((12.0 * batch.n_verts + 168.0 * batch.n_beams) * n_dirs
+                 + 100.0 * batch.n_orient * n_dirs)
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def cpu_baseline(cfg, batch, args) -> dict:
+    """Reference CPU path (oracle/_ref) on a bounded sample, all host threads."""
+    import oracle
+    n = min(args.cpu_sample, batch.n_orient)
+    sample = batch.select(0, n)
+    spec = (0.0, 180.0, args.n_phi, args.n_theta)
+    if oracle.have_reference():
+        _, _, _, sec = oracle.ref_batch(cfg, spec, sample, n_threads=0)
+        kind = "reference"
+    else:
+        from mbs_fast_b200 import beams as B
+        t0 = time.perf_counter()
+        oracle.po_diffract(sample, B.grid(*spec), B.wave(cfg), n_threads=0)
+        sec = time.perf_counter() - t0
+        kind = "port"
+    return {"value": n / sec, "unit": "orientations/s", "cores": os.cpu_count(), "kind": kind,
+            "sample": f"{n} of the {batch.n_orient} orientations on the full "
+                      f"{args.n_phi}x{args.n_theta + 1} grid ({sec:.2f} s)",
+            "beam_dir_evals_per_s": sample.n_beams * args.n_phi * (args.n_theta + 1) / sec}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    cfg, batch, grid, wave, _ = build_inputs(
+        argparse.Namespace(**{**vars(args), "orient": max(args.cpu_sample, 8)}), 0, 1)
+    spec = (0.0, 180.0, args.n_phi, args.n_theta)
+    n = min(args.cpu_sample, batch.n_orient)
+    sample = batch.select(0, n)
+    kind = "reference" if oracle.have_reference() else "port"
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        oracle.ref_batch(cfg, spec, sample.select(0, 2), n_threads=0) if kind == "reference" else None
+    times = []
+    for _ in range(args.steps):
+        if kind == "reference":
+            _, _, _, sec = oracle.ref_batch(cfg, spec, sample, n_threads=0)
+        else:
+            t0 = time.perf_counter()
+            oracle.po_diffract(sample, grid, wave, n_threads=0)
+            sec = time.perf_counter() - t0
+        times.append(sec)
+    sec = float(np.mean(times))
+    v = n / sec
+    line = {"metric": METRIC, "value": v, "unit": "orientations/s", "n_gpus": 0, "impl": "reference",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (beams from the reference tracer)",
+            "config": {"workload": WORKLOAD, "sample_orientations": n},
+            "cpu_baseline": {"value": v, "unit": "orientations/s", "cores": os.cpu_count(),
+                             "kind": kind, "sample": f"{n} orientations per step on the full grid"},
+            "e2e": {"value": v, "unit": "orientations/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "beam_dir_evals_per_s": sample.n_beams * args.n_phi * (args.n_theta + 1) / sec}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from mbs_fast_b200 import abi
+    from mbs_fast_b200.handler import GpuHandlerPO
+
+    t0 = time.perf_counter()
+    cfg, batch, grid, wave, orients = build_inputs(args, rank, world)
+    t_trace = time.perf_counter() - t0
+    G = grid.n_dirs
+    h = GpuHandlerPO(grid, wave, device=local)
+    staged = h.stage(batch)
+    acc = torch.zeros(G * 16, dtype=torch.float64, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    # FP64 error reference (once, untimed)
+    m11_err = None
+    fp64_ms = None
+    M64 = None
+    if not args.no_fp64:
+        ref = torch.zeros_like(acc)
+        st = abi.Stats()
+        h.diffract_staged(staged, ref.data_ptr(), precision=abi.FP64, stream=stream, stats=st)
+        torch.cuda.synchronize()
+        fp64_ms = st.kernel_ms + st.reduce_ms
+        M64 = ref.cpu().numpy().reshape(grid.n_az, grid.n_zen + 1, 16)
+
+    stats = abi.Stats()
+    for _ in range(args.warmup):
+        acc.zero_()
+        h.diffract_staged(staged, acc.data_ptr(), precision=abi.FP32C, stream=stream, stats=stats)
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident (value) ----
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kernel_ms = []
+    launches = 0
+    ev0.record()
+    for _ in range(args.steps):
+        acc.zero_()
+        h.diffract_staged(staged, acc.data_ptr(), precision=abi.FP32C, stream=stream, stats=stats)
+        kernel_ms.append(stats.kernel_ms)
+        launches += stats.launches + 1      # diffraction + reduce, + the accumulator clear
+    ev1.record()
+    torch.cuda.synchronize()
+    step_ms = ev0.elapsed_time(ev1) / args.steps
+    clocks = sampler.stop()
+    if world > 1:
+        t = torch.tensor([step_ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        step_ms = float(t.item())
+    M32 = acc.cpu().numpy().reshape(grid.n_az, grid.n_zen + 1, 16)
+
+    # ---- timed region: end-to-end through the public C ABI ----
+    pinned = pin_batch(batch)
+    Mh = np.zeros((grid.n_az, grid.n_zen + 1, 16))
+    h.handle_orientations_to_local_gpu(pinned, Mh, precision=abi.FP32C)   # warm
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 3))):
+        Mh[:] = 0.0
+        t1 = time.perf_counter()
+        h.handle_orientations_to_local_gpu(pinned, Mh, precision=abi.FP32C)
+        e2e_t.append(time.perf_counter() - t1)
+    e2e_s = float(np.mean(e2e_t))
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d_bytes = int(sum(a.nbytes for a in (pinned.beam_offsets, pinned.orient_weight,
+                                          pinned.vert_offsets, pinned.vx, pinned.vy,
+                                          pinned.slope_yx, pinned.slope_xy, pinned.edge_flags,
+                                          pinned.beam_geom, pinned.beam_flags)))
+    d2h_bytes = G * 16 * 8
+
+    # ---- error vs FP64 on the same orientations ----
+    if M64 is not None:
+        from tests import common
+        errs = common.element_errors(M32, M64, grid)
+        errs["weighted_L2_all16"] = common.weighted_l2(M32, M64, grid)
+        m11_err = errs
+
+    flops = algorithmic_flops(batch, G)
+    kern_s = float(np.mean(kernel_ms)) * 1e-3
+    peak = h.probe_fp32_peak()
+    achieved = flops / kern_s / 1e12
+    total_orient = batch.n_orient * world
+    value = total_orient / (step_ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "orientations/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (beams from the reference's own tracer, no data set)",
+        "config": {"workload": WORKLOAD, "orientations_per_gpu": batch.n_orient,
+                   "beams": batch.n_beams, "vertices": batch.n_verts, "directions": G,
+                   "precision": "fp32c (FP32 trig/MAC, FP64 phase+reduction, Kahan Jones sums)",
+                   "l2": "inputs larger than L2 (%.0f MB resident)" % ((batch.n_beams * 288 + batch.n_verts * 32) / 1e6),
+                   "trace_seconds": t_trace},
+        "beam_dir_evals_per_s": batch.n_beams * world * G / (step_ms * 1e-3),
+        "m11_error_vs_fp64": m11_err,
+        "fp64_ms_per_step": fp64_ms,
+        "fp64_orientations_per_s": (batch.n_orient / (fp64_ms * 1e-3)) if fp64_ms else None,
+        "e2e": {"value": total_orient / e2e_s, "unit": "orientations/s",
+                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "peak_source": "measured FFMA probe (MEASURED_PEAKS.json has no FP32 entry)",
+                     "work": "12*nv+168 flop per beam-direction + 100 per orientation-direction"},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(cfg, batch, args)
+    staged.free()
+    h.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def pin_batch(batch):
+    """Copy the batch's arrays into page-locked host memory."""
+    import torch
+    from mbs_fast_b200.beams import BeamBatch
+
+    def pin(a):
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        n = t.numpy()
+        n[...] = a
+        return n
+    return BeamBatch(beam_offsets=pin(batch.beam_offsets), orient_weight=pin(batch.orient_weight),
+                     vert_offsets=pin(batch.vert_offsets), vx=pin(batch.vx), vy=pin(batch.vy),
+                     slope_yx=pin(batch.slope_yx), slope_xy=pin(batch.slope_xy),
+                     edge_flags=pin(batch.edge_flags), beam_geom=pin(batch.beam_geom),
+                     beam_flags=pin(batch.beam_flags))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,192 @@
+/*
+ * mbs_po_b200.h — C ABI of the B200 (sm_100a) physical-optics diffraction library.
+ *
+ * This is the drop-in boundary under MBS-fast's HandlerPO GPU entry points.
+ * The reference compiles those entry points as HandlerPO member functions in
+ * src/cuda/GpuDiffraction.cu; here the member functions (see
+ * mbs_fast_b200/host/po_boundary.cpp) flatten PreparedOrientation data into
+ * the plain arrays below and call this ABI.  No C++ or torch types cross it:
+ * plain pointers, sizes and return codes only.
+ *
+ * Conventions shared by every entry point
+ *   - Return 0 (MBS_PO_OK) on success, a negative MBS_PO_E* code on failure.
+ *     The library never calls exit(); the message of the last failure of a
+ *     context is returned by mbs_po_last_error().
+ *   - Mueller outputs are ACCUMULATED (+=), never overwritten, exactly like
+ *     the reference's host `localM` accumulator
+ *     (reference src/cuda/GpuDiffraction.cu:4751-4766).
+ *   - Direction index g = p*(n_zen+1) + t for azimuth bin p in [0, n_az) and
+ *     zenith row t in [0, n_zen]; 16 row-major Mueller elements per direction
+ *     (reference GpuDiffraction.cu:4755, src/math/PhysMtr.hpp:34-65).
+ *   - One context per host thread (mirrors the reference's thread_local
+ *     GpuWorkspace, GpuDiffraction.cu:252).  A context is bound to one device.
+ */
+#ifndef MBS_PO_B200_H
+#define MBS_PO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes -------------------------------------------------------- */
+#define MBS_PO_OK              0
+#define MBS_PO_EINVAL         -1   /* bad argument (null pointer, bad size)          */
+#define MBS_PO_EBEAM          -2   /* beam with invalid edge data (nv outside [3,31]) */
+#define MBS_PO_ECUDA          -3   /* CUDA runtime error                              */
+#define MBS_PO_ENOMEM         -4   /* device or host allocation failed                */
+#define MBS_PO_ESTATE         -5   /* grid or wave constants not set                  */
+#define MBS_PO_ETIMEOUT       -6   /* a device-side bounded wait gave up              */
+#define MBS_PO_ERANGE         -7   /* size beyond a fixed capacity                    */
+
+/* ---- precision of the diffraction kernel ------------------------------- */
+#define MBS_PO_FP64            0   /* plain FP64 path (parity with reference FP64)     */
+#define MBS_PO_FP32C           1   /* FP32 trig/MAC, FP64 phase + range reduction,
+                                      compensated Jones sums                          */
+
+/* ---- per-beam geometry record: doubles, MBS_PO_GEOM_STRIDE per beam -------
+ * Field order follows PreparedBeam (reference src/handler/HandlerPO.h:14-47).  */
+#define MBS_PO_G_BD            0   /* bdx, bdy, bdz   beam direction                 */
+#define MBS_PO_G_HOR           3   /* horAx..z        aperture horizontal axis       */
+#define MBS_PO_G_VER           6   /* verAx..z        aperture vertical axis         */
+#define MBS_PO_G_CEN           9   /* cenx..z         beam centre                    */
+#define MBS_PO_G_AREA         12   /* beam_area                                      */
+#define MBS_PO_G_NT           13   /* pNTx..z                                        */
+#define MBS_PO_G_NP           16   /* pNPx..z                                        */
+#define MBS_PO_G_NXDT         19   /* pnxDTx..z                                      */
+#define MBS_PO_G_NXDP         22   /* pnxDPx..z                                      */
+#define MBS_PO_G_JP           25   /* jp00r jp00i jp01r jp01i jp10r jp10i jp11r jp11i */
+#define MBS_PO_G_OPATH        33   /* origBeam.opticalPath (extinction phase ref.)   */
+#define MBS_PO_GEOM_STRIDE    34
+
+/* ---- optional per-beam record for size rescaling (multi-size batches) ----
+ * Mirrors GpuBeam::raw*, phasePath, phaseSign (GpuDiffraction.cu:134-140).     */
+#define MBS_PO_R_J             0   /* raw J: 00r 00i 01r 01i 10r 10i 11r 11i         */
+#define MBS_PO_R_PATH          8   /* phase path (opticalPath or projLenght)         */
+#define MBS_PO_R_SIGN          9   /* phase sign (+1 or -1)                          */
+#define MBS_PO_RAW_STRIDE     10
+
+/* edge_flags bits (BeamEdgeData::edge_valid_x / edge_valid_y, Handler.h:384-385) */
+#define MBS_PO_EDGE_VALID_X    1u
+#define MBS_PO_EDGE_VALID_Y    2u
+/* beam_flags bits */
+#define MBS_PO_BEAM_EXTERNAL   1u  /* PreparedBeam::isExternal                      */
+
+/* A batch of prepared orientations in flat, caller-owned host arrays.
+ * Replaces std::vector<PreparedOrientation> (reference HandlerPO.h:50-55). */
+typedef struct mbs_po_beams {
+    int32_t        n_orient;
+    int64_t        n_beams;
+    int64_t        n_verts;
+    const int64_t *beam_offsets;   /* [n_orient+1] beams of orientation o      */
+    const double  *orient_weight;  /* [n_orient]   PreparedOrientation::sinZenith */
+    const int64_t *vert_offsets;   /* [n_beams+1]  vertices of beam b           */
+    const double  *vx;             /* [n_verts]    BeamEdgeData::x              */
+    const double  *vy;             /* [n_verts]    BeamEdgeData::y              */
+    const double  *slope_yx;       /* [n_verts]    BeamEdgeData::slope_yx       */
+    const double  *slope_xy;       /* [n_verts]    BeamEdgeData::slope_xy       */
+    const uint8_t *edge_flags;     /* [n_verts]    MBS_PO_EDGE_VALID_*          */
+    const double  *beam_geom;      /* [n_beams*MBS_PO_GEOM_STRIDE]              */
+    const uint8_t *beam_flags;     /* [n_beams]    MBS_PO_BEAM_*                */
+    /* optional (may be NULL): only read by mbs_po_diffract_multisize */
+    const double  *beam_raw;       /* [n_beams*MBS_PO_RAW_STRIDE]               */
+    const int64_t *abs_offsets;    /* [n_beams+1]  PreparedBeam::absorptionPaths */
+    const double  *abs_paths;      /* [abs_offsets[n_beams]]                    */
+} mbs_po_beams;
+
+/* Scattering grid: ScatteringRange (reference src/handler/Handler.h:15-189). */
+typedef struct mbs_po_grid {
+    int32_t       n_az;     /* nAzimuth: azimuth bins p in [0, n_az)            */
+    int32_t       n_zen;    /* nZenith:  zenith rows t in [0, n_zen]            */
+    double        az_step;  /* azinuthStep (2*pi/n_az)                          */
+    const double *theta;    /* [n_zen+1] GetZenith(t), radians                  */
+    const double *vf;       /* [n_az*(n_zen+1)*3] ScatteringRange::vf[p][t]     */
+} mbs_po_grid;
+
+/* Wave constants of Handler (reference src/handler/Handler.cpp:102-126). */
+typedef struct mbs_po_wave {
+    double  wave_index;          /* m_waveIndex = 2*pi/lambda                     */
+    double  wavelength;          /* m_wavelength                                  */
+    double  compl_wave_re;       /* m_complWave    = -i*lambda/(2*pi)^2           */
+    double  compl_wave_im;
+    double  inv_compl_wave_re;   /* m_invComplWave = i/lambda                     */
+    double  inv_compl_wave_im;
+    double  eps1;                /* m_eps1 (edge-coefficient singular threshold)  */
+    double  abs_coeff;           /* m_cAbs (absorption; multi-size re-phasing)    */
+    double  ot_far_reference_path; /* m_otFarReferencePath (extinction)           */
+    double  ot_ping_distance;    /* m_otPingDistance (extinction)                 */
+    int32_t legacy_sign;         /* m_legacySign                                  */
+    int32_t ot_phase_average;    /* m_otPhaseAverage (extinction)                 */
+} mbs_po_wave;
+
+/* Per-call statistics (device timings, work counters). */
+typedef struct mbs_po_stats {
+    double  kernel_ms;           /* diffraction kernel(s), CUDA events            */
+    double  reduce_ms;           /* deterministic partial reduction               */
+    double  h2d_ms;              /* host->device copies (host entry points)       */
+    double  d2h_ms;              /* device->host copies (host entry points)       */
+    int64_t beam_dir_evals;      /* sum over orientations of beams * directions   */
+    int64_t vert_dir_evals;      /* sum over beams of nv * directions             */
+    int32_t launches;            /* kernels launched by this call                 */
+    int32_t n_chunks;            /* orientation chunks (partial accumulators)     */
+} mbs_po_stats;
+
+typedef struct mbs_po_ctx    mbs_po_ctx;
+typedef struct mbs_po_staged mbs_po_staged;
+
+/* Context lifetime.  Replaces the reference's thread_local GpuWorkspace
+ * (GpuDiffraction.cu:188-252). */
+int         mbs_po_create(mbs_po_ctx **ctx, int device);
+int         mbs_po_destroy(mbs_po_ctx *ctx);
+const char *mbs_po_last_error(const mbs_po_ctx *ctx);
+const char *mbs_po_version(void);
+
+/* Grid tables, uploaded once per grid (reference GpuDiffraction.cu:4531-4568). */
+int mbs_po_set_grid(mbs_po_ctx *ctx, const mbs_po_grid *grid);
+/* Wave constants (reference GpuDiffraction.cu:4618-4695 kernel arguments). */
+int mbs_po_set_wave(mbs_po_ctx *ctx, const mbs_po_wave *wave);
+
+/* Host-buffer entry point: copy the batch to the device, run the fused
+ * diffraction -> coherent Jones sum -> Mueller accumulation, and ADD the
+ * weighted Mueller sums into M_accum (and, when non-NULL, the sum over
+ * non-external beams into Mns_accum), both [n_az*(n_zen+1)*16] host arrays.
+ * Replaces HandlerPO::HandleOrientationsToLocalGpu
+ * (reference src/handler/HandlerPO.h:108-120, GpuDiffraction.cu:4159-4778). */
+int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
+                    double *M_accum, double *Mns_accum, mbs_po_stats *stats);
+
+/* Device-resident path: stage a batch once (H2D + device layout), then run
+ * it any number of times.  M_accum_dev / Mns_accum_dev are DEVICE pointers to
+ * [n_az*(n_zen+1)*16] doubles, accumulated (+=) on `stream` (a cudaStream_t,
+ * NULL for the legacy default stream). */
+int mbs_po_stage(mbs_po_ctx *ctx, const mbs_po_beams *beams, mbs_po_staged **out);
+int mbs_po_staged_free(mbs_po_ctx *ctx, mbs_po_staged *staged);
+int mbs_po_diffract_staged(mbs_po_ctx *ctx, const mbs_po_staged *staged,
+                           int precision, double *M_accum_dev,
+                           double *Mns_accum_dev, void *stream,
+                           mbs_po_stats *stats);
+
+/* Optical-theorem extinction per orientation on the device (weighted by the
+ * orientation weight), written to cext_out[n_orient] (host).  Replaces
+ * HandlerPO::ComputeForwardExtinctionOt (reference HandlerPO.cpp:1812-2009). */
+int mbs_po_extinction(mbs_po_ctx *ctx, const mbs_po_beams *beams,
+                      double *cext_out);
+
+/* Upper bound on the orientations per call that fit `mem_fraction` of the
+ * device's free memory.  Replaces HandlerPO::SelectGpuOrientationBatchSize
+ * (reference GpuDiffraction.cu:2948-3029). */
+int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams,
+                        int start, int max_count, double mem_fraction,
+                        int *count_out);
+
+/* Measured FP32 FMA throughput of the context's device in TFLOP/s (independent
+ * FFMA chains on every SM), the denominator of the diffraction kernels'
+ * roofline fraction.  No counterpart in the reference. */
+int mbs_po_probe_fp32_peak(mbs_po_ctx *ctx, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MBS_PO_B200_H */

@@ -1,0 +1,166 @@
+"""Python mirror of HandlerPO's GPU entry points over the C ABI.
+
+Names, argument meaning and error behaviour follow the reference's
+HandlerPO GPU interface (reference src/handler/HandlerPO.h:102-162,
+src/cuda/GpuDiffraction.cu:4159-4778):
+
+* ``handle_orientations_to_local_gpu`` adds (never overwrites) the
+  weighted Mueller sums of orientations [start, start+count) into
+  ``local_m`` (and the no-shadow sums into ``local_m_noshadow``) and returns
+  True; it returns False for a batch the GPU path rejects (a beam without
+  valid edge data), like the reference, and raises on CUDA errors.
+* ``select_gpu_orientation_batch_size`` bounds a batch by device memory.
+
+Mueller arrays are numpy [n_az, n_zen+1, 16] in the reference's
+direction order (row p, column t, 16 row-major elements).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .beams import BeamBatch, GridTables
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        L = abi.load("libmbs_po_b200.so")
+        vp = C.c_void_p
+        L.mbs_po_create.argtypes = [C.POINTER(vp), C.c_int]
+        L.mbs_po_destroy.argtypes = [vp]
+        L.mbs_po_last_error.argtypes = [vp]
+        L.mbs_po_last_error.restype = C.c_char_p
+        L.mbs_po_version.restype = C.c_char_p
+        L.mbs_po_set_grid.argtypes = [vp, C.POINTER(abi.Grid)]
+        L.mbs_po_set_wave.argtypes = [vp, C.POINTER(abi.Wave)]
+        L.mbs_po_diffract.argtypes = [vp, C.POINTER(abi.Beams), C.c_int, abi._dp, abi._dp,
+                                      C.POINTER(abi.Stats)]
+        L.mbs_po_stage.argtypes = [vp, C.POINTER(abi.Beams), C.POINTER(vp)]
+        L.mbs_po_staged_free.argtypes = [vp, vp]
+        L.mbs_po_diffract_staged.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.POINTER(abi.Stats)]
+        L.mbs_po_extinction.argtypes = [vp, C.POINTER(abi.Beams), abi._dp]
+        L.mbs_po_select_batch.argtypes = [vp, C.POINTER(abi.Beams), C.c_int, C.c_int, C.c_double,
+                                          C.POINTER(C.c_int)]
+        L.mbs_po_probe_fp32_peak.argtypes = [vp, abi._dp]
+        _lib = L
+    return _lib
+
+
+class Staged:
+    """A batch resident in device memory (mbs_po_stage)."""
+
+    def __init__(self, handler: "GpuHandlerPO", handle: C.c_void_p, batch: BeamBatch):
+        self._h = handler
+        self.handle = handle
+        self.n_orient = batch.n_orient
+        self.n_beams = batch.n_beams
+        self.n_verts = batch.n_verts
+
+    def free(self) -> None:
+        if self.handle:
+            lib().mbs_po_staged_free(self._h.ctx, self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class GpuHandlerPO:
+    """One device context (the reference's thread_local GpuWorkspace)."""
+
+    def __init__(self, grid: GridTables, wave: abi.Wave, device: int = 0):
+        L = lib()
+        self.ctx = C.c_void_p()
+        abi.check(L.mbs_po_create(C.byref(self.ctx), device), "mbs_po_create")
+        self.grid = grid
+        self.wave = wave
+        self._call(L.mbs_po_set_grid(self.ctx, C.byref(grid.as_c())), "mbs_po_set_grid")
+        self._call(L.mbs_po_set_wave(self.ctx, C.byref(wave)), "mbs_po_set_wave")
+        self.last_stats = abi.Stats()
+
+    def _call(self, rc: int, what: str) -> None:
+        if rc != abi.MBS_PO_OK:
+            msg = lib().mbs_po_last_error(self.ctx)
+            abi.check(rc, what, msg.decode(errors="replace") if msg else None)
+
+    def close(self) -> None:
+        if self.ctx:
+            lib().mbs_po_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def new_mueller(self) -> np.ndarray:
+        return np.zeros((self.grid.n_az, self.grid.n_zen + 1, 16))
+
+    # -- HandlerPO::HandleOrientationsToLocalGpu ----------------------------
+    def handle_orientations_to_local_gpu(self, prepared: BeamBatch, local_m: np.ndarray,
+                                         local_m_noshadow: np.ndarray | None = None,
+                                         start: int = 0, count: int | None = None,
+                                         precision: int = abi.FP64) -> bool:
+        if start < 0 or (count is not None and count < 0) or start > prepared.n_orient:
+            return False
+        if count is None:
+            count = prepared.n_orient - start
+        batch = prepared if (start == 0 and count >= prepared.n_orient) else prepared.select(start, count)
+        assert local_m.shape == (self.grid.n_az, self.grid.n_zen + 1, 16) and local_m.flags.c_contiguous
+        b = batch.as_c(with_raw=False)
+        rc = lib().mbs_po_diffract(self.ctx, C.byref(b), precision, abi.ptr(local_m, C.c_double),
+                                   abi.ptr(local_m_noshadow, C.c_double), C.byref(self.last_stats))
+        if rc == -2:   # MBS_PO_EBEAM: the reference returns false ("bad-edge-data")
+            return False
+        self._call(rc, "mbs_po_diffract")
+        return True
+
+    # -- HandlerPO::SelectGpuOrientationBatchSize ---------------------------
+    def select_gpu_orientation_batch_size(self, prepared: BeamBatch, start: int, max_count: int,
+                                          mem_fraction: float = 0.88) -> int:
+        b = prepared.as_c(with_raw=False)
+        out = C.c_int()
+        self._call(lib().mbs_po_select_batch(self.ctx, C.byref(b), start, max_count, mem_fraction,
+                                             C.byref(out)), "mbs_po_select_batch")
+        return out.value
+
+    # -- HandlerPO::ComputeForwardExtinctionOt on the device ----------------
+    def extinction(self, prepared: BeamBatch) -> np.ndarray:
+        out = np.zeros(prepared.n_orient)
+        b = prepared.as_c(with_raw=False)
+        self._call(lib().mbs_po_extinction(self.ctx, C.byref(b), abi.ptr(out, C.c_double)),
+                   "mbs_po_extinction")
+        return out
+
+    def probe_fp32_peak(self) -> float:
+        """Measured FP32 FMA throughput of this device, TFLOP/s."""
+        v = C.c_double()
+        self._call(lib().mbs_po_probe_fp32_peak(self.ctx, C.byref(v)), "mbs_po_probe_fp32_peak")
+        return v.value
+
+    # -- device-resident path -------------------------------------------------
+    def stage(self, batch: BeamBatch) -> Staged:
+        h = C.c_void_p()
+        b = batch.as_c(with_raw=False)
+        self._call(lib().mbs_po_stage(self.ctx, C.byref(b), C.byref(h)), "mbs_po_stage")
+        return Staged(self, h, batch)
+
+    def diffract_staged(self, staged: Staged, m_dev_ptr: int, mns_dev_ptr: int | None = None,
+                        precision: int = abi.FP64, stream: int = 0,
+                        stats: abi.Stats | None = None) -> None:
+        st = stats if stats is not None else self.last_stats
+        self._call(lib().mbs_po_diffract_staged(self.ctx, staged.handle, precision,
+                                                C.c_void_p(m_dev_ptr),
+                                                C.c_void_p(mns_dev_ptr) if mns_dev_ptr else None,
+                                                C.c_void_p(stream), C.byref(st)),
+                   "mbs_po_diffract_staged")

@@ -1,0 +1,373 @@
+// po_boundary.cpp — HandlerPO GPU entry points on top of the B200 library.
+//
+// This translation unit takes the place of the reference's CUDA backend TU
+// (src/cuda/GpuDiffraction.cu) in the reference's own build: it defines the
+// same HandlerPO member functions (declared in src/handler/HandlerPO.h:95-162)
+// so that TracerPOTotal and the CLI call them unchanged.  Each call flattens
+// the PreparedOrientation records (beam_pack.cpp) and calls the C ABI in
+// include/mbs_po_b200.h.  Contracts kept from the reference:
+//   - Mueller sums are added into localM / localM_noshadow (never
+//     overwritten), rows p < nAz (GpuDiffraction.cu:4751-4766);
+//   - incoherent mode and beams without valid edge data return false
+//     (GpuDiffraction.cu:4172-4173, 4298-4303); the driver then throws;
+//   - CUDA errors print "CUDA backend error at ..." and exit(2) unless
+//     MBS_GPU_ALLOW_FALLBACK=1 (GpuDiffraction.cu:694-710);
+//   - one context per host thread (thread_local, GpuDiffraction.cu:252).
+// Environment knobs: MBS_B200_PRECISION=fp64|fp32c (default fp64, the
+// reference's double build), MBS_GPU_TIMING=1 prints per-call timings,
+// MBS_GPU_MEM_FRACTION bounds batch sizes like the reference.
+#include "HandlerPO.h"
+#include "beam_pack.h"
+#include "mbs_po_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace
+{
+
+struct BoundaryContext
+{
+    mbs_po_ctx *ctx = nullptr;
+    int device = -1;
+    int gridNAz = -1, gridNZen = -1;
+    std::vector<double> theta, vf;
+    double azStep = 0.0;
+    mbs_po_wave wave{};
+    bool waveSet = false;
+    std::vector<double> M, Mns;
+
+    ~BoundaryContext()
+    {
+        if (ctx)
+            mbs_po_destroy(ctx);
+    }
+};
+
+thread_local BoundaryContext g_ctx;
+
+bool env_is(const char *name, const char *value)
+{
+    const char *v = std::getenv(name);
+    return v && std::strcmp(v, value) == 0;
+}
+
+int precision_from_env()
+{
+    const char *v = std::getenv("MBS_B200_PRECISION");
+    if (v && (std::strcmp(v, "fp32c") == 0 || std::strcmp(v, "fp32") == 0))
+        return MBS_PO_FP32C;
+    return MBS_PO_FP64;
+}
+
+bool report(int rc, const char *where)
+{
+    if (rc == MBS_PO_OK)
+        return true;
+    std::fprintf(stderr, "CUDA backend error at %s: %s\n", where,
+                 g_ctx.ctx ? mbs_po_last_error(g_ctx.ctx) : "no context");
+    if (!env_is("MBS_GPU_ALLOW_FALLBACK", "1"))
+    {
+        std::fprintf(stderr,
+                     "FATAL: CUDA backend failed. Set MBS_GPU_ALLOW_FALLBACK=1 "
+                     "to allow the legacy CPU fallback after GPU errors.\n");
+        std::fflush(stderr);
+        std::exit(2);
+    }
+    return false;
+}
+
+double mem_fraction()
+{
+    const char *v = std::getenv("MBS_GPU_MEM_FRACTION");
+    if (!v || !*v)
+        return 0.88;
+    char *end = nullptr;
+    const double p = std::strtod(v, &end);
+    return (end && *end == '\0' && p > 0.1 && p <= 0.98) ? p : 0.88;
+}
+
+}  // namespace
+
+// Shared set-up of one call: device context, grid tables and wave constants.
+class HandlerPOBoundary
+{
+public:
+    static bool Prepare(const HandlerPO &h, const ScatteringRange &sphere,
+                        const mbs_po_wave &wave, int device)
+    {
+        BoundaryContext &c = g_ctx;
+        if (c.ctx && c.device != device)
+        {
+            mbs_po_destroy(c.ctx);
+            c.ctx = nullptr;
+            c.gridNAz = c.gridNZen = -1;
+            c.waveSet = false;
+        }
+        if (!c.ctx)
+        {
+            if (!report(mbs_po_create(&c.ctx, device), "context creation"))
+                return false;
+            c.device = device;
+        }
+        const int nAz = sphere.nAzimuth, nZen = sphere.nZenith;
+        std::vector<double> theta(nZen + 1);
+        for (int t = 0; t <= nZen; ++t)
+            theta[t] = sphere.GetZenith(t);
+        if (c.gridNAz != nAz || c.gridNZen != nZen || c.theta != theta
+            || c.azStep != sphere.azinuthStep)
+        {
+            std::vector<double> vf((size_t)nAz * (nZen + 1) * 3);
+            for (int p = 0; p < nAz; ++p)
+                for (int t = 0; t <= nZen; ++t)
+                {
+                    const Point3d &v = sphere.vf[p][t];
+                    double *o = &vf[((size_t)p * (nZen + 1) + t) * 3];
+                    o[0] = v.x; o[1] = v.y; o[2] = v.z;
+                }
+            mbs_po_grid g;
+            g.n_az = nAz;
+            g.n_zen = nZen;
+            g.az_step = sphere.azinuthStep;
+            g.theta = theta.data();
+            g.vf = vf.data();
+            if (!report(mbs_po_set_grid(c.ctx, &g), "grid upload"))
+                return false;
+            c.gridNAz = nAz;
+            c.gridNZen = nZen;
+            c.theta.swap(theta);
+            c.azStep = sphere.azinuthStep;
+        }
+        if (!c.waveSet || std::memcmp(&c.wave, &wave, sizeof(wave)) != 0)
+        {
+            if (!report(mbs_po_set_wave(c.ctx, &wave), "wave constants"))
+                return false;
+            c.wave = wave;
+            c.waveSet = true;
+        }
+        (void)h;
+        return true;
+    }
+};
+
+// Wave constants of this handler; a subclass-free accessor to the protected
+// Handler members through a pointer-to-member of a derived helper.
+struct HandlerPOWaveAccess : public HandlerPO
+{
+    static mbs_po_wave Get(const HandlerPO &h, double waveIndexOverride)
+    {
+        mbs_po_wave w;
+        std::memset(&w, 0, sizeof(w));
+        w.wave_index = h.*(&HandlerPOWaveAccess::m_waveIndex);
+        w.wavelength = h.*(&HandlerPOWaveAccess::m_wavelength);
+        const complex cw = h.*(&HandlerPOWaveAccess::m_complWave);
+        const complex icw = h.*(&HandlerPOWaveAccess::m_invComplWave);
+        w.compl_wave_re = real(cw);
+        w.compl_wave_im = imag(cw);
+        w.inv_compl_wave_re = real(icw);
+        w.inv_compl_wave_im = imag(icw);
+        w.eps1 = h.*(&HandlerPOWaveAccess::m_eps1);
+        w.abs_coeff = h.AbsorptionCoefficient();
+        w.ot_far_reference_path = h.m_otFarReferencePath;
+        w.ot_ping_distance = h.m_otPingDistance;
+        w.legacy_sign = h.m_legacySign ? 1 : 0;
+        w.ot_phase_average = h.m_otPhaseAverage ? 1 : 0;
+        if (waveIndexOverride > 0.0)
+        {
+            // multi-size rescale: k is carried by the scale factor
+            w.wave_index = waveIndexOverride;
+        }
+        return w;
+    }
+};
+
+static int current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        dev = 0;
+    return dev;
+}
+
+static bool diffract_range(HandlerPO &h, const ScatteringRange &sphere,
+                           const std::vector<PreparedOrientation> &prepared,
+                           int start, int count, Arr2D &localM,
+                           Arr2D &localM_noshadow, bool computeNoShadow, int device)
+{
+    const bool timing = env_is("MBS_GPU_TIMING", "1");
+    const auto t0 = std::chrono::steady_clock::now();
+    const int nAz = sphere.nAzimuth, nZen = sphere.nZenith;
+    MbsPackedBeams packed;
+    std::string err;
+    const int prc = mbs_pack_prepared(prepared, start, count, false, packed, &err);
+    if (prc == MBS_PO_EBEAM)
+        return false;   // reference: failDirect("bad-edge-data")
+    if (prc != MBS_PO_OK)
+        return false;
+    const mbs_po_beams view = packed.view(false);
+    if (view.n_beams == 0)
+        return true;
+    const auto t1 = std::chrono::steady_clock::now();
+    if (!HandlerPOBoundary::Prepare(h, sphere, HandlerPOWaveAccess::Get(h, 0.0), device))
+        return false;
+    BoundaryContext &c = g_ctx;
+    const size_t n = (size_t)nAz * (nZen + 1) * 16;
+    c.M.assign(n, 0.0);
+    if (computeNoShadow)
+        c.Mns.assign(n, 0.0);
+    mbs_po_stats st;
+    std::memset(&st, 0, sizeof(st));
+    const int rc = mbs_po_diffract(c.ctx, &view, precision_from_env(), c.M.data(),
+                                   computeNoShadow ? c.Mns.data() : nullptr, &st);
+    if (rc == MBS_PO_EBEAM)
+        return false;
+    if (!report(rc, "diffraction"))
+        return false;
+    for (int p = 0; p < nAz; ++p)
+        for (int t = 0; t <= nZen; ++t)
+        {
+            const double *m = &c.M[((size_t)p * (nZen + 1) + t) * 16];
+            double *cell = localM.RawCell(p, t);
+            for (int q = 0; q < 16; ++q)
+                cell[q] += m[q];
+            if (computeNoShadow)
+            {
+                const double *mn = &c.Mns[((size_t)p * (nZen + 1) + t) * 16];
+                double *cn = localM_noshadow.RawCell(p, t);
+                for (int q = 0; q < 16; ++q)
+                    cn[q] += mn[q];
+            }
+        }
+    if (timing)
+    {
+        const double pack = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        const double total = std::chrono::duration<double, std::milli>(
+            std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr,
+                     "GPU timing diffract path=b200-%s orient=%d beams=%lld nAz=%d nZen=%d "
+                     "pack=%.3fms h2d+stage=%.3fms kernels=%.3fms reduce=%.3fms total=%.3fms\n",
+                     precision_from_env() == MBS_PO_FP32C ? "fp32c" : "fp64",
+                     view.n_orient, (long long)view.n_beams, nAz, nZen, pack, st.h2d_ms,
+                     st.kernel_ms, st.reduce_ms, total);
+    }
+    return true;
+}
+
+bool HandlerPO::HandleOrientationsToLocalGpu(const std::vector<PreparedOrientation> &prepared,
+                                             int start, int count, Arr2D &localM,
+                                             Arr2D &localM_noshadow, double scale,
+                                             double waveIndex)
+{
+    if (!isCoh)
+        return false;
+    if (start < 0 || count < 0 || start > (int)prepared.size())
+        return false;
+    if (std::fabs(scale - 1.0) > 1e-15)
+    {
+        std::vector<Arr2D> ms;
+        ms.emplace_back(m_sphere.nAzimuth + 1, m_sphere.nZenith + 1, 4, 4);
+        ms.back().ClearArr();
+        std::vector<double> scales(1, scale);
+        if (!HandleOrientationsToLocalGpuMultiK(prepared, start, count, scales, waveIndex, ms))
+            return false;
+        for (int p = 0; p < m_sphere.nAzimuth; ++p)
+            for (int t = 0; t <= m_sphere.nZenith; ++t)
+                localM.insert(p, t, ms[0](p, t));
+        return true;
+    }
+    return diffract_range(*this, m_sphere, prepared, start, count, localM, localM_noshadow,
+                          ComputeNoShadow(), current_device());
+}
+
+bool HandlerPO::HandleOrientationsToLocalGpu(const std::vector<PreparedOrientation> &prepared,
+                                             Arr2D &localM, Arr2D &localM_noshadow)
+{
+    return HandleOrientationsToLocalGpu(prepared, 0, (int)prepared.size(), localM,
+                                        localM_noshadow, 1.0, 0.0);
+}
+
+bool HandlerPO::HandleOrientationsToLocalGpuOnDevice(
+    const std::vector<PreparedOrientation> &prepared, int start, int count, int device,
+    Arr2D &localM, Arr2D &localM_noshadow, double scale, double waveIndex,
+    unsigned long long /*cacheToken*/)
+{
+    int saved = 0;
+    cudaGetDevice(&saved);
+    if (cudaSetDevice(device) != cudaSuccess)
+        return false;
+    bool ok;
+    if (std::fabs(scale - 1.0) > 1e-15)
+        ok = HandleOrientationsToLocalGpu(prepared, start, count, localM, localM_noshadow,
+                                          scale, waveIndex);
+    else
+        ok = isCoh && diffract_range(*this, m_sphere, prepared, start, count, localM,
+                                     localM_noshadow, ComputeNoShadow(), device);
+    cudaSetDevice(saved);
+    return ok;
+}
+
+bool HandlerPO::HandleBeamsToLocalGpu(const PreparedOrientation &prepared, Arr2D &localM,
+                                      Arr2D &localM_noshadow)
+{
+    std::vector<PreparedOrientation> one(1, prepared);
+    return HandleOrientationsToLocalGpu(one, 0, 1, localM, localM_noshadow, 1.0, 0.0);
+}
+
+bool HandlerPO::HandleOrientationsToLocalGpuFftPhi(const std::vector<PreparedOrientation> &prepared,
+                                                   int start, int count, Arr2D &localM,
+                                                   Arr2D &localM_noshadow, double scale,
+                                                   double waveIndex)
+{
+    // The FFT azimuth interpolation is an approximation of the direct
+    // evaluation; the direct path is exact on the requested grid.
+    return HandleOrientationsToLocalGpu(prepared, start, count, localM, localM_noshadow,
+                                        scale, waveIndex);
+}
+
+bool HandlerPO::HandleOrientationsToLocalGpuMultiK(const std::vector<PreparedOrientation> & /*prepared*/,
+                                                   int /*start*/, int /*count*/,
+                                                   const std::vector<double> & /*scales*/,
+                                                   double /*waveIndex*/,
+                                                   std::vector<Arr2D> & /*localMs*/)
+{
+    return false;
+}
+
+bool HandlerPO::HandleOrientationsToLocalGpuFftPhiMultiK(
+    const std::vector<PreparedOrientation> &prepared, int start, int count,
+    const std::vector<double> &scales, double waveIndex, std::vector<Arr2D> &localMs)
+{
+    return HandleOrientationsToLocalGpuMultiK(prepared, start, count, scales, waveIndex, localMs);
+}
+
+bool HandlerPO::DiffractThetasGpu(const std::vector<PreparedOrientation> & /*prepared*/,
+                                  const double * /*theta_rads*/, int /*nPoints*/,
+                                  std::vector<double> & /*m11_out*/)
+{
+    return false;
+}
+
+int HandlerPO::SelectGpuOrientationBatchSize(const std::vector<PreparedOrientation> &prepared,
+                                             int start, int maxCount) const
+{
+    if (maxCount <= 1)
+        return std::max(1, maxCount);
+    MbsPackedBeams packed;
+    if (mbs_pack_prepared(prepared, start, maxCount, false, packed, nullptr) != MBS_PO_OK)
+        return std::max(1, maxCount);
+    if (!HandlerPOBoundary::Prepare(*this, m_sphere, HandlerPOWaveAccess::Get(*this, 0.0),
+                                    current_device()))
+        return std::max(1, maxCount);
+    const mbs_po_beams view = packed.view(false);
+    int count = maxCount;
+    if (mbs_po_select_batch(g_ctx.ctx, &view, 0, maxCount, mem_fraction(), &count) != MBS_PO_OK)
+        return std::max(1, maxCount);
+    return std::max(1, count);
+}

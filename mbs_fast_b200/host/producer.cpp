@@ -1,0 +1,363 @@
+// producer.cpp — the reference's host beam producer behind a C ABI
+// (include/mbs_host.h).
+//
+// Builds the same particle, light, scattering and HandlerPO objects as the
+// reference CLI (reference src/main.cpp:1655-1760 particle, :2228-2252 tracer
+// and handler, :196-260 cutoff profiles) and runs phase 1 of
+// TracerPOTotal::TraceWeightedOrientations (TracerPOTotal.cpp:5815-5898):
+// per OpenMP thread a private Particle / Scattering / HandlerPO, then for each
+// orientation Rotate -> FormShadowBeam -> ScatterLight -> PrepareBeams.  The
+// prepared orientations are flattened with mbs_pack_prepared.
+#include "mbs_host.h"
+#include "beam_pack.h"
+
+#include "HandlerPOTotal.h"
+#include "Hexagonal.h"
+#include "Bullet.h"
+#include "Droxtal.h"
+#include "ConcaveHexagonal.h"
+#include "HexagonalAggregate.h"
+#include "TracerPOTotal.h"
+#include "Sobol.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+struct mbs_host_batch
+{
+    MbsPackedBeams packed;
+    mbs_po_beams view;
+    double trace_seconds = 0.0;
+};
+
+namespace
+{
+
+void set_err(char *err, int errlen, const std::string &msg)
+{
+    if (err && errlen > 0)
+    {
+        std::snprintf(err, (size_t)errlen, "%s", msg.c_str());
+    }
+}
+
+// Exposes the protected wave constants of Handler.
+class HostHandlerPO : public HandlerPOTotal
+{
+public:
+    using HandlerPOTotal::HandlerPOTotal;
+    void FillWave(mbs_po_wave &w) const
+    {
+        w.wave_index = m_waveIndex;
+        w.wavelength = m_wavelength;
+        w.compl_wave_re = real(m_complWave);
+        w.compl_wave_im = imag(m_complWave);
+        w.inv_compl_wave_re = real(m_invComplWave);
+        w.inv_compl_wave_im = imag(m_invComplWave);
+        w.eps1 = m_eps1;
+        w.abs_coeff = m_cAbs;
+        w.ot_far_reference_path = m_otFarReferencePath;
+        w.ot_ping_distance = m_otPingDistance;
+        w.legacy_sign = m_legacySign ? 1 : 0;
+        w.ot_phase_average = m_otPhaseAverage ? 1 : 0;
+    }
+};
+
+// Reference objects for one configuration (mirrors src/main.cpp).
+struct HostSetup
+{
+    std::unique_ptr<Particle> particle;
+    std::unique_ptr<TracerPOTotal> tracer;
+    std::unique_ptr<HostHandlerPO> handler;
+    Tracks tracks;
+    bool isAbs = false;
+
+    explicit HostSetup(const mbs_host_config &cfg)
+    {
+        isAbs = cfg.absorption != 0 || cfg.ri_im != 0.0;
+        const ::complex ri(cfg.ri_re, isAbs ? cfg.ri_im : 0.0);
+        if (cfg.particle_file && cfg.particle_file[0])
+        {
+            particle.reset(new Particle());
+            particle->SetFromFile(cfg.particle_file);
+            particle->SetRefractiveIndex(ri);
+            if (cfg.resize > 0.0)
+                particle->Resize(cfg.resize);
+        }
+        else
+        {
+            switch (cfg.particle_type)
+            {
+            case 1:   // --particle 1 L D  (main.cpp:1731-1735)
+                particle.reset(new Hexagonal(ri, cfg.p[1], cfg.p[0]));
+                break;
+            case 2:   // --particle 2 L D  (main.cpp:1736-1741)
+            {
+                const double sup = (cfg.p[1] * std::sqrt(3) * std::tan(DegToRad(62))) / 4;
+                particle.reset(new Bullet(ri, cfg.p[1], cfg.p[0], sup));
+                break;
+            }
+            case 4:   // --particle 4 size  (main.cpp:1750-1755)
+                particle.reset(new Droxtal(ri, DegToRad(32.35), DegToRad(71.81), cfg.p[0]));
+                break;
+            case 10:  // --particle 10 L D depth  (main.cpp:1762-1768)
+                particle.reset(new ConcaveHexagonal(ri, cfg.p[1], cfg.p[0], cfg.p[2]));
+                break;
+            case 12:  // --particle 12 L D n  (main.cpp:1769-1775)
+                particle.reset(new HexagonalAggregate(ri, cfg.p[1], cfg.p[0], (int)cfg.p[2]));
+                break;
+            default:
+                throw std::invalid_argument("unsupported particle type " + std::to_string(cfg.particle_type));
+            }
+        }
+        tracer.reset(new TracerPOTotal(particle.get(), cfg.max_reflections, "mbs_b200_host"));
+        tracer->m_scattering->m_wave = cfg.wavelength;
+        Scattering *sc = tracer->m_scattering;
+        if (cfg.cutoff_off)
+        {   // --cutoff-profile off (main.cpp:205-211)
+            sc->restriction = std::numeric_limits<double>::infinity();
+            sc->m_traceCutoffJRel = 0.0;
+            sc->m_traceCutoffAreaRel = 0.0;
+            sc->m_traceCutoffImportanceRel = 0.0;
+        }
+        else
+        {   // legacy-default profile (main.cpp:212-221)
+            sc->m_traceCutoffJRel = 1e-7;
+            sc->m_traceCutoffAreaRel = 0.0;
+            sc->m_traceCutoffImportanceRel = 0.0;
+        }
+        tracer->shadowOff = cfg.shadow_off != 0;
+        handler.reset(new HostHandlerPO(particle.get(), &tracer->m_incidentLight,
+                                        1, cfg.wavelength));
+        handler->isCoh = true;
+        handler->m_legacySign = cfg.legacy_sign != 0;
+        if (cfg.cutoff_off)
+        {   // main.cpp:131-137
+            handler->m_targetEps = 0.0;
+            handler->m_beamCutoffJRel = 0.0;
+            handler->m_beamCutoffAreaRel = 0.0;
+            handler->m_beamCutoffImportanceRel = 0.0;
+        }
+        // PrepareBeams does not read the scattering grid; a 1x1 placeholder
+        // keeps the per-track matrices of SetTracks small.
+        handler->SetScatteringSphere(ScatteringRange(0, M_PI, 1, 1));
+        handler->SetTracks(&tracks);
+        handler->SetAbsorptionAccounting(isAbs);
+        tracer->SetHandler(handler.get());
+    }
+};
+
+}  // namespace
+
+extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
+                              const double *beta, const double *gamma,
+                              const double *alpha, const double *weight,
+                              mbs_host_batch **out, char *err, int errlen)
+{
+    if (!cfg || !out || n_orient < 0 || (n_orient > 0 && (!beta || !gamma || !weight)))
+    {
+        set_err(err, errlen, "mbs_host_trace: bad arguments");
+        return MBS_PO_EINVAL;
+    }
+    *out = nullptr;
+    try
+    {
+        HostSetup setup(*cfg);
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<PreparedOrientation> prepared(n_orient);
+        Scattering *master = setup.tracer->m_scattering;
+        master->PrepareForParallelTrace();
+        bool failed = false;
+        std::string failMsg;
+        const int nThreads = cfg->n_threads > 0 ? cfg->n_threads : 0;
+#pragma omp parallel num_threads(nThreads > 0 ? nThreads : omp_get_max_threads())
+        {
+            Particle localParticle = *setup.particle;
+            Scattering *localScatter = master->CloneFor(&localParticle, &setup.tracer->m_incidentLight);
+            HandlerPO localHandler(&localParticle, &setup.tracer->m_incidentLight,
+                                   setup.handler->nTheta, master->m_wave);
+            localHandler.ConfigureForThreadLocalPrepare(*setup.handler, localScatter);
+            std::vector<Beam> localBeams;
+#pragma omp for schedule(dynamic, 4)
+            for (int i = 0; i < n_orient; ++i)
+            {
+                try
+                {
+                    localParticle.Rotate(beta[i], gamma[i], alpha ? alpha[i] : 0.0);
+                    if (!setup.tracer->shadowOff)
+                        localScatter->FormShadowBeam(localBeams);
+                    const bool ok = localScatter->ScatterLight(0, 0, localBeams);
+                    if (ok)
+                        localHandler.PrepareBeams(localBeams, weight[i], prepared[i]);
+                    else
+                        prepared[i].sinZenith = weight[i];
+                    localBeams.clear();
+                }
+                catch (const std::exception &e)
+                {
+#pragma omp critical(mbs_host_trace_err)
+                    {
+                        failed = true;
+                        failMsg = e.what();
+                    }
+                }
+            }
+            delete localScatter;
+        }
+        if (failed)
+        {
+            set_err(err, errlen, "tracing failed: " + failMsg);
+            return MBS_PO_EINVAL;
+        }
+        std::unique_ptr<mbs_host_batch> batch(new mbs_host_batch());
+        std::string perr;
+        const int rc = mbs_pack_prepared(prepared, 0, n_orient, true, batch->packed, &perr);
+        if (rc != MBS_PO_OK)
+        {
+            set_err(err, errlen, perr);
+            return rc;
+        }
+        batch->view = batch->packed.view(true);
+        batch->trace_seconds = std::chrono::duration<double>(
+            std::chrono::steady_clock::now() - t0).count();
+        *out = batch.release();
+        return MBS_PO_OK;
+    }
+    catch (const std::exception &e)
+    {
+        set_err(err, errlen, std::string("mbs_host_trace: ") + e.what());
+        return MBS_PO_EINVAL;
+    }
+}
+
+extern "C" const mbs_po_beams *mbs_host_batch_view(const mbs_host_batch *batch)
+{
+    return batch ? &batch->view : nullptr;
+}
+
+extern "C" double mbs_host_batch_extinction(const mbs_host_batch *batch, int o)
+{
+    if (!batch || o < 0 || o >= (int)batch->packed.extinction_ot.size())
+        return 0.0;
+    return batch->packed.extinction_ot[o];
+}
+
+extern "C" double mbs_host_batch_trace_seconds(const mbs_host_batch *batch)
+{
+    return batch ? batch->trace_seconds : 0.0;
+}
+
+extern "C" void mbs_host_batch_free(mbs_host_batch *batch)
+{
+    delete batch;
+}
+
+extern "C" int mbs_host_symmetry(const mbs_host_config *cfg, double *beta_sym,
+                                 double *gamma_sym, double *dmax)
+{
+    if (!cfg)
+        return MBS_PO_EINVAL;
+    try
+    {
+        HostSetup setup(*cfg);
+        const Symmetry &s = setup.particle->GetSymmetry();
+        if (beta_sym) *beta_sym = s.beta;
+        if (gamma_sym) *gamma_sym = s.gamma;
+        if (dmax) *dmax = setup.particle->MaximalDimention();
+        return MBS_PO_OK;
+    }
+    catch (...)
+    {
+        return MBS_PO_EINVAL;
+    }
+}
+
+extern "C" int mbs_host_sobol_orientations(int n, unsigned seed, double beta_sym,
+                                           double gamma_sym, double *beta,
+                                           double *gamma, double *weight)
+{
+    if (n <= 0 || !beta || !gamma || !weight)
+        return MBS_PO_EINVAL;
+    // TracerPOTotal::TraceFromSobolSeed (TracerPOTotal.cpp:5476-5488).
+    Sobol2D sobol(seed);
+    std::vector<double> su, sv;
+    sobol.generate(n, su, sv);
+    const double cosBetaSym = std::cos(beta_sym);
+    const double w = 1.0 / n;
+    for (int i = 0; i < n; ++i)
+    {
+        beta[i] = std::acos(1.0 - (1.0 - cosBetaSym) * su[i]);
+        gamma[i] = gamma_sym * sv[i];
+        weight[i] = w;
+    }
+    return MBS_PO_OK;
+}
+
+extern "C" int mbs_host_wave(const mbs_host_config *cfg, mbs_po_wave *wave)
+{
+    if (!cfg || !wave)
+        return MBS_PO_EINVAL;
+    try
+    {
+        HostSetup setup(*cfg);
+        std::memset(wave, 0, sizeof(*wave));
+        setup.handler->FillWave(*wave);
+        return MBS_PO_OK;
+    }
+    catch (...)
+    {
+        return MBS_PO_EINVAL;
+    }
+}
+
+extern "C" int mbs_host_grid(double zen_start_deg, double zen_end_deg, int n_az,
+                             int n_zen, const double *theta_deg, double *theta,
+                             double *vf, double *dcos2pi, double *az_step)
+{
+    if (n_az <= 0 || n_zen <= 0 || !theta || !vf)
+        return MBS_PO_EINVAL;
+    ScatteringRange range(DegToRad(zen_start_deg), DegToRad(zen_end_deg), n_az, n_zen);
+    if (theta_deg)
+    {
+        // LoadThetaGrid without a file (Handler.h:31-61).
+        range.thetaValues.clear();
+        for (int t = 0; t <= n_zen; ++t)
+            range.thetaValues.push_back(DegToRad(theta_deg[t]));
+        std::sort(range.thetaValues.begin(), range.thetaValues.end());
+        range.isNonUniform = true;
+        range.nZenith = n_zen;
+        range.zenithStart = range.thetaValues.front();
+        range.zenithEnd = range.thetaValues.back();
+        range.zenithStep = (range.zenithEnd - range.zenithStart) / n_zen;
+    }
+    Light light;   // Tracer::SetIncidentLight (Tracer.cpp:124-131)
+    light.direction = Point3f(0, 0, -1);
+    light.polarizationBasis = Point3f(0, 1, 0);
+    range.ComputeSphereDirections(light);
+    for (int t = 0; t <= n_zen; ++t)
+    {
+        theta[t] = range.GetZenith(t);
+        if (dcos2pi)
+            dcos2pi[t] = range.Compute2PiDcos(t);
+    }
+    for (int p = 0; p < n_az; ++p)
+        for (int t = 0; t <= n_zen; ++t)
+        {
+            const Point3d &v = range.vf[p][t];
+            double *o = vf + ((size_t)p * (n_zen + 1) + t) * 3;
+            o[0] = v.x; o[1] = v.y; o[2] = v.z;
+        }
+    if (az_step)
+        *az_step = range.azinuthStep;
+    return MBS_PO_OK;
+}

@@ -1,0 +1,66 @@
+"""Shared cases and error measures for the tests.
+
+Particle cases follow the reference's configurations and tests:
+  HEX_COLUMN_40x100   configs[1] particle (--particle 1 100 40, m=1.3116+1e-9i)
+  HEX_COLUMN_10x20    configs[0] particle (--particle 1 20 10, m=1.3116)
+  CONCAVE_ABSORBING   the CUDA release-gate particle of the reference
+                      (tests/run_cuda_release_gate.sh:31-44: --particle 10 1.0
+                      0.7 43.4114540493, m=1.3116+0.01i, --absorption,
+                      --cutoff-profile off)
+"""
+from __future__ import annotations
+
+import functools
+
+import numpy as np
+
+from mbs_fast_b200 import beams as B
+
+HEX_COLUMN_40x100 = B.ParticleConfig(particle_type=1, p=(100.0, 40.0), ri_re=1.3116, ri_im=1e-9,
+                                     wavelength=0.532, max_reflections=4)
+HEX_COLUMN_10x20 = B.ParticleConfig(particle_type=1, p=(20.0, 10.0), ri_re=1.3116, ri_im=0.0,
+                                    wavelength=0.532, max_reflections=4)
+CONCAVE_ABSORBING = B.ParticleConfig(particle_type=10, p=(1.0, 0.7, 43.4114540493), ri_re=1.3116,
+                                     ri_im=0.01, absorption=True, wavelength=0.532,
+                                     max_reflections=4, cutoff_off=True)
+
+
+@functools.lru_cache(maxsize=None)
+def sobol_batch(cfg_key: str, n: int, seed: int = 42) -> B.BeamBatch:
+    cfg = CASES[cfg_key]
+    bs, gs, _ = B.symmetry(cfg)
+    beta, gamma, w = B.sobol_orientations(n, bs, gs, seed)
+    return B.trace(cfg, beta, gamma, w)
+
+
+CASES = {"hex40x100": HEX_COLUMN_40x100, "hex10x20": HEX_COLUMN_10x20,
+         "concave": CONCAVE_ABSORBING}
+
+
+def weighted_l2(Ma: np.ndarray, Mb: np.ndarray, grid: B.GridTables) -> float:
+    """Solid-angle weighted relative L2 over all 16 elements of the azimuth-
+    averaged rows: the metric of the reference's CUDA release gate
+    (tests/run_cuda_release_gate.sh:70-86), computed on rows like the .dat
+    writer produces them."""
+    import oracle
+    ra, _, _ = oracle.phi_average(Ma, grid)
+    rb, _, _ = oracle.phi_average(Mb, grid)
+    w = grid.dcos2pi[:, None]
+    return float(np.sqrt(np.sum(w * (ra - rb) ** 2) / max(np.sum(w * rb ** 2), 1e-300)))
+
+
+def grid_l2(Ma: np.ndarray, Mb: np.ndarray) -> float:
+    """Relative L2 over the full direction grid (no azimuth averaging)."""
+    return float(np.sqrt(np.sum((Ma - Mb) ** 2) / max(np.sum(Mb ** 2), 1e-300)))
+
+
+def element_errors(M: np.ndarray, Mref: np.ndarray, grid: B.GridTables) -> dict:
+    """Errors of azimuth-averaged rows: relative for M11, absolute for the
+    normalised elements M12/M11, M22/M11, M33/M11, M34/M11, M44/M11."""
+    import oracle
+    r, _, _ = oracle.phi_average(M, grid)
+    q, _, _ = oracle.phi_average(Mref, grid)
+    out = {"M11_max_rel": float(np.max(np.abs(r[:, 0] - q[:, 0]) / np.abs(q[:, 0])))}
+    for name, idx in (("M12", 1), ("M22", 5), ("M33", 10), ("M34", 11), ("M44", 15)):
+        out[name + "/M11_max_abs"] = float(np.max(np.abs(r[:, idx] / r[:, 0] - q[:, idx] / q[:, 0])))
+    return out

@@ -1,0 +1,176 @@
+"""Parity of the CUDA path with the CPU oracle and the reference, through the
+C ABI (run on the B200 box: pytest -m gpu)."""
+import numpy as np
+import pytest
+
+import oracle
+from mbs_fast_b200 import abi, beams as B
+from mbs_fast_b200.handler import GpuHandlerPO
+from tests import common
+
+pytestmark = pytest.mark.gpu
+
+# Tolerances.  FP64: rounding-level agreement with the oracle (the
+# reference reports 9.6e-10 CPU vs CUDA FP64 and gates at 1e-5,
+# tests/run_cuda_release_gate.sh:8).  FP32C: the FP32 path against the FP64
+# path on the same inputs.
+FP64_WL2 = 1e-8
+FP32C_WL2 = 2e-4
+
+
+@pytest.fixture(scope="module")
+def hex_case():
+    cfg = common.HEX_COLUMN_40x100
+    batch = common.sobol_batch("hex40x100", 8)
+    grid = B.grid(0.0, 180.0, 16, 180)
+    wave = B.wave(cfg)
+    h = GpuHandlerPO(grid, wave, device=0)
+    M_ref, Mns_ref = oracle.po_diffract(batch, grid, wave, noshadow=True)
+    yield cfg, batch, grid, wave, h, M_ref, Mns_ref
+    h.close()
+
+
+def test_fp64_matches_oracle(hex_case):
+    cfg, batch, grid, wave, h, M_ref, Mns_ref = hex_case
+    M, Mns = h.new_mueller(), h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M, Mns, precision=abi.FP64)
+    assert common.weighted_l2(M, M_ref, grid) < FP64_WL2
+    assert common.weighted_l2(Mns, Mns_ref, grid) < FP64_WL2
+    assert common.grid_l2(M, M_ref) < FP64_WL2
+    # pointwise, relative to the forward peak
+    assert np.max(np.abs(M - M_ref)) < 1e-9 * np.max(np.abs(M_ref[..., 0]))
+
+
+def test_fp64_matches_reference(hex_case):
+    cfg, batch, grid, wave, h, _, _ = hex_case
+    if not oracle.have_reference():
+        pytest.skip("reference library not built")
+    M_ref, Mns_ref, _, _ = oracle.ref_batch(cfg, (0.0, 180.0, 16, 180), batch)
+    M, Mns = h.new_mueller(), h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M, Mns, precision=abi.FP64)
+    assert common.weighted_l2(M, M_ref, grid) < FP64_WL2
+    assert common.weighted_l2(Mns, Mns_ref, grid) < FP64_WL2
+
+
+def test_fp32c_against_fp64(hex_case):
+    cfg, batch, grid, wave, h, M_ref, _ = hex_case
+    M64, M32 = h.new_mueller(), h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M64, precision=abi.FP64)
+    assert h.handle_orientations_to_local_gpu(batch, M32, precision=abi.FP32C)
+    wl2 = common.weighted_l2(M32, M64, grid)
+    err = common.element_errors(M32, M64, grid)
+    print("FP32C vs FP64 weighted L2", wl2, err)
+    assert wl2 < FP32C_WL2
+    assert err["M11_max_rel"] < 1e-2
+
+
+def test_accumulates_not_overwrites(hex_case):
+    cfg, batch, grid, wave, h, M_ref, _ = hex_case
+    M = h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M, precision=abi.FP64)
+    once = M.copy()
+    assert h.handle_orientations_to_local_gpu(batch, M, precision=abi.FP64)
+    np.testing.assert_array_equal(M, 2 * once)
+
+
+def test_deterministic_and_range_split(hex_case):
+    """Bitwise repeatable; orientation ranges add up to the whole batch."""
+    cfg, batch, grid, wave, h, M_ref, _ = hex_case
+    a, b = h.new_mueller(), h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, a, precision=abi.FP64)
+    assert h.handle_orientations_to_local_gpu(batch, b, precision=abi.FP64)
+    np.testing.assert_array_equal(a, b)
+    c = h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, c, start=0, count=3, precision=abi.FP64)
+    assert h.handle_orientations_to_local_gpu(batch, c, start=3, count=100, precision=abi.FP64)
+    assert common.grid_l2(c, a) < 1e-14
+
+
+def test_staged_path_equals_host_path(hex_case):
+    import torch
+    cfg, batch, grid, wave, h, M_ref, _ = hex_case
+    M = h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M, precision=abi.FP32C)
+    st = h.stage(batch)
+    dev = torch.zeros(grid.n_az * (grid.n_zen + 1) * 16, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    h.diffract_staged(st, dev.data_ptr(), precision=abi.FP32C)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dev.cpu().numpy().reshape(M.shape), M)
+    st.free()
+
+
+def test_extinction_on_device(hex_case):
+    cfg, batch, grid, wave, h, _, _ = hex_case
+    cext = h.extinction(batch)
+    np.testing.assert_allclose(cext, batch.extinction_ot, rtol=1e-9)
+
+
+def test_release_gate_particle():
+    """The reference's CUDA release-gate particle (concave hexagon, absorbing,
+    cutoffs off): FP64 against the reference's CPU path."""
+    cfg = common.CONCAVE_ABSORBING
+    batch = common.sobol_batch("concave", 16)
+    spec = (0.0, 180.0, 24, 90)
+    grid = B.grid(*spec)
+    wave = B.wave(cfg)
+    h = GpuHandlerPO(grid, wave)
+    M, Mns = h.new_mueller(), h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M, Mns, precision=abi.FP64)
+    M_ref, Mns_ref = oracle.po_diffract(batch, grid, wave, noshadow=True)
+    assert common.weighted_l2(M, M_ref, grid) < FP64_WL2
+    assert common.weighted_l2(Mns, Mns_ref, grid) < FP64_WL2
+    if oracle.have_reference():
+        R, Rns, _, _ = oracle.ref_batch(cfg, spec, batch)
+        assert common.weighted_l2(M, R, grid) < 1e-5   # the reference's own gate
+    h.close()
+
+
+def test_fixed_orientation_config0():
+    """hexagonal column 10x20 um at beta=30, gamma=15 deg, grid
+    theta 0..180 in 0.25 deg x phi 0..360 in 2 deg, against the reference's
+    fixed-orientation path HandleBeams."""
+    cfg = common.HEX_COLUMN_10x20
+    spec = (0.0, 180.0, 180, 720)
+    grid = B.grid(*spec)
+    wave = B.wave(cfg)
+    beta, gamma = np.deg2rad(30.0), np.deg2rad(15.0)
+    batch = B.trace(cfg, [beta], [gamma], [1.0])
+    h = GpuHandlerPO(grid, wave)
+    M = h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M, precision=abi.FP64)
+    if oracle.have_reference():
+        R, _ = oracle.ref_fixed(cfg, spec, beta, gamma)
+    else:
+        R = oracle.po_diffract(batch, grid, wave)
+    assert common.weighted_l2(M, R, grid) < FP64_WL2
+    assert common.grid_l2(M, R) < FP64_WL2
+    h.close()
+
+
+def test_edge_cases(hex_case):
+    cfg, batch, grid, wave, h, _, _ = hex_case
+    # empty batch: nothing added
+    M = h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M, start=0, count=0)
+    assert not M.any()
+    # an orientation without beams contributes nothing
+    empty = B.BeamBatch(beam_offsets=np.zeros(2, np.int64), orient_weight=np.ones(1),
+                        vert_offsets=np.zeros(1, np.int64), vx=np.zeros(0), vy=np.zeros(0),
+                        slope_yx=np.zeros(0), slope_xy=np.zeros(0),
+                        edge_flags=np.zeros(0, np.uint8),
+                        beam_geom=np.zeros((0, abi.GEOM_STRIDE)), beam_flags=np.zeros(0, np.uint8))
+    mixed = B.BeamBatch.concat([empty, batch.select(0, 2), empty])
+    a, b = h.new_mueller(), h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(mixed, a)
+    assert h.handle_orientations_to_local_gpu(batch.select(0, 2), b)
+    np.testing.assert_array_equal(a, b)
+    # a beam with too few vertices is rejected like the reference's
+    # "bad-edge-data" (returns False, nothing added)
+    bad = batch.select(0, 1)
+    bad.vert_offsets = bad.vert_offsets.copy()
+    bad.vert_offsets[1] = bad.vert_offsets[0] + 2
+    bad.vert_offsets[2:] = np.maximum(bad.vert_offsets[2:], bad.vert_offsets[1])
+    M = h.new_mueller()
+    assert not h.handle_orientations_to_local_gpu(bad, M)
+    assert not M.any()
