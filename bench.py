@@ -236,8 +236,12 @@ def main():
     acc = torch.zeros(G * 16, dtype=torch.float64, device=f"cuda:{local}")
     stream = torch.cuda.current_stream().cuda_stream
 
-    # FP64 error reference (once, untimed)
     m11_err = None
+    # launch-shape autotuner on a slice of the batch (untimed)
+    tuned = {}
+    for prec, name in ((abi.FP32C, "fp32c"), (abi.FP64, "fp64")):
+        best, ms = h.autotune(staged, prec, max_orient=min(256, batch.n_orient))
+        tuned[name] = {"variant": best, "ms_per_variant": [round(m, 3) for m in ms]}
     fp64_ms = None
     M64 = None
     if not args.no_fp64:
@@ -334,6 +338,7 @@ def main():
         "e2e": {"value": total_orient / e2e_s, "unit": "orientations/s",
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
         "gpu_launches": launches,
+        "autotune": tuned,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None, "traffic": None,
                      "peak_source": "measured FFMA probe (MEASURED_PEAKS.json has no FP32 entry)",

@@ -181,6 +181,17 @@ int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams,
                         int start, int max_count, double mem_fraction,
                         int *count_out);
 
+/* Launch-shape autotuner (project-written; no counterpart in the reference):
+ * times each compiled shape of the diffraction kernel (threads per CTA,
+ * directions per thread, register budget) on the first max_orient (<= 0:
+ * all) orientations of a staged batch, keeps the fastest for `precision` in
+ * the context and returns its index in *best; ms_out[v] (may be NULL)
+ * receives the kernel time of shape v. */
+int mbs_po_autotune(mbs_po_ctx *ctx, const mbs_po_staged *staged, int precision,
+                    int max_orient, int *best, double *ms_out, int ms_len);
+/* Select a launch shape explicitly (0 = default). */
+int mbs_po_set_variant(mbs_po_ctx *ctx, int precision, int variant);
+
 /* Measured FP32 FMA throughput of the context's device in TFLOP/s (independent
  * FFMA chains on every SM), the denominator of the diffraction kernels'
  * roofline fraction.  No counterpart in the reference. */

@@ -1,20 +1,17 @@
-// po_b200.cu — B200 (sm_100a) kernels and C ABI of the PO diffraction library.
+// po_b200.cu — C ABI of the B200 (sm_100a) PO diffraction library.
 //
 // Data path of one call (replaces HandlerPO::HandleOrientationsToLocalGpu,
 // reference src/cuda/GpuDiffraction.cu:4159-4778):
 //   1. stage:    flat mbs_po_beams arrays -> HBM (one cudaMemcpyAsync each),
-//                then po_pack_kernel builds fixed DevBeam/DevVert records.
-//   2. diffract: po_diffract_kernel<Prec,NS>, one CTA per (azimuth bin,
-//                zenith tile, orientation chunk).  Each thread owns one
-//                direction and accumulates the coherent Jones sum over the
-//                orientation's beams (staged per azimuth in shared memory),
-//                converts it to Mueller and accumulates the orientation
-//                average in registers.  No atomics: each chunk writes its own
-//                partial Mueller plane.
+//                then po_pack_kernel builds the device records.
+//   2. diffract: po_diffract_kernel (regular zenith rows) and po_pole_kernel
+//                (polar rows) write one partial Mueller plane per orientation
+//                chunk, no atomics.
 //   3. reduce:   po_reduce_kernel adds the chunk partials in a fixed order
 //                into the caller's accumulator (deterministic).
 #include "mbs_po_b200.h"
 #include "po_device.cuh"
+#include "po_kernels.cuh"
 
 #include <cuda_runtime.h>
 
@@ -29,705 +26,56 @@ using namespace mbs;
 
 namespace {
 
-// ------------------------------------------------------------ parameters ---
-
-constexpr int kStageBeams = 64;     // beams per shared-memory stage
-constexpr int kStageVerts = 512;    // vertices per shared-memory stage
-
 struct GridDev {
     int n_az = 0, n_zen = 0;
     double *st = nullptr, *ct = nullptr;      // [n_zen+1]
     double *sphi = nullptr, *cphi = nullptr;  // [n_az]
     double *vf = nullptr;                     // [n_az*(n_zen+1)*3]
+    int8_t *row_kind = nullptr;               // [n_zen+1]
+    int32_t *pole_rows = nullptr;             // [n_pole]
+    int n_pole = 0;
+    int n_general = 0;
 };
 
-struct KParams {
-    const DevBeam *beams;
-    const DevVert *verts;
-    const int32_t *vbeg;       // [n_beams+1]
-    const int32_t *beam_off;   // [n_orient+1]
-    const double *weight;      // [n_orient]
-    const double *st, *ct, *sphi, *cphi, *vf;
-    int n_az, n_t;             // n_t = n_zen+1
-    int n_orient;
-    int orient_per_chunk;
-    int tile;                  // directions per CTA (== blockDim.x)
-    int tiles_per_row;
-    WaveConst wc;
-    double *partial;           // [n_chunks][16][G]
-    double *partial_ns;        // [n_chunks][16][G] or null
+// Launch shapes of the diffraction kernel: threads per CTA, directions per
+// thread and the minimum resident CTAs per SM the register budget is cut
+// for.  mbs_po_autotune times them on the caller's batch and keeps the
+// fastest per precision; variant 0 is the default.
+struct Variant {
+    int tpb, dpt, minb;
 };
+constexpr Variant kVariantsF32[] = {{128, 2, 4}, {128, 1, 6}, {256, 1, 3}, {128, 2, 3}, {128, 1, 4}};
+constexpr Variant kVariantsF64[] = {{128, 1, 4}, {128, 2, 3}, {128, 1, 3}};
+constexpr int kNumVariantsF32 = sizeof(kVariantsF32) / sizeof(Variant);
+constexpr int kNumVariantsF64 = sizeof(kVariantsF64) / sizeof(Variant);
 
-// ------------------------------------------------------------ pack kernel --
-
-struct PackParams {
-    int64_t n_beams;
-    const int64_t *vert_off;
-    const double *vx, *vy, *syx, *sxy;
-    const uint8_t *eflags;
-    const double *geom;
-    const uint8_t *bflags;
-    double k;
-    DevBeam *beams;
-    DevVert *verts;
-    int32_t *vbeg;
-    int *status;   // set to 1 on a malformed beam
+// One device allocation holding every per-batch array.
+struct Arena {
+    void *base = nullptr;
+    size_t cap = 0;
 };
-
-__global__ void po_pack_kernel(PackParams P)
-{
-    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b > P.n_beams)
-        return;
-    const int64_t v0 = P.vert_off[b];
-    P.vbeg[b] = (int32_t)v0;
-    if (b == P.n_beams)
-        return;
-    const int nv = (int)(P.vert_off[b + 1] - v0);
-    if (nv < 3 || nv > kMaxNv) {
-        atomicExch(P.status, 1);
-        return;
-    }
-    const double *g = P.geom + b * MBS_PO_GEOM_STRIDE;
-    DevBeam d;
-    // a0 = bd.hor, b0 = bd.ver as the reference packs them (GpuDiffraction.cu:301-302)
-    d.a0 = g[MBS_PO_G_BD] * g[MBS_PO_G_HOR] + g[MBS_PO_G_BD + 1] * g[MBS_PO_G_HOR + 1]
-         + g[MBS_PO_G_BD + 2] * g[MBS_PO_G_HOR + 2];
-    d.b0 = g[MBS_PO_G_BD] * g[MBS_PO_G_VER] + g[MBS_PO_G_BD + 1] * g[MBS_PO_G_VER + 1]
-         + g[MBS_PO_G_BD + 2] * g[MBS_PO_G_VER + 2];
-    for (int i = 0; i < 3; ++i) {
-        d.h[i] = g[MBS_PO_G_HOR + i];
-        d.v[i] = g[MBS_PO_G_VER + i];
-        d.c[i] = g[MBS_PO_G_CEN + i];
-    }
-    d.area = g[MBS_PO_G_AREA];
-    for (int i = 0; i < 12; ++i)
-        d.rot[i] = g[MBS_PO_G_NT + i];
-    for (int i = 0; i < 8; ++i)
-        d.jp[i] = g[MBS_PO_G_JP + i];
-    d.opath = g[MBS_PO_G_OPATH];
-    d.vbeg = (int32_t)v0;
-    d.nv = nv;
-    d.flags = P.bflags[b];
-    d.pad = 0;
-    // Small-phase prefilter.  max_v |q.v| >= |q| * sqrt(lambda_min(S)) with
-    // S the second-moment matrix of the vertices, so the moment branch
-    // (max_v |k(A x_v + B y_v)| <= 1e-3) is impossible once
-    // k^2 (A^2+B^2) lambda_min > 1e-6.
-    double sxx = 0, sxy_ = 0, syy = 0;
-    const double nan = __longlong_as_double(0x7ff8000000000000LL);
-    for (int e = 0; e < nv; ++e) {
-        const double x = P.vx[v0 + e], y = P.vy[v0 + e];
-        sxx += x * x; sxy_ += x * y; syy += y * y;
-        DevVert dv;
-        dv.x = x;
-        dv.y = y;
-        const uint8_t f = P.eflags[v0 + e];
-        dv.syx = (f & MBS_PO_EDGE_VALID_X) ? P.syx[v0 + e] : nan;
-        dv.sxy = (f & MBS_PO_EDGE_VALID_Y) ? P.sxy[v0 + e] : nan;
-        P.verts[v0 + e] = dv;
-    }
-    sxx /= nv; sxy_ /= nv; syy /= nv;
-    const double hm = 0.5 * (sxx + syy), hd = 0.5 * (sxx - syy);
-    const double lmin = hm - sqrt(hd * hd + sxy_ * sxy_);
-    const double kl2 = P.k * P.k * lmin;
-    // 0.98 keeps the prefilter conservative against rounding of lmin.
-    d.sp_thr2 = (kl2 > 1e-300) ? (kSmallPhase * kSmallPhase) / (0.98 * kl2) : 1.0e300;
-    P.beams[b] = d;
-}
-
-// ------------------------------------------------------- diffraction kernel
-
-// Shared-memory record of one beam for the CTA's azimuth (the per-azimuth
-// coefficients of precompute_theta_coeffs, HandlerPO_fast.h:504-560).
-struct __align__(16) SBeam {
-    double a_sin, a_cos, a0;   // A(theta) = sin*a_sin + cos*a_cos + a0
-    double b_sin, b_cos, b0;
-    double cm_sin, cm_cos;     // internal-beam common phase (folded into vertices)
-    double area, thr2;
-    double rot[12];
-    double jp[8];
-    float  fa[6];              // FP32 copies of the A/B coefficients
-    float  frot[12];
-    float  fjp[8];
-    float  farea, fthr2;
-    int32_t vs;                // first vertex in the stage
-    int32_t nv;
-    int32_t flags;
-    int32_t gbeam;             // global beam index
-};
-
-// Per vertex: phase(theta) = sin*ps + cos*pc + p0 (radians for FP64,
-// turns for FP32C), slopes (NaN = invalid edge for that branch).
-struct __align__(16) SVert {
-    double ps, pc, p0;
-    double x, y;
-    double syx, sxy;
-    float fsyx, fsxy;
-};
-
-template <int Prec>
-struct Acc;
-
-template <>
-struct Acc<MBS_PO_FP64> {
-    double j[8];
-    __device__ __forceinline__ void zero() {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) j[i] = 0.0;
-    }
-    __device__ __forceinline__ void add(const double *d) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) j[i] += d[i];
-    }
-    __device__ __forceinline__ void get(double *o) const {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) o[i] = j[i];
-    }
-};
-
-// FP32 Jones sums with Kahan compensation.
-template <>
-struct Acc<MBS_PO_FP32C> {
-    float s[8], c[8];
-    __device__ __forceinline__ void zero() {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) { s[i] = 0.f; c[i] = 0.f; }
-    }
-    __device__ __forceinline__ void add(const float *d) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float y = __fsub_rn(d[i], c[i]);
-            const float t = __fadd_rn(s[i], y);
-            c[i] = __fsub_rn(__fsub_rn(t, s[i]), y);
-            s[i] = t;
-        }
-    }
-    __device__ __forceinline__ void get(double *o) const {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) o[i] = (double)s[i] - (double)c[i];
-    }
-};
-
-// Per-thread direction constants.
-struct DirCtx {
-    double st, ct, cp, sp;
-    double dir[3], vf[3], vt[3], w[3], u[3];
-};
-
-__device__ __forceinline__ void cross3(const double *a, const double *b, double *o)
-{
-    o[0] = a[1] * b[2] - a[2] * b[1];
-    o[1] = a[2] * b[0] - a[0] * b[2];
-    o[2] = a[0] * b[1] - a[1] * b[0];
-}
-
-// Rotation of the beam's Jones matrix into the scattering basis
-// (GpuDiffraction.cu:831-856), rewritten with the per-direction vectors
-// w = vt x dir and u = vf x dir:  (dir x NT).vt = NT.w, (dir x NT).vf = NT.u;
-// the dir(dir.nxDT) terms vanish because vt and vf are orthogonal to dir.
-template <typename T>
-__device__ __forceinline__ void rotation(const T *rot, const T *w, const T *u,
-                                         const T *vt, const T *vf, T *r)
-{
-    const T *NT = rot, *NP = rot + 3, *DT = rot + 6, *DP = rot + 9;
-    r[0] = NT[0] * w[0] + NT[1] * w[1] + NT[2] * w[2] + DT[0] * vt[0] + DT[1] * vt[1] + DT[2] * vt[2];
-    r[1] = NP[0] * w[0] + NP[1] * w[1] + NP[2] * w[2] + DP[0] * vt[0] + DP[1] * vt[1] + DP[2] * vt[2];
-    r[2] = NT[0] * u[0] + NT[1] * u[1] + NT[2] * u[2] + DT[0] * vf[0] + DT[1] * vf[1] + DT[2] * vf[2];
-    r[3] = NP[0] * u[0] + NP[1] * u[1] + NP[2] * u[2] + DP[0] * vf[0] + DP[1] * vf[1] + DP[2] * vf[2];
-}
-
-// d = (F R) x J_phased (GpuDiffraction.cu:1149-1164).
-template <typename T>
-__device__ __forceinline__ void jones_product(T fr, T fi, const T *r, const T *jp, T *d)
-{
-    const T s00r = fr * r[0], s00i = fi * r[0];
-    const T s01r = fr * r[1], s01i = fi * r[1];
-    const T s10r = fr * r[2], s10i = fi * r[2];
-    const T s11r = fr * r[3], s11i = fi * r[3];
-    d[0] = s00r * jp[0] - s00i * jp[1] + s01r * jp[4] - s01i * jp[5];
-    d[1] = s00r * jp[1] + s00i * jp[0] + s01r * jp[5] + s01i * jp[4];
-    d[2] = s00r * jp[2] - s00i * jp[3] + s01r * jp[6] - s01i * jp[7];
-    d[3] = s00r * jp[3] + s00i * jp[2] + s01r * jp[7] + s01i * jp[6];
-    d[4] = s10r * jp[0] - s10i * jp[1] + s11r * jp[4] - s11i * jp[5];
-    d[5] = s10r * jp[1] + s10i * jp[0] + s11r * jp[5] + s11i * jp[4];
-    d[6] = s10r * jp[2] - s10i * jp[3] + s11r * jp[6] - s11i * jp[7];
-    d[7] = s10r * jp[3] + s10i * jp[2] + s11r * jp[7] + s11i * jp[6];
-}
-
-// Moment branch in FP64 from the global records (rare).  Returns false when
-// the exact test rejects the small-phase branch.
-__device__ bool small_phase_fp64(const DevBeam &gb, const DevVert *gv, const DirCtx &dc,
-                                 const WaveConst &wc, double &fr, double &fi)
-{
-    const double a_sin = -dc.cp * gb.h[0] - dc.sp * gb.h[1];
-    const double b_sin = -dc.cp * gb.v[0] - dc.sp * gb.v[1];
-    const double A = dc.st * a_sin + dc.ct * gb.h[2] + gb.a0;
-    const double B = dc.st * b_sin + dc.ct * gb.v[2] + gb.b0;
-    double pr, pi;
-    if (!small_phase_factor(&gv[gb.vbeg].x, &gv[gb.vbeg].y, 4, gb.nv, A, B, wc.k, pr, pi))
-        return false;
-    const double sgn = wc.legacy_sign ? 1.0 : -1.0;
-    const double ar = sgn * wc.icw_re * gb.area, ai = sgn * wc.icw_im * gb.area;
-    fr = ar * pr - ai * pi;
-    fi = ar * pi + ai * pr;
-    if (!(gb.flags & MBS_PO_BEAM_EXTERNAL)) {
-        // common internal-beam phase (GpuDiffraction.cu:1106-1143)
-        const double cm = -wc.k * (dc.st * (dc.cp * gb.c[0] + dc.sp * gb.c[1]) + dc.ct * (-gb.c[2]));
-        double s, c;
-        sincos_fp64(cm, &s, &c);
-        const double tr = fr * c - fi * s;
-        fi = fr * s + fi * c;
-        fr = tr;
-    }
-    return true;
-}
-
-// FP64 contribution of one beam to one direction.
-__device__ __forceinline__ bool beam_fp64(const SBeam &b, const SVert *sv, const DevBeam *gbeams,
-                                          const DevVert *gverts, const DirCtx &dc,
-                                          const WaveConst &wc, double *d)
-{
-    const double A = fma(dc.st, b.a_sin, fma(dc.ct, b.a_cos, b.a0));
-    const double B = fma(dc.st, b.b_sin, fma(dc.ct, b.b_cos, b.b0));
-    double fr, fi;
-    bool done = false;
-    if (A * A + B * B <= b.thr2)
-        done = small_phase_fp64(gbeams[b.gbeam], gverts, dc, wc, fr, fi);
-    if (!done) {
-        const bool useX = fabs(B) > fabs(A);
-        const double al = useX ? A : B, be = useX ? B : A;
-        const SVert *v = sv + b.vs;
-        const int nv = b.nv;
-        double s0, c0;
-        sincos_fp64(fma(dc.st, v[0].ps, fma(dc.ct, v[0].pc, v[0].p0)), &s0, &c0);
-        double cprev = c0, sprev = s0, sr = 0.0, si = 0.0;
-        for (int e = 0; e < nv; ++e) {
-            const int en = (e + 1 < nv) ? e + 1 : 0;
-            double cn = c0, sn = s0;
-            if (en != 0)
-                sincos_fp64(fma(dc.st, v[en].ps, fma(dc.ct, v[en].pc, v[en].p0)), &sn, &cn);
-            const double s = useX ? v[e].syx : v[e].sxy;
-            if (s == s) {
-                const double coef = fma(s, be, al);   // A + s*B  or  A*s + B
-                const double ac = fabs(coef);
-                const double inv = (ac > wc.eps1) ? 1.0 / coef : 0.0;
-                sr = fma(cn - cprev, inv, sr);
-                si = fma(sn - sprev, inv, si);
-                if (ac <= wc.eps1) {
-                    const double delta = useX ? (v[en].x - v[e].x) : (v[en].y - v[e].y);
-                    stable_edge(cprev, sprev, delta, coef, wc.k, sr, si);
-                }
-            }
-            cprev = cn;
-            sprev = sn;
-        }
-        const double m = useX ? 1.0 / B : -1.0 / A;
-        sr *= m;
-        si *= m;
-        fr = wc.cw_re * sr - wc.cw_im * si;
-        fi = wc.cw_re * si + wc.cw_im * sr;
-    }
-    if (isnan(fr))
-        return false;
-    double r[4];
-    rotation(b.rot, dc.w, dc.u, dc.vt, dc.vf, r);
-    jones_product(fr, fi, r, b.jp, d);
-    return true;
-}
-
-// Fraction of the phase u (in turns) as a float in [-0.5, 0.5): adding
-// 1.5*2^29 leaves frac(u) rounded to 2^-23 in the low 23 mantissa bits.
-__device__ __forceinline__ float turn_fraction(double u)
-{
-    const double t = u + 805306368.0;
-    const unsigned lo = (unsigned)__double2loint(t);
-    float f = __int_as_float(0x3F800000u | (lo & 0x007FFFFFu)) - 1.0f;
-    return f >= 0.5f ? f - 1.0f : f;
-}
-
-__device__ __forceinline__ void phasor_f32(double u, float &s, float &c)
-{
-    __sincosf(turn_fraction(u) * 6.28318530717958647f, &s, &c);
-}
-
-// FP32C contribution of one beam to one direction.
-__device__ __forceinline__ bool beam_fp32c(const SBeam &b, const SVert *sv, const DevBeam *gbeams,
-                                           const DevVert *gverts, const DirCtx &dc,
-                                           const float *fdir, const WaveConst &wc, float *d)
-{
-    const float st = fdir[0], ct = fdir[1];
-    const float A = fmaf(st, b.fa[0], fmaf(ct, b.fa[1], b.fa[2]));
-    const float B = fmaf(st, b.fa[3], fmaf(ct, b.fa[4], b.fa[5]));
-    float fr, fi;
-    bool done = false;
-    if (A * A + B * B <= b.fthr2) {
-        double dr, di;
-        done = small_phase_fp64(gbeams[b.gbeam], gverts, dc, wc, dr, di);
-        fr = (float)dr;
-        fi = (float)di;
-    }
-    if (!done) {
-        const bool useX = fabsf(B) > fabsf(A);
-        const float al = useX ? A : B, be = useX ? B : A;
-        const float eps = (float)wc.eps1_f32;
-        const SVert *v = sv + b.vs;
-        const int nv = b.nv;
-        float s0, c0;
-        phasor_f32(fma(dc.st, v[0].ps, fma(dc.ct, v[0].pc, v[0].p0)), s0, c0);
-        float cprev = c0, sprev = s0, sr = 0.f, si = 0.f;
-        for (int e = 0; e < nv; ++e) {
-            const int en = (e + 1 < nv) ? e + 1 : 0;
-            float cn = c0, sn = s0;
-            if (en != 0)
-                phasor_f32(fma(dc.st, v[en].ps, fma(dc.ct, v[en].pc, v[en].p0)), sn, cn);
-            const float s = useX ? v[e].fsyx : v[e].fsxy;
-            if (s == s) {
-                const float coef = fmaf(s, be, al);
-                const float ac = fabsf(coef);
-                if (ac > eps) {
-                    const float inv = __frcp_rn(coef);
-                    sr = fmaf(cn - cprev, inv, sr);
-                    si = fmaf(sn - sprev, inv, si);
-                } else {
-                    // near-singular edge: FP64 half-angle form (rare)
-                    const DevBeam &gb = gbeams[b.gbeam];
-                    const DevVert *gv = gverts + gb.vbeg;
-                    const double a_sin = -dc.cp * gb.h[0] - dc.sp * gb.h[1];
-                    const double b_sin = -dc.cp * gb.v[0] - dc.sp * gb.v[1];
-                    const double Ad = dc.st * a_sin + dc.ct * gb.h[2] + gb.a0;
-                    const double Bd = dc.st * b_sin + dc.ct * gb.v[2] + gb.b0;
-                    const double sd = useX ? gv[e].syx : gv[e].sxy;
-                    const double cd = useX ? fma(sd, Bd, Ad) : fma(sd, Ad, Bd);
-                    const double delta = useX ? (gv[en].x - gv[e].x) : (gv[en].y - gv[e].y);
-                    double dsr = 0.0, dsi = 0.0;
-                    if (fabs(cd) > wc.eps1) {
-                        // exact difference quotient from the FP64 phases
-                        const double ud0 = fma(dc.st, v[e].ps, fma(dc.ct, v[e].pc, v[e].p0)) * kTwoPi;
-                        const double ud1 = fma(dc.st, v[en].ps, fma(dc.ct, v[en].pc, v[en].p0)) * kTwoPi;
-                        double s1, c1, s2, c2;
-                        sincos_fp64(ud0, &s1, &c1);
-                        sincos_fp64(ud1, &s2, &c2);
-                        dsr = (c2 - c1) / cd;
-                        dsi = (s2 - s1) / cd;
-                    } else {
-                        stable_edge((double)cprev, (double)sprev, delta, cd, wc.k, dsr, dsi);
-                    }
-                    sr += (float)dsr;
-                    si += (float)dsi;
-                }
-            }
-            cprev = cn;
-            sprev = sn;
-        }
-        const float m = useX ? __frcp_rn(B) : -__frcp_rn(A);
-        sr *= m;
-        si *= m;
-        const float cwr = (float)wc.cw_re, cwi = (float)wc.cw_im;
-        fr = cwr * sr - cwi * si;
-        fi = cwr * si + cwi * sr;
-    }
-    if (isnan(fr))
-        return false;
-    float r[4];
-    rotation(b.frot, fdir + 2, fdir + 5, fdir + 8, fdir + 11, r);
-    jones_product(fr, fi, r, b.fjp, d);
-    return true;
-}
-
-template <int Prec, bool NS>
-__global__ void __launch_bounds__(128) po_diffract_kernel(KParams P)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SBeam *sb = reinterpret_cast<SBeam *>(smem_raw);
-    SVert *sv = reinterpret_cast<SVert *>(smem_raw + kStageBeams * sizeof(SBeam));
-
-    const int p = blockIdx.x / P.tiles_per_row;
-    const int tile = blockIdx.x - p * P.tiles_per_row;
-    const int t = tile * P.tile + threadIdx.x;
-    const bool active = t < P.n_t;
-    const int chunk = blockIdx.y;
-    const int o0 = chunk * P.orient_per_chunk;
-    const int o1 = min(P.n_orient, o0 + P.orient_per_chunk);
-    const WaveConst &wc = P.wc;
-    const double k = wc.k;
-    const double cp = P.cphi[p], sp = P.sphi[p];
-
-    DirCtx dc;
-    {
-        const int tt = active ? t : P.n_t - 1;
-        dc.st = P.st[tt];
-        dc.ct = P.ct[tt];
-        dc.cp = cp;
-        dc.sp = sp;
-        dc.dir[0] = dc.st * cp;
-        dc.dir[1] = dc.st * sp;
-        dc.dir[2] = -dc.ct;
-        const double *vfp = P.vf + ((size_t)p * P.n_t + tt) * 3;
-        dc.vf[0] = vfp[0]; dc.vf[1] = vfp[1]; dc.vf[2] = vfp[2];
-        cross3(dc.vf, dc.dir, dc.u);          // u = vf x dir
-        const double l2 = dc.u[0] * dc.u[0] + dc.u[1] * dc.u[1] + dc.u[2] * dc.u[2];
-        const double il = (l2 > 1e-30) ? rsqrt(l2) : 1.0;   // transverse_basis_gpu
-        dc.vt[0] = dc.u[0] * il; dc.vt[1] = dc.u[1] * il; dc.vt[2] = dc.u[2] * il;
-        cross3(dc.vt, dc.dir, dc.w);          // w = vt x dir
-    }
-    float fdir[14];
-    fdir[0] = (float)dc.st;
-    fdir[1] = (float)dc.ct;
-    for (int i = 0; i < 3; ++i) {
-        fdir[2 + i] = (float)dc.w[i];
-        fdir[5 + i] = (float)dc.u[i];
-        fdir[8 + i] = (float)dc.vt[i];
-        fdir[11 + i] = (float)dc.vf[i];
-    }
-
-    double M[16], Mns[NS ? 16 : 1];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) M[i] = 0.0;
-    if (NS) {
-#pragma unroll
-        for (int i = 0; i < (NS ? 16 : 1); ++i) Mns[i] = 0.0;
-    }
-    const double turn = (Prec == MBS_PO_FP32C) ? kInvTwoPi : 1.0;
-
-    for (int o = o0; o < o1; ++o) {
-        Acc<Prec> J, Jn;
-        J.zero();
-        Jn.zero();
-        const int b0 = P.beam_off[o], b1 = P.beam_off[o + 1];
-        for (int bs = b0; bs < b1;) {
-            // stage [bs, be): at most kStageBeams beams and kStageVerts vertices
-            int lo = bs + 1, hi = min(b1, bs + kStageBeams);
-            const int vb0 = P.vbeg[bs];
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (P.vbeg[mid] - vb0 <= kStageVerts) lo = mid; else hi = mid - 1;
-            }
-            const int be = lo;
-            const int nb = be - bs;
-            for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-                const DevBeam &g = P.beams[bs + i];
-                SBeam s;
-                s.a_sin = -cp * g.h[0] - sp * g.h[1];
-                s.a_cos = g.h[2];
-                s.a0 = g.a0;
-                s.b_sin = -cp * g.v[0] - sp * g.v[1];
-                s.b_cos = g.v[2];
-                s.b0 = g.b0;
-                const bool internal = !(g.flags & MBS_PO_BEAM_EXTERNAL);
-                s.cm_sin = internal ? -k * (cp * g.c[0] + sp * g.c[1]) : 0.0;
-                s.cm_cos = internal ? -k * (-g.c[2]) : 0.0;
-                s.area = g.area;
-                s.thr2 = g.sp_thr2;
-                for (int q = 0; q < 12; ++q) { s.rot[q] = g.rot[q]; s.frot[q] = (float)g.rot[q]; }
-                for (int q = 0; q < 8; ++q) { s.jp[q] = g.jp[q]; s.fjp[q] = (float)g.jp[q]; }
-                s.fa[0] = (float)s.a_sin; s.fa[1] = (float)s.a_cos; s.fa[2] = (float)s.a0;
-                s.fa[3] = (float)s.b_sin; s.fa[4] = (float)s.b_cos; s.fa[5] = (float)s.b0;
-                s.farea = (float)s.area;
-                // FP32 prefilter: widen for the rounding of A, B in float.
-                s.fthr2 = (float)fmin(4.0 * g.sp_thr2 + 1e-12, 3.0e38);
-                s.vs = g.vbeg - vb0;
-                s.nv = g.nv;
-                s.flags = g.flags;
-                s.gbeam = bs + i;
-                for (int e = 0; e < g.nv; ++e) {
-                    const DevVert gv = P.verts[g.vbeg + e];
-                    SVert w;
-                    w.ps = (k * (s.a_sin * gv.x + s.b_sin * gv.y) + s.cm_sin) * turn;
-                    w.pc = (k * (s.a_cos * gv.x + s.b_cos * gv.y) + s.cm_cos) * turn;
-                    w.p0 = (k * (s.a0 * gv.x + s.b0 * gv.y)) * turn;
-                    w.x = gv.x;
-                    w.y = gv.y;
-                    w.syx = gv.syx;
-                    w.sxy = gv.sxy;
-                    w.fsyx = (float)gv.syx;
-                    w.fsxy = (float)gv.sxy;
-                    sv[s.vs + e] = w;
-                }
-                sb[i] = s;
-            }
-            __syncthreads();
-            if (active) {
-                for (int j = 0; j < nb; ++j) {
-                    const SBeam &b = sb[j];
-                    if constexpr (Prec == MBS_PO_FP64) {
-                        double d[8];
-                        if (beam_fp64(b, sv, P.beams, P.verts, dc, wc, d)) {
-                            J.add(d);
-                            if (NS && !(b.flags & MBS_PO_BEAM_EXTERNAL))
-                                Jn.add(d);
-                        }
-                    } else {
-                        float d[8];
-                        if (beam_fp32c(b, sv, P.beams, P.verts, dc, fdir, wc, d)) {
-                            J.add(d);
-                            if (NS && !(b.flags & MBS_PO_BEAM_EXTERNAL))
-                                Jn.add(d);
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-            bs = be;
-        }
-        if (active) {
-            const double wgt = P.weight[o] * 0.25;
-            double j[8];
-            J.get(j);
-            mueller_add(j, wgt, M);
-            if (NS) {
-                Jn.get(j);
-                mueller_add(j, wgt, Mns);
-            }
-        }
-    }
-    if (active) {
-        const size_t G = (size_t)P.n_az * P.n_t;
-        const size_t g = (size_t)p * P.n_t + t;
-        double *out = P.partial + (size_t)chunk * 16 * G + g;
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-            out[i * G] = M[i];
-        if (NS) {
-            double *outn = P.partial_ns + (size_t)chunk * 16 * G + g;
-#pragma unroll
-            for (int i = 0; i < (NS ? 16 : 1); ++i)
-                outn[i * G] = Mns[i];
-        }
-    }
-}
-
-// out[g*16+k] += sum_c partial[c][k][g], in chunk order.
-__global__ void po_reduce_kernel(const double *__restrict__ partial, int n_chunks,
-                                 int64_t G, double *__restrict__ out)
-{
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= G * 16)
-        return;
-    const int64_t k = i / G, g = i - k * G;
-    double s = 0.0;
-    for (int c = 0; c < n_chunks; ++c)
-        s += partial[(int64_t)c * 16 * G + i];
-    out[g * 16 + k] += s;
-}
-
-// --------------------------------------------------------- extinction kernel
-// One thread per orientation: HandlerPO::ComputeForwardExtinctionOt
-// (reference HandlerPO.cpp:1812-2009) at theta = 0, phi = 0.
-__global__ void po_extinction_kernel(const DevBeam *beams, const DevVert *verts,
-                                     const int32_t *beam_off, const double *weight,
-                                     int n_orient, WaveConst wc, double *cext)
-{
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= n_orient)
-        return;
-    const double k = wc.k;
-    double f00r = 0, f00i = 0, f11r = 0, f11i = 0;
-    const double vf[3] = {0.0, 1.0, 0.0}, dir[3] = {0.0, 0.0, -1.0};
-    double u[3], vt[3], w[3];
-    cross3(vf, dir, u);
-    const double l2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-    const double il = rsqrt(l2);
-    vt[0] = u[0] * il; vt[1] = u[1] * il; vt[2] = u[2] * il;
-    cross3(vt, dir, w);
-    for (int b = beam_off[o]; b < beam_off[o + 1]; ++b) {
-        const DevBeam &g = beams[b];
-        const bool external = (g.flags & MBS_PO_BEAM_EXTERNAL) != 0;
-        if (wc.ot_phase_avg && !external)
-            continue;
-        const DevVert *v = verts + g.vbeg;
-        const int nv = g.nv;
-        const double A = 1.0 * g.h[2] + g.a0;
-        const double B = 1.0 * g.v[2] + g.b0;
-        double fr, fi, pr, pi;
-        if (small_phase_factor(&v[0].x, &v[0].y, 4, nv, A, B, k, pr, pi)) {
-            const double sgn = wc.legacy_sign ? 1.0 : -1.0;
-            const double ar = sgn * wc.icw_re * g.area, ai = sgn * wc.icw_im * g.area;
-            fr = ar * pr - ai * pi;
-            fi = ar * pi + ai * pr;
-        } else {
-            const bool useX = fabs(B) > fabs(A);
-            double sr = 0, si = 0;
-            double c0, s0;
-            sincos_fp64(k * (g.h[2] * v[0].x + g.v[2] * v[0].y) + k * (g.a0 * v[0].x + g.b0 * v[0].y), &s0, &c0);
-            double cprev = c0, sprev = s0;
-            for (int e = 0; e < nv; ++e) {
-                const int en = (e + 1 < nv) ? e + 1 : 0;
-                double cn = c0, sn = s0;
-                if (en != 0)
-                    sincos_fp64(k * (g.h[2] * v[en].x + g.v[2] * v[en].y) + k * (g.a0 * v[en].x + g.b0 * v[en].y), &sn, &cn);
-                const double s = useX ? v[e].syx : v[e].sxy;
-                if (s == s) {
-                    const double coef = useX ? A + s * B : A * s + B;
-                    const double inv = fabs(coef) > wc.eps1 ? 1.0 / coef : 0.0;
-                    sr += (cn - cprev) * inv;
-                    si += (sn - sprev) * inv;
-                    if (fabs(coef) <= wc.eps1)
-                        stable_edge(cprev, sprev, useX ? v[en].x - v[e].x : v[en].y - v[e].y, coef, k, sr, si);
-                }
-                cprev = cn;
-                sprev = sn;
-            }
-            if (useX) {
-                if (fabs(B) <= wc.eps1) continue;
-                sr /= B; si /= B;
-            } else {
-                if (fabs(A) <= wc.eps1) continue;
-                sr *= -1.0 / A; si *= -1.0 / A;
-            }
-            fr = wc.cw_re * sr - wc.cw_im * si;
-            fi = wc.cw_re * si + wc.cw_im * sr;
-        }
-        if (isnan(fr))
-            continue;
-        const double ref = external ? g.opath : wc.ot_far_ref;
-        double dpr = 1.0, dpi = 0.0;
-        if (!external)
-            sincos_fp64(-k * (1.0 * (-g.c[2]) + ref), &dpi, &dpr);
-        else if (ref != 0.0)
-            sincos_fp64(-k * ref, &dpi, &dpr);
-        const double cr = fr * dpr - fi * dpi, ci = fr * dpi + fi * dpr;
-        double r[4], d[8];
-        rotation(g.rot, w, u, vt, vf, r);
-        // reference rotation carries 0.5 on the CPU (HandlerPO_fast.h:643-646)
-        for (int q = 0; q < 4; ++q) r[q] *= 0.5;
-        jones_product(cr, ci, r, g.jp, d);
-        f00r += d[0]; f00i += d[1];
-        f11r += d[6]; f11i += d[7];
-    }
-    const double fwr = f00r + f11r, fwi = f00i + f11i;
-    double amp = fwi;
-    if (wc.ot_ping != 0.0) {
-        double sn, cs;
-        sincos_fp64(2.0 * k * wc.ot_ping, &sn, &cs);
-        amp = fwi * cs - fwr * sn;
-    }
-    const double c = wc.wavelength * amp * weight[o];
-    cext[o] = isfinite(c) ? c : 0.0;
-}
 
 }  // namespace
 
-// =============================================================== host side ==
-
 struct mbs_po_staged {
+    Arena arena;
     DevBeam *beams = nullptr;
     DevVert *verts = nullptr;
+    BeamRec *brec = nullptr;
+    VertRec *vrec = nullptr;
+    double *moments = nullptr;
     int32_t *vbeg = nullptr;
     int32_t *beam_off = nullptr;
     double *weight = nullptr;
     int n_orient = 0;
     int64_t n_beams = 0, n_verts = 0;
-    int64_t cap_beams = 0, cap_verts = 0, cap_orient = 0, cap_vbeg = 0;
     int max_nv = 0;
-    std::vector<int64_t> beams_per_orient_prefix;   // host copy for statistics
-    int64_t sum_beams = 0;
-    int64_t sum_verts = 0;
 };
 
 struct mbs_po_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;          // polar-row kernel, concurrent
     std::string err;
     bool has_grid = false, has_wave = false;
     GridDev grid;
@@ -740,12 +88,11 @@ struct mbs_po_ctx {
     size_t macc_cap = 0;
     double *hres = nullptr;      // pinned [2][G*16]
     size_t hres_cap = 0;
-    // raw upload buffers for staging
-    void *raw = nullptr;
-    size_t raw_cap = 0;
+    Arena raw;                   // raw upload area for staging
     int *d_status = nullptr;
     mbs_po_staged host_staged;   // reused by mbs_po_diffract
-    cudaEvent_t ev[6] = {};
+    cudaEvent_t ev[8] = {};
+    int variant[2] = {0, 0};     // chosen launch shape per precision
 };
 
 namespace {
@@ -785,27 +132,26 @@ int ensure(mbs_po_ctx *ctx, T *&ptr, size_t &cap, size_t n, const char *what)
     return MBS_PO_OK;
 }
 
-int ensure64(mbs_po_ctx *ctx, DevBeam *&p, int64_t &cap, int64_t n)
+int ensure_arena(mbs_po_ctx *ctx, Arena &a, size_t bytes, const char *what)
 {
-    size_t c = (size_t)cap;
-    int rc = ensure(ctx, p, c, (size_t)n, "beams");
-    cap = (int64_t)c;
-    return rc;
+    if (bytes <= a.cap && a.base)
+        return MBS_PO_OK;
+    cudaFree(a.base);
+    a.base = nullptr;
+    a.cap = 0;
+    cudaError_t e = cudaMalloc(&a.base, std::max<size_t>(bytes, 256));
+    if (e != cudaSuccess)
+        return fail(ctx, MBS_PO_ENOMEM, std::string("cudaMalloc ") + what + ": " + cudaGetErrorString(e));
+    a.cap = std::max<size_t>(bytes, 256);
+    return MBS_PO_OK;
 }
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 void staged_release(mbs_po_staged *s)
 {
-    cudaFree(s->beams);
-    cudaFree(s->verts);
-    cudaFree(s->vbeg);
-    cudaFree(s->beam_off);
-    cudaFree(s->weight);
-    s->beams = nullptr;
-    s->verts = nullptr;
-    s->vbeg = nullptr;
-    s->beam_off = nullptr;
-    s->weight = nullptr;
-    s->cap_beams = s->cap_verts = s->cap_orient = s->cap_vbeg = 0;
+    cudaFree(s->arena.base);
+    *s = mbs_po_staged();
 }
 
 int validate(mbs_po_ctx *ctx, const mbs_po_beams *b)
@@ -835,13 +181,20 @@ int validate(mbs_po_ctx *ctx, const mbs_po_beams *b)
     return MBS_PO_OK;
 }
 
+void grid_release(GridDev &d)
+{
+    cudaFree(d.st); cudaFree(d.ct); cudaFree(d.sphi); cudaFree(d.cphi); cudaFree(d.vf);
+    cudaFree(d.row_kind); cudaFree(d.pole_rows);
+    d = GridDev();
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI --
 
 extern "C" const char *mbs_po_version(void)
 {
-    return "mbs-b200 0.1 sm_100a (FP64 plain + FP32 compensated PO diffraction)";
+    return "mbs-b200 0.2 sm_100a (FP64 plain + FP32 compensated PO diffraction)";
 }
 
 extern "C" int mbs_po_create(mbs_po_ctx **out, int device)
@@ -854,7 +207,9 @@ extern "C" int mbs_po_create(mbs_po_ctx **out, int device)
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess)
         e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-    for (int i = 0; i < 6 && e == cudaSuccess; ++i)
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i)
         e = cudaEventCreate(&ctx->ev[i]);
     if (e == cudaSuccess)
         e = cudaMalloc((void **)&ctx->d_status, sizeof(int));
@@ -873,21 +228,21 @@ extern "C" int mbs_po_destroy(mbs_po_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
-    cudaFree(ctx->grid.st);
-    cudaFree(ctx->grid.ct);
-    cudaFree(ctx->grid.sphi);
-    cudaFree(ctx->grid.cphi);
-    cudaFree(ctx->grid.vf);
+    if (ctx->side)
+        cudaStreamSynchronize(ctx->side);
+    grid_release(ctx->grid);
     cudaFree(ctx->partial);
     cudaFree(ctx->macc);
     cudaFreeHost(ctx->hres);
-    cudaFree(ctx->raw);
+    cudaFree(ctx->raw.base);
     cudaFree(ctx->d_status);
     staged_release(&ctx->host_staged);
-    for (int i = 0; i < 6; ++i)
+    for (int i = 0; i < 8; ++i)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
     if (ctx->stream)
         cudaStreamDestroy(ctx->stream);
+    if (ctx->side)
+        cudaStreamDestroy(ctx->side);
     delete ctx;
     return MBS_PO_OK;
 }
@@ -913,22 +268,55 @@ extern "C" int mbs_po_set_grid(mbs_po_ctx *ctx, const mbs_po_grid *g)
         sphi[p] = std::sin(phi);
         cphi[p] = std::cos(phi);
     }
+    // Zenith rows whose basis is not (-sin phi, cos phi, 0) are the polar
+    // rows of ScatteringRange::ComputeSphereDirections (Handler.h:147-160).
+    // When the basis and the direction are the same for every azimuth bin the
+    // row is evaluated once (kind 1); otherwise per direction (kind 2).
+    std::vector<int8_t> kind(nT, 0);
+    std::vector<int32_t> poles;
+    int nGeneral = 0;
+    for (int t = 0; t < nT; ++t) {
+        bool regular = true, same = true;
+        const double *v0 = g->vf + (size_t)t * 3;
+        for (int p = 0; p < nAz; ++p) {
+            const double *v = g->vf + ((size_t)p * nT + t) * 3;
+            if (std::fabs(v[0] + sphi[p]) + std::fabs(v[1] - cphi[p]) + std::fabs(v[2]) > 1e-12)
+                regular = false;
+            if (v[0] != v0[0] || v[1] != v0[1] || v[2] != v0[2])
+                same = false;
+        }
+        if (regular)
+            continue;
+        if (same && std::fabs(st[t]) < 1e-12) {
+            kind[t] = 1;
+            poles.push_back(t);
+        } else {
+            kind[t] = 2;
+            ++nGeneral;
+        }
+    }
     GridDev &d = ctx->grid;
-    cudaFree(d.st); cudaFree(d.ct); cudaFree(d.sphi); cudaFree(d.cphi); cudaFree(d.vf);
-    d = GridDev();
+    grid_release(d);
     const size_t nvf = (size_t)nAz * nT * 3;
     CK(cudaMalloc((void **)&d.st, nT * sizeof(double)), "cudaMalloc grid");
     CK(cudaMalloc((void **)&d.ct, nT * sizeof(double)), "cudaMalloc grid");
     CK(cudaMalloc((void **)&d.sphi, nAz * sizeof(double)), "cudaMalloc grid");
     CK(cudaMalloc((void **)&d.cphi, nAz * sizeof(double)), "cudaMalloc grid");
     CK(cudaMalloc((void **)&d.vf, nvf * sizeof(double)), "cudaMalloc grid");
+    CK(cudaMalloc((void **)&d.row_kind, nT * sizeof(int8_t)), "cudaMalloc grid");
+    CK(cudaMalloc((void **)&d.pole_rows, std::max<size_t>(poles.size(), 1) * sizeof(int32_t)), "cudaMalloc grid");
     CK(cudaMemcpy(d.st, st.data(), nT * sizeof(double), cudaMemcpyHostToDevice), "grid copy");
     CK(cudaMemcpy(d.ct, ct.data(), nT * sizeof(double), cudaMemcpyHostToDevice), "grid copy");
     CK(cudaMemcpy(d.sphi, sphi.data(), nAz * sizeof(double), cudaMemcpyHostToDevice), "grid copy");
     CK(cudaMemcpy(d.cphi, cphi.data(), nAz * sizeof(double), cudaMemcpyHostToDevice), "grid copy");
     CK(cudaMemcpy(d.vf, g->vf, nvf * sizeof(double), cudaMemcpyHostToDevice), "grid copy");
+    CK(cudaMemcpy(d.row_kind, kind.data(), nT * sizeof(int8_t), cudaMemcpyHostToDevice), "grid copy");
+    if (!poles.empty())
+        CK(cudaMemcpy(d.pole_rows, poles.data(), poles.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "grid copy");
     d.n_az = nAz;
     d.n_zen = g->n_zen;
+    d.n_pole = (int)poles.size();
+    d.n_general = nGeneral;
     ctx->has_grid = true;
     return MBS_PO_OK;
 }
@@ -957,54 +345,53 @@ extern "C" int mbs_po_set_wave(mbs_po_ctx *ctx, const mbs_po_wave *w)
 
 namespace {
 
-// Upload a batch and build device records into `s` (capacity reused).
+// Upload a batch and build the device records into `s` (capacity reused).
+// The records carry wave-dependent coefficients: a staged batch belongs to
+// the wave constants set when it was staged.
 int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStream_t st)
 {
     int rc = validate(ctx, b);
     if (rc)
         return rc;
+    if (!ctx->has_wave)
+        return fail(ctx, MBS_PO_ESTATE, "wave constants must be set before staging");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const int64_t nB = b->n_beams, nV = b->n_verts, nO = b->n_orient;
-    // raw upload area: vert_off, vx, vy, syx, sxy, geom (doubles/int64), flags (bytes)
-    const size_t bytes_vo = (nB + 1) * 8, bytes_v = nV * 8, bytes_g = nB * MBS_PO_GEOM_STRIDE * 8;
-    const size_t off_vo = 0, off_vx = off_vo + bytes_vo, off_vy = off_vx + bytes_v;
-    const size_t off_syx = off_vy + bytes_v, off_sxy = off_syx + bytes_v, off_g = off_sxy + bytes_v;
-    const size_t off_ef = off_g + bytes_g, off_bf = off_ef + ((nV + 15) & ~(size_t)15);
-    const size_t raw_bytes = off_bf + ((nB + 15) & ~(size_t)15) + 16;
-    size_t rawcap = ctx->raw_cap;
-    unsigned char *raw = (unsigned char *)ctx->raw;
-    if (raw_bytes > rawcap || !raw) {
-        cudaFree(raw);
-        ctx->raw = nullptr;
-        ctx->raw_cap = 0;
-        cudaError_t e = cudaMalloc(&ctx->raw, raw_bytes);
-        if (e != cudaSuccess)
-            return fail(ctx, MBS_PO_ENOMEM, std::string("cudaMalloc staging: ") + cudaGetErrorString(e));
-        ctx->raw_cap = raw_bytes;
-        raw = (unsigned char *)ctx->raw;
-    }
-    size_t cap;
-    cap = (size_t)s->cap_verts;
-    if ((rc = ensure(ctx, s->verts, cap, (size_t)std::max<int64_t>(nV, 1), "verts"))) return rc;
-    s->cap_verts = (int64_t)cap;
-    if ((rc = ensure64(ctx, s->beams, s->cap_beams, std::max<int64_t>(nB, 1)))) return rc;
-    if (s->cap_vbeg < nB + 1 || !s->vbeg) {
-        cudaFree(s->vbeg);
-        s->vbeg = nullptr;
-        s->cap_vbeg = 0;
-        CK(cudaMalloc((void **)&s->vbeg, (size_t)(nB + 1) * sizeof(int32_t)), "cudaMalloc vbeg");
-        s->cap_vbeg = nB + 1;
-    }
-    if ((size_t)s->cap_orient < (size_t)nO + 1 || !s->beam_off) {
-        cudaFree(s->beam_off);
-        cudaFree(s->weight);
-        s->beam_off = nullptr;
-        s->weight = nullptr;
-        CK(cudaMalloc((void **)&s->beam_off, (nO + 1) * sizeof(int32_t)), "cudaMalloc offsets");
-        CK(cudaMalloc((void **)&s->weight, std::max<int64_t>(nO, 1) * sizeof(double)), "cudaMalloc weights");
-        s->cap_orient = nO + 1;
-    }
-    // orientation offsets to int32 on the host (small)
+    // raw upload area: vert_off, vx, vy, syx, sxy, geom, flags
+    const size_t off_vo = 0;
+    const size_t off_vx = off_vo + align256((nB + 1) * 8);
+    const size_t off_vy = off_vx + align256(nV * 8);
+    const size_t off_syx = off_vy + align256(nV * 8);
+    const size_t off_sxy = off_syx + align256(nV * 8);
+    const size_t off_g = off_sxy + align256(nV * 8);
+    const size_t off_ef = off_g + align256(nB * MBS_PO_GEOM_STRIDE * 8);
+    const size_t off_bf = off_ef + align256(nV);
+    const size_t raw_bytes = off_bf + align256(nB);
+    if ((rc = ensure_arena(ctx, ctx->raw, raw_bytes, "staging")))
+        return rc;
+    unsigned char *raw = (unsigned char *)ctx->raw.base;
+    // device records
+    const size_t o_beams = 0;
+    const size_t o_verts = o_beams + align256(nB * sizeof(DevBeam));
+    const size_t o_brec = o_verts + align256(nV * sizeof(DevVert));
+    const size_t o_vrec = o_brec + align256(nB * sizeof(BeamRec));
+    const size_t o_mom = o_vrec + align256(nV * sizeof(VertRec));
+    const size_t o_vbeg = o_mom + align256(nB * kNumMoments * sizeof(double));
+    const size_t o_boff = o_vbeg + align256((nB + 1) * sizeof(int32_t));
+    const size_t o_w = o_boff + align256((nO + 1) * sizeof(int32_t));
+    const size_t bytes = o_w + align256(std::max<int64_t>(nO, 1) * sizeof(double));
+    if ((rc = ensure_arena(ctx, s->arena, bytes, "staged batch")))
+        return rc;
+    unsigned char *base = (unsigned char *)s->arena.base;
+    s->beams = (DevBeam *)(base + o_beams);
+    s->verts = (DevVert *)(base + o_verts);
+    s->brec = (BeamRec *)(base + o_brec);
+    s->vrec = (VertRec *)(base + o_vrec);
+    s->moments = (double *)(base + o_mom);
+    s->vbeg = (int32_t *)(base + o_vbeg);
+    s->beam_off = (int32_t *)(base + o_boff);
+    s->weight = (double *)(base + o_w);
+
     std::vector<int32_t> boff(nO + 1);
     for (int64_t o = 0; o <= nO; ++o)
         boff[o] = (int32_t)b->beam_offsets[o];
@@ -1012,12 +399,12 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     if (nO > 0)
         CK(cudaMemcpyAsync(s->weight, b->orient_weight, nO * sizeof(double), cudaMemcpyHostToDevice, st), "H2D weights");
     if (nB > 0) {
-        CK(cudaMemcpyAsync(raw + off_vo, b->vert_offsets, bytes_vo, cudaMemcpyHostToDevice, st), "H2D vert_offsets");
-        CK(cudaMemcpyAsync(raw + off_vx, b->vx, bytes_v, cudaMemcpyHostToDevice, st), "H2D vx");
-        CK(cudaMemcpyAsync(raw + off_vy, b->vy, bytes_v, cudaMemcpyHostToDevice, st), "H2D vy");
-        CK(cudaMemcpyAsync(raw + off_syx, b->slope_yx, bytes_v, cudaMemcpyHostToDevice, st), "H2D slope_yx");
-        CK(cudaMemcpyAsync(raw + off_sxy, b->slope_xy, bytes_v, cudaMemcpyHostToDevice, st), "H2D slope_xy");
-        CK(cudaMemcpyAsync(raw + off_g, b->beam_geom, bytes_g, cudaMemcpyHostToDevice, st), "H2D geom");
+        CK(cudaMemcpyAsync(raw + off_vo, b->vert_offsets, (nB + 1) * 8, cudaMemcpyHostToDevice, st), "H2D vert_offsets");
+        CK(cudaMemcpyAsync(raw + off_vx, b->vx, nV * 8, cudaMemcpyHostToDevice, st), "H2D vx");
+        CK(cudaMemcpyAsync(raw + off_vy, b->vy, nV * 8, cudaMemcpyHostToDevice, st), "H2D vy");
+        CK(cudaMemcpyAsync(raw + off_syx, b->slope_yx, nV * 8, cudaMemcpyHostToDevice, st), "H2D slope_yx");
+        CK(cudaMemcpyAsync(raw + off_sxy, b->slope_xy, nV * 8, cudaMemcpyHostToDevice, st), "H2D slope_xy");
+        CK(cudaMemcpyAsync(raw + off_g, b->beam_geom, nB * MBS_PO_GEOM_STRIDE * 8, cudaMemcpyHostToDevice, st), "H2D geom");
         CK(cudaMemcpyAsync(raw + off_ef, b->edge_flags, nV, cudaMemcpyHostToDevice, st), "H2D edge_flags");
         CK(cudaMemcpyAsync(raw + off_bf, b->beam_flags, nB, cudaMemcpyHostToDevice, st), "H2D beam_flags");
         CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st), "memset status");
@@ -1031,9 +418,12 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
         P.eflags = raw + off_ef;
         P.geom = (const double *)(raw + off_g);
         P.bflags = raw + off_bf;
-        P.k = ctx->has_wave ? ctx->wc.k : 1.0;
+        P.wc = ctx->wc;
         P.beams = s->beams;
         P.verts = s->verts;
+        P.brec = s->brec;
+        P.vrec = s->vrec;
+        P.moments = s->moments;
         P.vbeg = s->vbeg;
         P.status = ctx->d_status;
         const int threads = 128;
@@ -1049,8 +439,6 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     s->n_orient = (int)nO;
     s->n_beams = nB;
     s->n_verts = nV;
-    s->sum_beams = nB;
-    s->sum_verts = nV;
     int mx = 0;
     for (int64_t i = 0; i < nB; ++i)
         mx = std::max<int>(mx, (int)(b->vert_offsets[i + 1] - b->vert_offsets[i]));
@@ -1059,14 +447,13 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
 }
 
 struct LaunchPlan {
-    int tile, tiles_per_row, n_chunks, orient_per_chunk;
+    int tiles_per_row, n_chunks, orient_per_chunk;
 };
 
-LaunchPlan plan_launch(int n_az, int n_t, int n_orient)
+LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ctas_per_sm)
 {
     LaunchPlan L;
-    L.tile = 128;
-    L.tiles_per_row = (n_t + L.tile - 1) / L.tile;
+    L.tiles_per_row = (n_t + dirs_per_cta - 1) / dirs_per_cta;
     const long long ctas_per_chunk = (long long)n_az * L.tiles_per_row;
     int sms = 148;
     {
@@ -1075,7 +462,7 @@ LaunchPlan plan_launch(int n_az, int n_t, int n_orient)
             && cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
             sms = v;
     }
-    const long long target = (long long)sms * 4 * 4;   // ~4 waves of 4 CTAs per SM
+    const long long target = (long long)sms * ctas_per_sm * 6;   // ~6 waves
     long long chunks = (target + ctas_per_chunk - 1) / ctas_per_chunk;
     chunks = std::max<long long>(1, std::min<long long>(chunks, std::max(1, n_orient)));
     chunks = std::min<long long>(chunks, 64);
@@ -1085,8 +472,45 @@ LaunchPlan plan_launch(int n_az, int n_t, int n_orient)
     return L;
 }
 
+template <typename T, int TPB, int DPT, bool NS, int MINB>
+cudaError_t launch_one(const KParams &P, dim3 grid, cudaStream_t st)
+{
+    auto kern = po_diffract_kernel<T, TPB, DPT, NS, MINB>;
+    const size_t smem = diffract_smem_bytes<T, TPB, DPT, NS>();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return e;
+    kern<<<grid, TPB, smem, st>>>(P);
+    return cudaGetLastError();
+}
+
+// No-shadow sums use the default shape of each precision.
+cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &P, dim3 grid,
+                            cudaStream_t st)
+{
+    if (precision == MBS_PO_FP64) {
+        if (ns)
+            return launch_one<double, 128, 1, true, 4>(P, grid, st);
+        switch (variant) {
+        case 1: return launch_one<double, 128, 2, false, 3>(P, grid, st);
+        case 2: return launch_one<double, 128, 1, false, 3>(P, grid, st);
+        default: return launch_one<double, 128, 1, false, 4>(P, grid, st);
+        }
+    }
+    if (ns)
+        return launch_one<float, 128, 2, true, 4>(P, grid, st);
+    switch (variant) {
+    case 1: return launch_one<float, 128, 1, false, 6>(P, grid, st);
+    case 2: return launch_one<float, 256, 1, false, 3>(P, grid, st);
+    case 3: return launch_one<float, 128, 2, false, 3>(P, grid, st);
+    case 4: return launch_one<float, 128, 1, false, 4>(P, grid, st);
+    default: return launch_one<float, 128, 2, false, 4>(P, grid, st);
+    }
+}
+
 int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double *M_dev,
-                 double *Mns_dev, cudaStream_t st, mbs_po_stats *stats)
+                 double *Mns_dev, cudaStream_t st, mbs_po_stats *stats, int variant = -1,
+                 int orient_limit = -1)
 {
     if (!ctx->has_grid || !ctx->has_wave)
         return fail(ctx, MBS_PO_ESTATE, "grid and wave constants must be set first");
@@ -1103,8 +527,15 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     }
     if (s->n_orient == 0 || s->n_beams == 0 || G == 0)
         return MBS_PO_OK;
-    const LaunchPlan L = plan_launch(nAz, nT, s->n_orient);
     const bool ns = Mns_dev != nullptr;
+    const int pi = precision == MBS_PO_FP64 ? 0 : 1;
+    if (variant < 0)
+        variant = ctx->variant[pi];
+    if (ns)
+        variant = 0;
+    const Variant V = pi == 0 ? kVariantsF64[variant] : kVariantsF32[variant];
+    const int n_orient = orient_limit > 0 ? std::min(orient_limit, s->n_orient) : s->n_orient;
+    const LaunchPlan L = plan_launch(nAz, nT, n_orient, V.tpb * V.dpt, V.minb);
     const size_t plane = (size_t)16 * G;
     int rc;
     if ((rc = ensure(ctx, ctx->partial, ctx->partial_cap, plane * L.n_chunks * (ns ? 2 : 1), "partials")))
@@ -1112,6 +543,9 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     KParams P;
     P.beams = s->beams;
     P.verts = s->verts;
+    P.brec = s->brec;
+    P.vrec = s->vrec;
+    P.moments = s->moments;
     P.vbeg = s->vbeg;
     P.beam_off = s->beam_off;
     P.weight = s->weight;
@@ -1120,39 +554,46 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     P.sphi = ctx->grid.sphi;
     P.cphi = ctx->grid.cphi;
     P.vf = ctx->grid.vf;
+    P.row_kind = ctx->grid.row_kind;
     P.n_az = nAz;
     P.n_t = nT;
-    P.n_orient = s->n_orient;
+    P.n_orient = n_orient;
     P.orient_per_chunk = L.orient_per_chunk;
-    P.tile = L.tile;
     P.tiles_per_row = L.tiles_per_row;
     P.wc = ctx->wc;
     P.partial = ctx->partial;
     P.partial_ns = ns ? ctx->partial + plane * L.n_chunks : nullptr;
-    const size_t smem = kStageBeams * sizeof(SBeam) + kStageVerts * sizeof(SVert);
     dim3 grid((unsigned)(nAz * L.tiles_per_row), (unsigned)L.n_chunks);
-    auto launch = [&](auto kern) -> cudaError_t {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        kern<<<grid, L.tile, smem, st>>>(P);
-        return cudaGetLastError();
-    };
+    int launches = 0;
     CK(cudaEventRecord(ctx->ev[0], st), "event");
-    cudaError_t e;
-    if (precision == MBS_PO_FP64)
-        e = ns ? launch(po_diffract_kernel<MBS_PO_FP64, true>) : launch(po_diffract_kernel<MBS_PO_FP64, false>);
-    else
-        e = ns ? launch(po_diffract_kernel<MBS_PO_FP32C, true>) : launch(po_diffract_kernel<MBS_PO_FP32C, false>);
+    // polar rows on the side stream, concurrently with the main kernel
+    if (ctx->grid.n_pole > 0) {
+        CK(cudaStreamWaitEvent(ctx->side, ctx->ev[0], 0), "side wait");
+        dim3 pg((unsigned)L.n_chunks, (unsigned)ctx->grid.n_pole);
+        if (ns)
+            po_pole_kernel<true><<<pg, 256, 0, ctx->side>>>(P, ctx->grid.pole_rows);
+        else
+            po_pole_kernel<false><<<pg, 256, 0, ctx->side>>>(P, ctx->grid.pole_rows);
+        CK(cudaGetLastError(), "pole kernel launch");
+        CK(cudaEventRecord(ctx->ev[6], ctx->side), "event");
+        ++launches;
+    }
+    const cudaError_t e = launch_diffract(precision, variant, ns, P, grid, st);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "diffraction kernel launch");
+    ++launches;
+    if (ctx->grid.n_pole > 0)
+        CK(cudaStreamWaitEvent(st, ctx->ev[6], 0), "join side stream");
     CK(cudaEventRecord(ctx->ev[1], st), "event");
     const int rb = 256;
     const int rg = (int)((G * 16 + rb - 1) / rb);
     po_reduce_kernel<<<rg, rb, 0, st>>>(ctx->partial, L.n_chunks, G, M_dev);
     CK(cudaGetLastError(), "reduce launch");
+    ++launches;
     if (ns) {
         po_reduce_kernel<<<rg, rb, 0, st>>>(P.partial_ns, L.n_chunks, G, Mns_dev);
         CK(cudaGetLastError(), "reduce launch");
+        ++launches;
     }
     CK(cudaEventRecord(ctx->ev[2], st), "event");
     if (stats) {
@@ -1162,13 +603,63 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
         cudaEventElapsedTime(&b2, ctx->ev[1], ctx->ev[2]);
         stats->kernel_ms = a;
         stats->reduce_ms = b2;
-        stats->launches = 1 + (ns ? 2 : 1);
+        stats->launches = launches;
         stats->n_chunks = L.n_chunks;
     }
     return MBS_PO_OK;
 }
 
 }  // namespace
+
+extern "C" int mbs_po_autotune(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision,
+                               int max_orient, int *best, double *ms_out, int ms_len)
+{
+    if (!ctx || !s || (precision != MBS_PO_FP64 && precision != MBS_PO_FP32C))
+        return fail(ctx, MBS_PO_EINVAL, "bad arguments");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const int pi = precision == MBS_PO_FP64 ? 0 : 1;
+    const int nv = pi == 0 ? kNumVariantsF64 : kNumVariantsF32;
+    const int64_t G = (int64_t)ctx->grid.n_az * (ctx->grid.n_zen + 1);
+    double *acc = nullptr;
+    CK(cudaMalloc((void **)&acc, G * 16 * sizeof(double)), "cudaMalloc autotune");
+    int bestv = 0;
+    double bestms = 1e300;
+    for (int v = 0; v < nv; ++v) {
+        mbs_po_stats st;
+        double ms = 0.0;
+        for (int rep = 0; rep < 2; ++rep) {   // first run warms up
+            const int rc = run_diffract(ctx, s, precision, acc, nullptr, ctx->stream, &st, v, max_orient);
+            if (rc) {
+                cudaFree(acc);
+                return rc;
+            }
+            ms = st.kernel_ms;
+        }
+        if (ms_out && v < ms_len)
+            ms_out[v] = ms;
+        if (ms < bestms) {
+            bestms = ms;
+            bestv = v;
+        }
+    }
+    cudaFree(acc);
+    ctx->variant[pi] = bestv;
+    if (best)
+        *best = bestv;
+    return MBS_PO_OK;
+}
+
+extern "C" int mbs_po_set_variant(mbs_po_ctx *ctx, int precision, int variant)
+{
+    if (!ctx || (precision != MBS_PO_FP64 && precision != MBS_PO_FP32C))
+        return fail(ctx, MBS_PO_EINVAL, "bad arguments");
+    const int pi = precision == MBS_PO_FP64 ? 0 : 1;
+    const int nv = pi == 0 ? kNumVariantsF64 : kNumVariantsF32;
+    if (variant < 0 || variant >= nv)
+        return fail(ctx, MBS_PO_ERANGE, "no such launch variant");
+    ctx->variant[pi] = variant;
+    return MBS_PO_OK;
+}
 
 extern "C" int mbs_po_stage(mbs_po_ctx *ctx, const mbs_po_beams *beams, mbs_po_staged **out)
 {
@@ -1247,9 +738,11 @@ extern "C" int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int p
         return rc;
     CK(cudaEventRecord(ctx->ev[5], st), "event");
     CK(cudaMemcpyAsync(ctx->hres, ctx->macc, n * (ns ? 2 : 1) * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+    CK(cudaEventRecord(ctx->ev[7], st), "event");
     CK(cudaStreamSynchronize(st), "sync");
-    float h2d = 0.f;
+    float h2d = 0.f, d2h = 0.f;
     cudaEventElapsedTime(&h2d, ctx->ev[3], ctx->ev[4]);
+    cudaEventElapsedTime(&d2h, ctx->ev[5], ctx->ev[7]);
     for (size_t i = 0; i < n; ++i)
         M_accum[i] += ctx->hres[i];
     if (ns)
@@ -1257,7 +750,8 @@ extern "C" int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int p
             Mns_accum[i] += ctx->hres[n + i];
     if (stats) {
         stats->h2d_ms = h2d;
-        stats->d2h_ms = 0.0;
+        stats->d2h_ms = d2h;
+        stats->launches += 1;   // pack kernel
     }
     return MBS_PO_OK;
 }
@@ -1310,12 +804,13 @@ extern "C" int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams, i
     double budget = freeB * mem_fraction - fixed;
     int count = 0;
     const int end = std::min(beams->n_orient, start + std::max(0, max_count));
+    const double per_beam = sizeof(DevBeam) + sizeof(BeamRec) + kNumMoments * 8 + 4
+                          + MBS_PO_GEOM_STRIDE * 8 + 8 + 1;
+    const double per_vert = sizeof(DevVert) + sizeof(VertRec) + 4 * 8 + 1;
     for (int o = start; o < end; ++o) {
         const int64_t b0 = beams->beam_offsets[o], b1 = beams->beam_offsets[o + 1];
         const int64_t nv = b1 > b0 ? beams->vert_offsets[b1] - beams->vert_offsets[b0] : 0;
-        // device records + raw upload copies
-        const double need = (double)(b1 - b0) * (sizeof(DevBeam) + MBS_PO_GEOM_STRIDE * 8 + 8 + 1 + 4)
-                          + (double)nv * (sizeof(DevVert) + 4 * 8 + 1) + 16;
+        const double need = (double)(b1 - b0) * per_beam + (double)nv * per_vert + 16;
         if (need > budget && count > 0)
             break;
         budget -= need;
@@ -1324,33 +819,6 @@ extern "C" int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams, i
     *count_out = std::max(count, end > start ? 1 : 0);
     return MBS_PO_OK;
 }
-
-// ------------------------------------------------------------ peak probe --
-// Independent FFMA chains: measures this device's FP32 FMA throughput, the
-// denominator of the diffraction kernel's roofline fraction.
-namespace {
-__global__ void __launch_bounds__(256) po_fp32_probe_kernel(float *out, int iters, float a, float b)
-{
-    float x[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-        x[i] = threadIdx.x * 1e-3f + i;
-    for (int it = 0; it < iters; ++it) {
-#pragma unroll
-        for (int r = 0; r < 16; ++r) {
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                x[i] = fmaf(x[i], a, b);
-        }
-    }
-    float s = 0.f;
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-        s += x[i];
-    if (s == 1234.5f)
-        out[blockIdx.x] = s;
-}
-}  // namespace
 
 extern "C" int mbs_po_probe_fp32_peak(mbs_po_ctx *ctx, double *tflops)
 {

@@ -7,6 +7,11 @@
 //   Jones rotation      GpuDiffraction.cu:816-856 (no 0.5: the Mueller weight
 //                       carries 0.25, GpuDiffraction.cu:2319-2329)
 //   Jones -> Mueller    GpuDiffraction.cu:1645-1739, src/math/Mueller.hpp:37-87
+//
+// Phases are carried in turns (radians / 2 pi) in FP64.  Range reduction is
+// exact in FP64: adding 1.5*2^52 to 4u rounds it to the nearest integer n
+// (quadrant n mod 4) and u - n/4 is exact (Sterbenz), so the reduced
+// argument's only error is the FP64 rounding of the phase itself.
 #pragma once
 
 #include <cstdint>
@@ -18,6 +23,8 @@ constexpr int kMaxNv = 31;              // BeamEdgeData::MAX_EDGES - 1 (Handler.
 constexpr double kSmallPhase = 1e-3;    // HandlerPO_fast.h:170
 constexpr double kTwoPi = 6.283185307179586476925286766559;
 constexpr double kInvTwoPi = 0.15915494309189533576888376337251;
+constexpr double kMagic52 = 6755399441055744.0;   // 1.5 * 2^52
+constexpr double kMagic29 = 805306368.0;          // 1.5 * 2^29 (ulp 2^-23)
 
 // Device copy of one prepared beam (PreparedBeam, HandlerPO.h:14-47), in a
 // fixed 288-byte record.  Built by the pack kernel from mbs_po_beams.
@@ -30,11 +37,11 @@ struct __align__(16) DevBeam {
     double rot[12];      // NT, NP, nxDT, nxDP
     double jp[8];        // J_phased
     double opath;        // origBeam.opticalPath (extinction phase reference)
-    double sp_thr2;      // small-phase prefilter on A^2+B^2 (see pack kernel)
+    double sp_thr2;      // small-phase prefilter on A^2+B^2 (pack kernel)
     int32_t vbeg;        // first vertex
     int32_t nv;
     int32_t flags;       // MBS_PO_BEAM_EXTERNAL
-    int32_t pad;
+    float   near2;       // FP32 near-forward zone on A^2+B^2 (pack kernel)
 };
 static_assert(sizeof(DevBeam) == 288, "DevBeam layout");
 
@@ -59,9 +66,62 @@ struct WaveConst {
 
 // ---------------------------------------------------------------- FP64 math
 
-__device__ __forceinline__ void sincos_fp64(double x, double *s, double *c)
+// sin and cos of 2*pi*u.  Exact quadrant reduction (see file header), then
+// Taylor polynomials of sin (to x^17) and cos (to x^16) on |x| <= pi/4,
+// whose truncation error is below 1e-17.  Coefficients are 1/n! rounded to
+// double.
+__device__ __forceinline__ void sincos_turns(double u, double &s, double &c)
 {
-    sincos(x, s, c);
+    const double t = fma(u, 4.0, kMagic52);
+    const double n = t - kMagic52;
+    const int q = __double2loint(t) & 3;
+    const double x = fma(n, -0.25, u) * kTwoPi;
+    const double x2 = x * x;
+    double ps = 2.8114572543455206e-15;          // 1/17!
+    ps = fma(ps, x2, -7.6471637318198164e-13);   // -1/15!
+    ps = fma(ps, x2, 1.6059043836821613e-10);    // 1/13!
+    ps = fma(ps, x2, -2.5052108385441720e-08);   // -1/11!
+    ps = fma(ps, x2, 2.7557319223985893e-06);    // 1/9!
+    ps = fma(ps, x2, -1.9841269841269841e-04);   // -1/7!
+    ps = fma(ps, x2, 8.3333333333333333e-03);    // 1/5!
+    ps = fma(ps, x2, -1.6666666666666666e-01);   // -1/3!
+    const double sx = fma(x * x2, ps, x);
+    double pc = 4.7794773323873853e-14;          // 1/16!
+    pc = fma(pc, x2, -1.1470745597729725e-11);   // -1/14!
+    pc = fma(pc, x2, 2.0876756987868099e-09);    // 1/12!
+    pc = fma(pc, x2, -2.7557319223985888e-07);   // -1/10!
+    pc = fma(pc, x2, 2.4801587301587302e-05);    // 1/8!
+    pc = fma(pc, x2, -1.3888888888888889e-03);   // -1/6!
+    pc = fma(pc, x2, 4.1666666666666664e-02);    // 1/4!
+    pc = fma(pc, x2, -0.5);                      // -1/2!
+    const double cx = fma(x2, pc, 1.0);
+    const double ss = (q & 1) ? cx : sx;
+    const double cc = (q & 1) ? sx : cx;
+    s = (q & 2) ? -ss : ss;
+    c = ((q + 1) & 2) ? -cc : cc;
+}
+
+__device__ __forceinline__ void sincos_rad(double x, double &s, double &c)
+{
+    sincos_turns(x * kInvTwoPi, s, c);
+}
+
+// Reciprocal: hardware approximation refined by one Newton step.
+__device__ __forceinline__ double rcp64(double x)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    const double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    const double e2 = fma(-x, r, 1.0);
+    return fma(r, e2, r);
+}
+
+__device__ __forceinline__ float rcp32(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 }
 
 // HandlerPO_fast.h:228-237 / GpuDiffraction.cu:940-949.
@@ -71,7 +131,9 @@ __device__ __forceinline__ double stable_sinc(double x)
         const double x2 = x * x;
         return 1.0 - x2 / 6.0 + x2 * x2 / 120.0;
     }
-    return sin(x) / x;
+    double s, c;
+    sincos_rad(x, s, c);
+    return s / x;
 }
 
 // exp(i*phaseStart)*(exp(i*k*c*delta)-1)/c in half-angle form for a nearly
@@ -91,23 +153,22 @@ __device__ __forceinline__ void stable_edge(double pr, double pi, double delta,
 // Second-order polygon-moment factor for a small phase span
 // (HandlerPO_fast.h:161-226, GpuDiffraction.cu:876-938).  Returns false when
 // some vertex phase exceeds 1e-3.
-__device__ __forceinline__ bool small_phase_factor(const double *vx, const double *vy,
-                                                   int stride, int nv, double A, double B,
+__device__ __forceinline__ bool small_phase_factor(const DevVert *v, int nv, double A, double B,
                                                    double k, double &fr, double &fi)
 {
     if (nv < 3)
         return false;
     const double qx = k * A, qy = k * B;
     for (int i = 0; i < nv; ++i)
-        if (fabs(qx * vx[i * stride] + qy * vy[i * stride]) > kSmallPhase)
+        if (fabs(qx * v[i].x + qy * v[i].y) > kSmallPhase)
             return false;
     double twiceArea = 0, fx6 = 0, fy6 = 0, sx12 = 0, sy12 = 0, sxy24 = 0;
     double minX = 1.7976931348623157e308, maxX = -1.7976931348623157e308;
     double minY = minX, maxY = maxX;
     for (int i = 0; i < nv; ++i) {
         const int j = (i + 1 < nv) ? i + 1 : 0;
-        const double xi = vx[i * stride], yi = vy[i * stride];
-        const double xj = vx[j * stride], yj = vy[j * stride];
+        const double xi = v[i].x, yi = v[i].y;
+        const double xj = v[j].x, yj = v[j].y;
         const double cross = xi * yj - xj * yi;
         twiceArea += cross;
         fx6 += (xi + xj) * cross;
@@ -135,9 +196,54 @@ __device__ __forceinline__ bool small_phase_factor(const double *vx, const doubl
     return true;
 }
 
+// ---------------------------------------------------------------- FP32 math
+
+// sin and cos of 2*pi*u, u in turns (FP64).  The FP64 add of 1.5*2^29 to
+// 4u + 1/2 leaves round(4u) mod 4 in mantissa bits 23-24 and the remaining
+// quarter-turn fraction in bits 0-22, so the reduced argument is exact to
+// 2^-23 quarter turns without an FP64->FP32 conversion.
+__device__ __forceinline__ void reduce_quarter(double u, float &x, int &q)
+{
+    const double t = fma(u, 4.0, kMagic29 + 0.5);
+    const unsigned lo = (unsigned)__double2loint(t);
+    q = (int)((lo >> 23) & 3u);
+    x = (__int_as_float(0x3F800000u | (lo & 0x007FFFFFu)) - 1.5f) * 1.57079632679489662f;
+}
+
+// Hardware (MUFU) sine/cosine of the reduced argument |x| <= pi/4.
+__device__ __forceinline__ void sincos_quarter_mufu(float x, int q, float &s, float &c)
+{
+    float sx, cx;
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(sx) : "f"(x));
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(cx) : "f"(x));
+    const float ss = (q & 1) ? cx : sx;
+    const float cc = (q & 1) ? sx : cx;
+    s = (q & 2) ? -ss : ss;
+    c = ((q + 1) & 2) ? -cc : cc;
+}
+
+// FMA-pipe sine/cosine of |x| <= pi/4: Taylor to x^9 (error < 2e-9) and
+// x^8 (error < 3e-8), coefficients 1/n! rounded to float.
+__device__ __forceinline__ void sincos_quarter_poly(float x, int q, float &s, float &c)
+{
+    const float x2 = x * x;
+    float ps = fmaf(x2, 2.7557319e-06f, -1.9841270e-04f);
+    ps = fmaf(ps, x2, 8.3333333e-03f);
+    ps = fmaf(ps, x2, -1.6666667e-01f);
+    const float sx = fmaf(x * x2, ps, x);
+    float pc = fmaf(x2, 2.4801587e-05f, -1.3888889e-03f);
+    pc = fmaf(pc, x2, 4.1666668e-02f);
+    pc = fmaf(pc, x2, -0.5f);
+    const float cx = fmaf(x2, pc, 1.0f);
+    const float ss = (q & 1) ? cx : sx;
+    const float cc = (q & 1) ? sx : cx;
+    s = (q & 2) ? -ss : ss;
+    c = ((q + 1) & 2) ? -cc : cc;
+}
+
 // Jones -> Mueller times weight, added into out[16] (Mueller.hpp:37-87).
 template <typename T>
-__device__ __forceinline__ void mueller_add(const T *j, T weight, T *out)
+__device__ __forceinline__ void mueller_add(const T *j, T weight, T *out, int stride = 1)
 {
     const T j00r = j[0], j00i = j[1], j01r = j[2], j01i = j[3];
     const T j10r = j[4], j10i = j[5], j11r = j[6], j11i = j[7];
@@ -145,29 +251,29 @@ __device__ __forceinline__ void mueller_add(const T *j, T weight, T *out)
     const T a21 = j10r * j10r + j10i * j10i, a22 = j11r * j11r + j11i * j11i;
     const T half = T(0.5);
     T A1 = a11 + a21, A2 = a12 + a22;
-    out[0] += ((A1 + A2) * half) * weight;
-    out[1] += ((A1 - A2) * half) * weight;
+    out[0 * stride] += ((A1 + A2) * half) * weight;
+    out[1 * stride] += ((A1 - A2) * half) * weight;
     A1 = a11 - a21; A2 = a12 - a22;
-    out[4] += ((A1 + A2) * half) * weight;
-    out[5] += ((A1 - A2) * half) * weight;
+    out[4 * stride] += ((A1 + A2) * half) * weight;
+    out[5 * stride] += ((A1 - A2) * half) * weight;
     T c1r = j00r * j01r + j00i * j01i, c1i = j00i * j01r - j00r * j01i;
     T c2r = j11r * j10r + j11i * j10i, c2i = j11i * j10r - j11r * j10i;
-    out[2] += (-c1r - c2r) * weight;
-    out[3] += (c2i - c1i) * weight;
-    out[6] += (c2r - c1r) * weight;
-    out[7] += (-c1i - c2i) * weight;
+    out[2 * stride] += (-c1r - c2r) * weight;
+    out[3 * stride] += (c2i - c1i) * weight;
+    out[6 * stride] += (c2r - c1r) * weight;
+    out[7 * stride] += (-c1i - c2i) * weight;
     c1r = j00r * j10r + j00i * j10i; c1i = j00i * j10r - j00r * j10i;
     c2r = j11r * j01r + j11i * j01i; c2i = j11i * j01r - j11r * j01i;
-    out[8] += (-c1r - c2r) * weight;
-    out[9] += (c2r - c1r) * weight;
-    out[12] += (c1i - c2i) * weight;
-    out[13] += (c2i + c1i) * weight;
+    out[8 * stride] += (-c1r - c2r) * weight;
+    out[9 * stride] += (c2r - c1r) * weight;
+    out[12 * stride] += (c1i - c2i) * weight;
+    out[13 * stride] += (c2i + c1i) * weight;
     c1r = j00r * j11r + j00i * j11i; c1i = j00i * j11r - j00r * j11i;
     c2r = j01r * j10r + j01i * j10i; c2i = j01i * j10r - j01r * j10i;
-    out[10] += (c1r + c2r) * weight;
-    out[11] += (c1i - c2i) * weight;
-    out[14] += (-c1i - c2i) * weight;
-    out[15] += (c1r - c2r) * weight;
+    out[10 * stride] += (c1r + c2r) * weight;
+    out[11 * stride] += (c1i - c2i) * weight;
+    out[14 * stride] += (-c1i - c2i) * weight;
+    out[15 * stride] += (c1r - c2r) * weight;
 }
 
 }  // namespace mbs

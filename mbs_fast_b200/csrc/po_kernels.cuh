@@ -1,0 +1,1017 @@
+// po_kernels.cuh — the sm_100a kernels of the PO diffraction path.
+//
+//   po_pack_kernel       flat mbs_po_beams arrays -> device beam records
+//   po_diffract_kernel   fused aperture integral -> coherent Jones sum ->
+//                        Mueller -> orientation average (one CTA per azimuth
+//                        bin x zenith tile x orientation chunk)
+//   po_pole_kernel       the polar zenith rows, whose direction and basis are
+//                        the same for every azimuth bin
+//   po_reduce_kernel     deterministic sum of the chunk partials
+//   po_extinction_kernel optical-theorem extinction per orientation
+#pragma once
+
+#include "mbs_po_b200.h"
+#include "po_device.cuh"
+
+namespace mbs {
+
+// ------------------------------------------------------------------ records
+
+// Azimuth-independent per-beam coefficients, precomputed at staging.
+//   A(t, phi) = sin t (-(cos phi h0 + sin phi h1)) + cos t h2 + a0, B likewise.
+//   With vf = (-sin phi, cos phi, 0) off the poles, u = vt = -(cos phi cos t,
+//   sin phi cos t, sin t) and w = vt x dir = -vf, so the rotation of
+//   GpuDiffraction.cu:831-856 is R = R0 + cos t Rc + sin t Rs with
+//     R0 = sin phi X1 + cos phi X2,  Rc = -(cos phi Y1 + sin phi Y2),  Rs = Z
+//   X1 = [[NTx, NPx], [-DTx, -DPx]], X2 = [[-NTy, -NPy], [DTy, DPy]],
+//   Y1 = [[DTx, DPx], [NTx, NPx]],   Y2 = [[DTy, DPy], [NTy, NPy]],
+//   Z  = [[-DTz, -DPz], [-NTz, -NPz]]  (NT, NP, DT = nxDT, DP = nxDP).
+//   Q holds complWave * (X J_phased) for X1, X2, Y1, Y2, Z (4 complex
+//   entries each), so d = s m (P0 + cos t Pc + sin t Ps) with
+//   P0 = sin phi Q1 + cos phi Q2, Pc = -(cos phi Q3 + sin phi Q4), Ps = Q5.
+struct __align__(16) BeamRec {
+    double ab[8];     // h0 h1 h2 a0 v0 v1 v2 b0
+    double Q[40];
+    double slab[4];   // k (xa, ya) / 1.25e-3, k (xb, yb) / 1.25e-3 (see pack kernel)
+    float nearr2;     // FP32C near-forward zone: A^2+B^2 <= nearr2
+    int32_t vbeg;
+    int32_t nv;
+    int32_t pad;
+};
+
+// Per vertex, azimuth-independent parts of the phase in turns:
+//   phase(t, phi) = sin t ps + cos t pc + p0,  ps = -(cos phi X + sin phi Y)
+// (internal beams include the common beam-centre phase, GpuDiffraction.cu:1110-1122).
+// Slopes of the x and y branches; an edge invalid for a branch (|dx| or |dy|
+// below the geometry tolerance, Handler.cpp:674-692) gets the slope 1e30, so
+// its coefficient is ~1e30 |B| (or |A|) and its term ~1e-30 of the others:
+// the reference skips it.
+struct __align__(16) VertRec {
+    double X, Y, pc, p0;
+    double syx, sxy;
+};
+
+constexpr double kInvalidSlope = 1.0e30;
+constexpr int kMomentOrder = 6;      // near-forward expansion order
+constexpr int kNumMoments = 28;      // (6+1)(6+2)/2
+// Angular half-width of the FP32C near-forward zone in radians of vertex
+// phase.  Inside it every |q.r| <= kNearPhase and the edge sum cancels
+// badly in FP32; the sixth-order moment expansion there truncates at
+// kNearPhase^7/7! < 1.3e-8.
+constexpr double kNearPhase = 0.25;
+
+struct KParams {
+    const DevBeam *beams;
+    const DevVert *verts;
+    const BeamRec *brec;
+    const VertRec *vrec;
+    const double *moments;     // [n_beams][kNumMoments] c_pq = <x^p y^q>/(p! q!)
+    const int32_t *vbeg;       // [n_beams+1]
+    const int32_t *beam_off;   // [n_orient+1]
+    const double *weight;      // [n_orient]
+    const double *st, *ct, *sphi, *cphi, *vf;
+    const int8_t *row_kind;    // [n_t] 0 regular, 1 polar (po_pole_kernel), 2 general
+    int n_az, n_t;             // n_t = n_zen+1
+    int n_orient;
+    int orient_per_chunk;
+    int tiles_per_row;
+    WaveConst wc;
+    double *partial;           // [n_chunks][16][G]
+    double *partial_ns;        // [n_chunks][16][G] or null
+};
+
+// ------------------------------------------------------------ pack kernel
+
+struct PackParams {
+    int64_t n_beams;
+    const int64_t *vert_off;
+    const double *vx, *vy, *syx, *sxy;
+    const uint8_t *eflags;
+    const double *geom;
+    const uint8_t *bflags;
+    WaveConst wc;
+    DevBeam *beams;
+    DevVert *verts;
+    BeamRec *brec;
+    VertRec *vrec;
+    double *moments;
+    int32_t *vbeg;
+    int *status;   // set to 1 on a malformed beam
+};
+
+__device__ __forceinline__ double binom(int n, int k)
+{
+    double r = 1.0;
+    for (int i = 1; i <= k; ++i)
+        r = r * (n - k + i) / i;
+    return r;
+}
+
+__global__ void po_pack_kernel(PackParams P)
+{
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > P.n_beams)
+        return;
+    const int64_t v0 = P.vert_off[b];
+    P.vbeg[b] = (int32_t)v0;
+    if (b == P.n_beams)
+        return;
+    const int nv = (int)(P.vert_off[b + 1] - v0);
+    if (nv < 3 || nv > kMaxNv) {
+        atomicExch(P.status, 1);
+        return;
+    }
+    const WaveConst &wc = P.wc;
+    const double k = wc.k, kt = wc.k * kInvTwoPi;
+    const double *g = P.geom + b * MBS_PO_GEOM_STRIDE;
+    DevBeam d;
+    // a0 = bd.hor, b0 = bd.ver (GpuDiffraction.cu:301-302)
+    d.a0 = g[MBS_PO_G_BD] * g[MBS_PO_G_HOR] + g[MBS_PO_G_BD + 1] * g[MBS_PO_G_HOR + 1]
+         + g[MBS_PO_G_BD + 2] * g[MBS_PO_G_HOR + 2];
+    d.b0 = g[MBS_PO_G_BD] * g[MBS_PO_G_VER] + g[MBS_PO_G_BD + 1] * g[MBS_PO_G_VER + 1]
+         + g[MBS_PO_G_BD + 2] * g[MBS_PO_G_VER + 2];
+    for (int i = 0; i < 3; ++i) {
+        d.h[i] = g[MBS_PO_G_HOR + i];
+        d.v[i] = g[MBS_PO_G_VER + i];
+        d.c[i] = g[MBS_PO_G_CEN + i];
+    }
+    d.area = g[MBS_PO_G_AREA];
+    for (int i = 0; i < 12; ++i)
+        d.rot[i] = g[MBS_PO_G_NT + i];
+    for (int i = 0; i < 8; ++i)
+        d.jp[i] = g[MBS_PO_G_JP + i];
+    d.opath = g[MBS_PO_G_OPATH];
+    d.vbeg = (int32_t)v0;
+    d.nv = nv;
+    d.flags = P.bflags[b];
+    const bool internal = !(d.flags & MBS_PO_BEAM_EXTERNAL);
+
+    // vertices: general records, phase coefficients, second moments
+    double sxx = 0, sxy = 0, syy = 0, rmax2 = 0;
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int e = 0; e < nv; ++e) {
+        const double x = P.vx[v0 + e], y = P.vy[v0 + e];
+        sxx += x * x; sxy += x * y; syy += y * y;
+        rmax2 = fmax(rmax2, x * x + y * y);
+        const uint8_t f = P.eflags[v0 + e];
+        DevVert dv;
+        dv.x = x;
+        dv.y = y;
+        dv.syx = (f & MBS_PO_EDGE_VALID_X) ? P.syx[v0 + e] : nan;
+        dv.sxy = (f & MBS_PO_EDGE_VALID_Y) ? P.sxy[v0 + e] : nan;
+        P.verts[v0 + e] = dv;
+        VertRec vr;
+        vr.X = kt * (d.h[0] * x + d.v[0] * y) + (internal ? kt * d.c[0] : 0.0);
+        vr.Y = kt * (d.h[1] * x + d.v[1] * y) + (internal ? kt * d.c[1] : 0.0);
+        vr.pc = kt * (d.h[2] * x + d.v[2] * y) + (internal ? kt * d.c[2] : 0.0);
+        vr.p0 = kt * (d.a0 * x + d.b0 * y);
+        vr.syx = (f & MBS_PO_EDGE_VALID_X) ? P.syx[v0 + e] : kInvalidSlope;
+        vr.sxy = (f & MBS_PO_EDGE_VALID_Y) ? P.sxy[v0 + e] : kInvalidSlope;
+        P.vrec[v0 + e] = vr;
+    }
+    // Small-phase candidates.  The reference's moment branch needs every
+    // vertex phase |k(A x_v + B y_v)| <= 1e-3 (HandlerPO_fast.h:161-173); in
+    // particular for the vertex a farthest from the origin and the vertex b
+    // farthest from the line through a.  Those two slabs in (A, B), widened
+    // by 25% for rounding, bound the candidates tightly even for sliver
+    // apertures; candidates take the exact FP64 test.
+    int ia = 0;
+    for (int e = 1; e < nv; ++e) {
+        const double x = P.vx[v0 + e], y = P.vy[v0 + e];
+        if (x * x + y * y > P.vx[v0 + ia] * P.vx[v0 + ia] + P.vy[v0 + ia] * P.vy[v0 + ia])
+            ia = e;
+    }
+    const double xa = P.vx[v0 + ia], ya = P.vy[v0 + ia];
+    int ib = ia == 0 ? 1 : 0;
+    for (int e = 0; e < nv; ++e) {
+        const double x = P.vx[v0 + e], y = P.vy[v0 + e];
+        const double xb = P.vx[v0 + ib], yb = P.vy[v0 + ib];
+        if (fabs(xa * y - ya * x) > fabs(xa * yb - ya * xb))
+            ib = e;
+    }
+    const double slab_scale = k / (1.25 * kSmallPhase);
+    double slab[4] = {xa * slab_scale, ya * slab_scale,
+                      P.vx[v0 + ib] * slab_scale, P.vy[v0 + ib] * slab_scale};
+    (void)sxx; (void)sxy; (void)syy;
+    d.sp_thr2 = 0.0;
+    // FP32C near-forward zone: |q| rmax <= kNearPhase, so every vertex phase
+    // is within kNearPhase and the moment expansion converges; 0.9 keeps the
+    // zone inside that bound after the FP32 rounding of A and B.
+    const double kr2 = k * k * rmax2;
+    d.near2 = (float)((kr2 > 1e-300) ? 0.9 * kNearPhase * kNearPhase / kr2 : 0.0);
+    P.beams[b] = d;
+
+    BeamRec r;
+    r.ab[0] = d.h[0]; r.ab[1] = d.h[1]; r.ab[2] = d.h[2]; r.ab[3] = d.a0;
+    r.ab[4] = d.v[0]; r.ab[5] = d.v[1]; r.ab[6] = d.v[2]; r.ab[7] = d.b0;
+    const double *NT = d.rot, *NP = d.rot + 3, *DT = d.rot + 6, *DP = d.rot + 9;
+    const double X[5][4] = {
+        {NT[0], NP[0], -DT[0], -DP[0]},     // X1
+        {-NT[1], -NP[1], DT[1], DP[1]},     // X2
+        {DT[0], DP[0], NT[0], NP[0]},       // Y1
+        {DT[1], DP[1], NT[1], NP[1]},       // Y2
+        {-DT[2], -DP[2], -NT[2], -NP[2]}};  // Z
+    const double *j = d.jp;
+    for (int q = 0; q < 5; ++q) {
+        const double r00 = X[q][0], r01 = X[q][1], r10 = X[q][2], r11 = X[q][3];
+        double m[8];   // X J
+        m[0] = r00 * j[0] + r01 * j[4]; m[1] = r00 * j[1] + r01 * j[5];
+        m[2] = r00 * j[2] + r01 * j[6]; m[3] = r00 * j[3] + r01 * j[7];
+        m[4] = r10 * j[0] + r11 * j[4]; m[5] = r10 * j[1] + r11 * j[5];
+        m[6] = r10 * j[2] + r11 * j[6]; m[7] = r10 * j[3] + r11 * j[7];
+        for (int e = 0; e < 4; ++e) {
+            r.Q[q * 8 + 2 * e] = wc.cw_re * m[2 * e] - wc.cw_im * m[2 * e + 1];
+            r.Q[q * 8 + 2 * e + 1] = wc.cw_re * m[2 * e + 1] + wc.cw_im * m[2 * e];
+        }
+    }
+    for (int i = 0; i < 4; ++i)
+        r.slab[i] = slab[i];
+    r.nearr2 = d.near2;
+    r.vbeg = (int32_t)v0;
+    r.nv = nv;
+    r.pad = 0;
+    P.brec[b] = r;
+
+    // Polygon moments I(p,q) = integral of x^p y^q over the aperture, by
+    // Green's theorem over the edges (exact for polygons), normalised by
+    // the signed area: c_pq = <x^p y^q> / (p! q!).
+    double *mom = P.moments + b * kNumMoments;
+    double area2 = 0.0, minX = 1e300, maxX = -1e300, minY = 1e300, maxY = -1e300;
+    for (int e = 0; e < nv; ++e) {
+        const int en = (e + 1 < nv) ? e + 1 : 0;
+        area2 += P.vx[v0 + e] * P.vy[v0 + en] - P.vx[v0 + en] * P.vy[v0 + e];
+        minX = fmin(minX, P.vx[v0 + e]); maxX = fmax(maxX, P.vx[v0 + e]);
+        minY = fmin(minY, P.vy[v0 + e]); maxY = fmax(maxY, P.vy[v0 + e]);
+    }
+    const bool degenerate = fabs(area2) <= 0x1p-40 * fmax((maxX - minX) * (maxY - minY), 2.2250738585072014e-308);
+    int idx = 0;
+    double fact[kMomentOrder + 3];
+    fact[0] = 1.0;
+    for (int i = 1; i < kMomentOrder + 3; ++i)
+        fact[i] = fact[i - 1] * i;
+    for (int n = 0; n <= kMomentOrder; ++n) {
+        for (int p = n; p >= 0; --p, ++idx) {
+            const int q = n - p;
+            if (degenerate) {
+                mom[idx] = (n == 0) ? 1.0 : 0.0;
+                continue;
+            }
+            double s = 0.0;
+            for (int e = 0; e < nv; ++e) {
+                const int en = (e + 1 < nv) ? e + 1 : 0;
+                const double xi = P.vx[v0 + e], yi = P.vy[v0 + e];
+                const double xj = P.vx[v0 + en], yj = P.vy[v0 + en];
+                const double cross = xi * yj - xj * yi;
+                double t = 0.0;
+                for (int a = 0; a <= p; ++a)
+                    for (int c = 0; c <= q; ++c)
+                        t += binom(a + c, c) * binom(p + q - a - c, q - c)
+                           * pow(xi, a) * pow(xj, p - a) * pow(yi, c) * pow(yj, q - c);
+                s += cross * t;
+            }
+            const double I = s * fact[p] * fact[q] / fact[p + q + 2];
+            mom[idx] = (I / (0.5 * area2)) / (fact[p] * fact[q]);
+        }
+    }
+}
+
+// ----------------------------------------------------- general FP64 path
+// Used for the rare (beam, direction) pairs that leave the vectorised path:
+// irregular polar rows, near-singular FP32 edges and the small-phase
+// candidates of the FP64 kernel.  Everything is recomputed in FP64 from the
+// general records, as compute_beam_jones_context does
+// (GpuDiffraction.cu:1064-1165).
+
+struct DirFull {
+    double st, ct, cp, sp;
+    double dir[3], vf[3], vt[3], u[3], w[3];
+};
+
+__device__ __forceinline__ void cross3(const double *a, const double *b, double *o)
+{
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+__device__ __forceinline__ void dir_full(const KParams &P, int p, int t, DirFull &d)
+{
+    d.st = P.st[t];
+    d.ct = P.ct[t];
+    d.cp = P.cphi[p];
+    d.sp = P.sphi[p];
+    d.dir[0] = d.st * d.cp;
+    d.dir[1] = d.st * d.sp;
+    d.dir[2] = -d.ct;
+    const double *vfp = P.vf + ((size_t)p * P.n_t + t) * 3;
+    d.vf[0] = vfp[0]; d.vf[1] = vfp[1]; d.vf[2] = vfp[2];
+    cross3(d.vf, d.dir, d.u);                 // u = vf x dir
+    const double l2 = d.u[0] * d.u[0] + d.u[1] * d.u[1] + d.u[2] * d.u[2];
+    const double il = (l2 > 1e-30) ? rsqrt(l2) : 1.0;   // transverse_basis_gpu
+    d.vt[0] = d.u[0] * il; d.vt[1] = d.u[1] * il; d.vt[2] = d.u[2] * il;
+    cross3(d.vt, d.dir, d.w);                 // w = vt x dir
+}
+
+// One beam's Jones contribution d[8] to one direction in FP64.  Returns
+// false when the reference would skip the beam (NaN integral).
+__device__ __noinline__ bool beam_general(const DevBeam &g, const DevVert *gv, const DirFull &dc,
+                                          const WaveConst &wc, double *d)
+{
+    const double k = wc.k;
+    const double a_sin = -dc.cp * g.h[0] - dc.sp * g.h[1];
+    const double b_sin = -dc.cp * g.v[0] - dc.sp * g.v[1];
+    const double A = fma(dc.st, a_sin, fma(dc.ct, g.h[2], g.a0));
+    const double B = fma(dc.st, b_sin, fma(dc.ct, g.v[2], g.b0));
+    const bool internal = !(g.flags & MBS_PO_BEAM_EXTERNAL);
+    const double cm = internal ? -k * (dc.st * (dc.cp * g.c[0] + dc.sp * g.c[1]) + dc.ct * (-g.c[2])) : 0.0;
+    const DevVert *v = gv + g.vbeg;
+    const int nv = g.nv;
+    double fr, fi, pr, pi;
+    if (small_phase_factor(v, nv, A, B, k, pr, pi)) {
+        const double sgn = wc.legacy_sign ? 1.0 : -1.0;
+        const double ar = sgn * wc.icw_re * g.area, ai = sgn * wc.icw_im * g.area;
+        fr = ar * pr - ai * pi;
+        fi = ar * pi + ai * pr;
+        if (internal) {
+            double s, c;
+            sincos_rad(cm, s, c);
+            const double tr = fr * c - fi * s;
+            fi = fr * s + fi * c;
+            fr = tr;
+        }
+    } else {
+        const bool useX = fabs(B) > fabs(A);
+        const double qx = k * A * kInvTwoPi, qy = k * B * kInvTwoPi, cmt = cm * kInvTwoPi;
+        double s0, c0;
+        sincos_turns(fma(qx, v[0].x, fma(qy, v[0].y, cmt)), s0, c0);
+        double cprev = c0, sprev = s0, sr = 0.0, si = 0.0;
+        for (int e = 0; e < nv; ++e) {
+            const int en = (e + 1 < nv) ? e + 1 : 0;
+            double cn = c0, sn = s0;
+            if (en != 0)
+                sincos_turns(fma(qx, v[en].x, fma(qy, v[en].y, cmt)), sn, cn);
+            const double coef = useX ? fma(v[e].syx, B, A) : fma(v[e].sxy, A, B);
+            const double ac = fabs(coef);
+            if (ac > wc.eps1) {
+                const double inv = 1.0 / coef;
+                sr = fma(cn - cprev, inv, sr);
+                si = fma(sn - sprev, inv, si);
+            } else if (ac <= wc.eps1) {   // valid, nearly singular edge (NaN: invalid edge)
+                const double delta = useX ? (v[en].x - v[e].x) : (v[en].y - v[e].y);
+                stable_edge(cprev, sprev, delta, coef, k, sr, si);
+            }
+            cprev = cn;
+            sprev = sn;
+        }
+        const double m = useX ? 1.0 / B : -1.0 / A;
+        sr *= m;
+        si *= m;
+        fr = wc.cw_re * sr - wc.cw_im * si;
+        fi = wc.cw_re * si + wc.cw_im * sr;
+    }
+    if (isnan(fr))
+        return false;
+    // rotation (GpuDiffraction.cu:831-856) with w = vt x dir, u = vf x dir:
+    // (dir x NT).vt = NT.w and (dir x NT).vf = NT.u; the dir(dir.nxDT)
+    // terms vanish since vt and vf are orthogonal to dir.
+    const double *NT = g.rot, *NP = g.rot + 3, *DT = g.rot + 6, *DP = g.rot + 9;
+    const double r00 = NT[0] * dc.w[0] + NT[1] * dc.w[1] + NT[2] * dc.w[2] + DT[0] * dc.vt[0] + DT[1] * dc.vt[1] + DT[2] * dc.vt[2];
+    const double r01 = NP[0] * dc.w[0] + NP[1] * dc.w[1] + NP[2] * dc.w[2] + DP[0] * dc.vt[0] + DP[1] * dc.vt[1] + DP[2] * dc.vt[2];
+    const double r10 = NT[0] * dc.u[0] + NT[1] * dc.u[1] + NT[2] * dc.u[2] + DT[0] * dc.vf[0] + DT[1] * dc.vf[1] + DT[2] * dc.vf[2];
+    const double r11 = NP[0] * dc.u[0] + NP[1] * dc.u[1] + NP[2] * dc.u[2] + DP[0] * dc.vf[0] + DP[1] * dc.vf[1] + DP[2] * dc.vf[2];
+    const double *jp = g.jp;
+    const double s00r = fr * r00, s00i = fi * r00, s01r = fr * r01, s01i = fi * r01;
+    const double s10r = fr * r10, s10i = fi * r10, s11r = fr * r11, s11i = fi * r11;
+    d[0] = s00r * jp[0] - s00i * jp[1] + s01r * jp[4] - s01i * jp[5];
+    d[1] = s00r * jp[1] + s00i * jp[0] + s01r * jp[5] + s01i * jp[4];
+    d[2] = s00r * jp[2] - s00i * jp[3] + s01r * jp[6] - s01i * jp[7];
+    d[3] = s00r * jp[3] + s00i * jp[2] + s01r * jp[7] + s01i * jp[6];
+    d[4] = s10r * jp[0] - s10i * jp[1] + s11r * jp[4] - s11i * jp[5];
+    d[5] = s10r * jp[1] + s10i * jp[0] + s11r * jp[5] + s11i * jp[4];
+    d[6] = s10r * jp[2] - s10i * jp[3] + s11r * jp[6] - s11i * jp[7];
+    d[7] = s10r * jp[3] + s10i * jp[2] + s11r * jp[7] + s11i * jp[6];
+    return true;
+}
+
+// FP32C near-forward zone: the aperture integral from the sixth-order
+// moment expansion in FP64,  F = areaLimit sum_pq i^(p+q) qx^p qy^q c_pq,
+// times the internal-beam common phase, returned as the edge-sum
+// equivalent s = F / complWave so the caller applies P0 + cos t Pc + sin t Ps.
+__device__ __noinline__ void near_forward_s(const DevBeam &g, const double *mom, double st, double ct,
+                                            double cp, double sp, const WaveConst &wc,
+                                            float &sr, float &si)
+{
+    const double k = wc.k;
+    const double a_sin = -cp * g.h[0] - sp * g.h[1];
+    const double b_sin = -cp * g.v[0] - sp * g.v[1];
+    const double qx = k * fma(st, a_sin, fma(ct, g.h[2], g.a0));
+    const double qy = k * fma(st, b_sin, fma(ct, g.v[2], g.b0));
+    double px[kMomentOrder + 1], py[kMomentOrder + 1];
+    px[0] = 1.0; py[0] = 1.0;
+    for (int i = 1; i <= kMomentOrder; ++i) {
+        px[i] = px[i - 1] * qx;
+        py[i] = py[i - 1] * qy;
+    }
+    double re = 0.0, im = 0.0;
+    int idx = 0;
+    for (int n = 0; n <= kMomentOrder; ++n) {
+        double s = 0.0;
+        for (int p = n; p >= 0; --p, ++idx)
+            s = fma(mom[idx], px[p] * py[n - p], s);
+        switch (n & 3) {
+        case 0: re += s; break;
+        case 1: im += s; break;
+        case 2: re -= s; break;
+        default: im -= s; break;
+        }
+    }
+    const double sgn = wc.legacy_sign ? 1.0 : -1.0;
+    const double ar = sgn * wc.icw_re * g.area, ai = sgn * wc.icw_im * g.area;
+    double fr = ar * re - ai * im, fi = ar * im + ai * re;
+    if (!(g.flags & MBS_PO_BEAM_EXTERNAL)) {
+        const double cm = -k * (st * (cp * g.c[0] + sp * g.c[1]) + ct * (-g.c[2]));
+        double s, c;
+        sincos_rad(cm, s, c);
+        const double tr = fr * c - fi * s;
+        fi = fr * s + fi * c;
+        fr = tr;
+    }
+    // s = F / complWave
+    const double n2 = wc.cw_re * wc.cw_re + wc.cw_im * wc.cw_im;
+    sr = (float)((fr * wc.cw_re + fi * wc.cw_im) / n2);
+    si = (float)((fi * wc.cw_re - fr * wc.cw_im) / n2);
+}
+
+// ----------------------------------------------- shared-memory records
+// Per (beam, azimuth of the CTA).
+
+template <typename T>
+struct __align__(16) SBeam {
+    T a[6];          // A(t) = sin t a[0] + cos t a[1] + a[2]; B likewise a[3..5]
+    T P[24];         // P0, Pc, Ps: 4 complex entries each (re, im)
+    T slab[4];       // small-phase candidate slabs
+    float nearr2;    // FP32C near-forward zone
+    int32_t gbeam;   // global beam index
+    int32_t vs;      // first vertex in the stage
+    int32_t nv;
+};
+
+template <typename T>
+struct __align__(16) SVert {
+    double ps, pc, p0;   // phase(t) = sin t ps + cos t pc + p0, in turns
+    T syx, sxy;
+};
+
+template <typename T, int TPB>
+struct StageCfg {
+    static constexpr int kBeams = TPB;
+    static constexpr int kVerts = 4 * TPB;
+    static constexpr size_t kBytes = kBeams * sizeof(SBeam<T>) + kVerts * sizeof(SVert<T>);
+};
+
+template <typename T>
+__device__ __forceinline__ void fill_beam(const BeamRec &r, double cp, double sp, int vs,
+                                          int gbeam, SBeam<T> &s)
+{
+    s.a[0] = (T)(-(cp * r.ab[0] + sp * r.ab[1])); s.a[1] = (T)r.ab[2]; s.a[2] = (T)r.ab[3];
+    s.a[3] = (T)(-(cp * r.ab[4] + sp * r.ab[5])); s.a[4] = (T)r.ab[6]; s.a[5] = (T)r.ab[7];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        s.P[e] = (T)(sp * r.Q[e] + cp * r.Q[8 + e]);
+        s.P[8 + e] = (T)(-(cp * r.Q[16 + e] + sp * r.Q[24 + e]));
+        s.P[16 + e] = (T)r.Q[32 + e];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        s.slab[i] = (T)r.slab[i];
+    s.nearr2 = r.nearr2;
+    s.gbeam = gbeam;
+    s.vs = vs;
+    s.nv = r.nv;
+}
+
+// Phasor (cos, sin) of 2 pi u.
+__device__ __forceinline__ void phasor(double u, double &s, double &c)
+{
+    sincos_turns(u, s, c);
+}
+
+// FP32: fraction f of u in [-1/2, 1/2) to 2^-23 without an FP64->FP32
+// conversion (1.5*2^29 + 1/2 added in FP64 leaves frac(u + 1/2) in the low
+// 23 mantissa bits), then the hardware sine and cosine of 2 pi f.
+__device__ __forceinline__ void phasor(double u, float &s, float &c)
+{
+    const double t = u + (kMagic29 + 0.5);
+    const unsigned lo = (unsigned)__double2loint(t);
+    const float x = (__int_as_float(0x3F800000u | (lo & 0x007FFFFFu)) - 1.5f) * 6.28318530717958647f;
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(x));
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
+}
+
+__device__ __forceinline__ double rcp_t(double x) { return rcp64(x); }
+__device__ __forceinline__ float rcp_t(float x) { return rcp32(x); }
+
+// Edge sums S_d = sum_e (P(e+1) - P(e)) / C_e of one beam for the DPT
+// directions of a thread; C_e = A + slope_yx B (x branch, |B| > |A|) or
+// A slope_xy + B.  All vertex phasors are independent, so the NV*DPT chains
+// interleave.  mn[d] receives the smallest |C_e| (nearly singular edges are
+// recomputed in FP64 by the caller).
+template <typename T, int DPT, int NV>
+__device__ __forceinline__ void edge_sums_fixed(const SVert<T> *v, const double *st, const double *ct,
+                                                const T *A, const T *B, const bool *useX,
+                                                T *sr, T *si, T *mn)
+{
+    T c[DPT][NV], s[DPT][NV];
+#pragma unroll
+    for (int e = 0; e < NV; ++e) {
+        const double ps = v[e].ps, pc = v[e].pc, p0 = v[e].p0;
+#pragma unroll
+        for (int d = 0; d < DPT; ++d)
+            phasor(fma(st[d], ps, fma(ct[d], pc, p0)), s[d][e], c[d][e]);
+    }
+#pragma unroll
+    for (int d = 0; d < DPT; ++d) {
+        mn[d] = T(1e30);
+        sr[d] = T(0);
+        si[d] = T(0);
+    }
+#pragma unroll
+    for (int e = 0; e < NV; ++e) {
+        const int en = (e + 1 < NV) ? e + 1 : 0;
+        const T syx = v[e].syx, sxy = v[e].sxy;
+#pragma unroll
+        for (int d = 0; d < DPT; ++d) {
+            const T coef = useX[d] ? fma(syx, B[d], A[d]) : fma(sxy, A[d], B[d]);
+            const T inv = rcp_t(coef);
+            mn[d] = fmin(mn[d], fabs(coef));
+            sr[d] = fma(c[d][en] - c[d][e], inv, sr[d]);
+            si[d] = fma(s[d][en] - s[d][e], inv, si[d]);
+        }
+    }
+}
+
+template <typename T, int DPT>
+__device__ __forceinline__ void edge_sums_loop(const SVert<T> *v, int nv, const double *st,
+                                               const double *ct, const T *A, const T *B,
+                                               const bool *useX, T *sr, T *si, T *mn)
+{
+    T c0[DPT], s0[DPT], cp_[DPT], sp_[DPT];
+#pragma unroll
+    for (int d = 0; d < DPT; ++d) {
+        phasor(fma(st[d], v[0].ps, fma(ct[d], v[0].pc, v[0].p0)), s0[d], c0[d]);
+        cp_[d] = c0[d];
+        sp_[d] = s0[d];
+        mn[d] = T(1e30);
+        sr[d] = T(0);
+        si[d] = T(0);
+    }
+    for (int e = 0; e < nv; ++e) {
+        const bool last = e + 1 == nv;
+        const int en = last ? 0 : e + 1;
+        const double ps = v[en].ps, pc = v[en].pc, p0 = v[en].p0;
+        const T syx = v[e].syx, sxy = v[e].sxy;
+#pragma unroll
+        for (int d = 0; d < DPT; ++d) {
+            T cn, sn;
+            if (last) {
+                cn = c0[d];
+                sn = s0[d];
+            } else {
+                phasor(fma(st[d], ps, fma(ct[d], pc, p0)), sn, cn);
+            }
+            const T coef = useX[d] ? fma(syx, B[d], A[d]) : fma(sxy, A[d], B[d]);
+            const T inv = rcp_t(coef);
+            mn[d] = fmin(mn[d], fabs(coef));
+            sr[d] = fma(cn - cp_[d], inv, sr[d]);
+            si[d] = fma(sn - sp_[d], inv, si[d]);
+            cp_[d] = cn;
+            sp_[d] = sn;
+        }
+    }
+}
+
+template <typename T, int DPT>
+__device__ __forceinline__ void edge_sums(const SVert<T> *v, int nv, const double *st,
+                                          const double *ct, const T *A, const T *B,
+                                          const bool *useX, T *sr, T *si, T *mn)
+{
+    switch (nv) {   // warp-uniform: every lane evaluates the same beam
+    case 3: edge_sums_fixed<T, DPT, 3>(v, st, ct, A, B, useX, sr, si, mn); break;
+    case 4: edge_sums_fixed<T, DPT, 4>(v, st, ct, A, B, useX, sr, si, mn); break;
+    case 5: edge_sums_fixed<T, DPT, 5>(v, st, ct, A, B, useX, sr, si, mn); break;
+    case 6: edge_sums_fixed<T, DPT, 6>(v, st, ct, A, B, useX, sr, si, mn); break;
+    default: edge_sums_loop<T, DPT>(v, nv, st, ct, A, B, useX, sr, si, mn); break;
+    }
+}
+
+// The rare pairs of one direction, in FP64: the near-forward moment
+// expansion (FP32C), or the complete general evaluation (small-phase
+// candidates, nearly singular edges, irregular polar rows).  Writes d[8];
+// returns false when the beam contributes nothing.
+template <typename T>
+__device__ __noinline__ bool beam_rare(const KParams &P, int gbeam, const SBeam<T> &b, int p, int t,
+                                       double st, double ct, double cp, double sp, bool near,
+                                       T *d)
+{
+    constexpr bool kF32 = sizeof(T) == 4;
+    if (kF32 && near) {
+        float sr, si;
+        near_forward_s(P.beams[gbeam], P.moments + (size_t)gbeam * kNumMoments, st, ct, cp, sp,
+                       P.wc, sr, si);
+        const T stT = (T)st, ctT = (T)ct;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const T rr = fma(stT, b.P[16 + 2 * e], fma(ctT, b.P[8 + 2 * e], b.P[2 * e]));
+            const T ri = fma(stT, b.P[17 + 2 * e], fma(ctT, b.P[9 + 2 * e], b.P[2 * e + 1]));
+            d[2 * e] = fma((T)sr, rr, -(T)si * ri);
+            d[2 * e + 1] = fma((T)sr, ri, (T)si * rr);
+        }
+        return true;
+    }
+    DirFull dc;
+    dir_full(P, p, t, dc);
+    double dd[8];
+    const bool ok = beam_general(P.beams[gbeam], P.verts, dc, P.wc, dd);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        d[q] = (T)dd[q];
+    return ok;
+}
+
+// Accumulators of the coherent Jones sum of one orientation.  FP32: plain
+// sums over blocks of kFlushEvery beams in registers, folded into a
+// Kahan-compensated running sum (kept in shared memory) at every block end.
+constexpr int kFlushEvery = 16;
+
+template <typename T>
+struct JonesAcc {
+    T b[8];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) b[i] = T(0);
+    }
+    __device__ __forceinline__ void add(const T *d) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) b[i] += d[i];
+    }
+};
+
+// Kahan fold of a block sum into (s, c) held in shared memory with stride.
+__device__ __forceinline__ void kahan_fold(float *b, float *s, float *c, int stride)
+{
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float si = s[i * stride], ci = c[i * stride];
+        const float y = __fsub_rn(b[i], ci);
+        const float t = __fadd_rn(si, y);
+        c[i * stride] = __fsub_rn(__fsub_rn(t, si), y);
+        s[i * stride] = t;
+        b[i] = 0.f;
+    }
+}
+
+// Fused diffraction kernel.  Grid: x = azimuth bin * zenith tiles, y =
+// orientation chunk.  Each thread owns DPT directions (zenith rows
+// t0 + d*TPB of the CTA's azimuth).  T = float selects FP32C.
+template <typename T, int TPB, int DPT, bool NS, int MINB>
+__global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
+{
+    using Cfg = StageCfg<T, TPB>;
+    constexpr int kDirs = TPB * DPT;
+    constexpr bool kF32 = sizeof(T) == 4;
+    constexpr int kSets = NS ? 2 : 1;        // full and no-shadow sums
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SBeam<T> *sb = reinterpret_cast<SBeam<T> *>(smem_raw);
+    SVert<T> *sv = reinterpret_cast<SVert<T> *>(smem_raw + Cfg::kBeams * sizeof(SBeam<T>));
+    // FP32C: Kahan running sums of the Jones matrices, [kSets][s, c][8][kDirs]
+    float *Ksm = reinterpret_cast<float *>(smem_raw + Cfg::kBytes);
+
+    const int p = blockIdx.x / P.tiles_per_row;
+    const int tile = blockIdx.x - p * P.tiles_per_row;
+    const int chunk = blockIdx.y;
+    const int o0 = chunk * P.orient_per_chunk;
+    const int o1 = min(P.n_orient, o0 + P.orient_per_chunk);
+    const double cp = P.cphi[p], sp = P.sphi[p];
+    const T eps = (T)(kF32 ? P.wc.eps1_f32 : P.wc.eps1);
+
+    int t[DPT];
+    bool active[DPT], general[DPT];
+    double st[DPT], ct[DPT];
+    T stT[DPT], ctT[DPT];
+#pragma unroll
+    for (int d = 0; d < DPT; ++d) {
+        const int tr = tile * kDirs + d * TPB + threadIdx.x;
+        t[d] = tr < P.n_t ? tr : P.n_t - 1;
+        const int kind = P.row_kind[t[d]];
+        active[d] = tr < P.n_t && kind != 1;
+        general[d] = kind == 2;
+        st[d] = P.st[t[d]];
+        ct[d] = P.ct[t[d]];
+        stT[d] = (T)st[d];
+        ctT[d] = (T)ct[d];
+    }
+    const size_t G = (size_t)P.n_az * P.n_t;
+
+    for (int o = o0; o < o1; ++o) {
+        JonesAcc<T> J[DPT], Jn[NS ? DPT : 1];
+#pragma unroll
+        for (int d = 0; d < DPT; ++d) {
+            J[d].zero();
+            if (NS) Jn[d].zero();
+        }
+        if (kF32) {
+            for (int i = threadIdx.x; i < kSets * 16 * kDirs; i += TPB)
+                Ksm[i] = 0.f;
+        }
+        const int b0 = P.beam_off[o], b1 = P.beam_off[o + 1];
+        for (int bs = b0; bs < b1;) {
+            // stage [bs, be): at most kBeams beams and kVerts vertices
+            int lo = bs + 1, hi = min(b1, bs + Cfg::kBeams);
+            const int vb0 = P.vbeg[bs];
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (P.vbeg[mid] - vb0 <= Cfg::kVerts) lo = mid; else hi = mid - 1;
+            }
+            const int be = lo;
+            const int nb = be - bs;
+            const int nvs = P.vbeg[be] - vb0;
+            __syncthreads();   // previous stage fully consumed
+            for (int i = threadIdx.x; i < nb; i += TPB) {
+                const BeamRec &r = P.brec[bs + i];
+                fill_beam<T>(r, cp, sp, r.vbeg - vb0, bs + i, sb[i]);
+            }
+            for (int i = threadIdx.x; i < nvs; i += TPB) {
+                const VertRec &r = P.vrec[vb0 + i];
+                SVert<T> w;
+                w.ps = -(cp * r.X + sp * r.Y);
+                w.pc = r.pc;
+                w.p0 = r.p0;
+                w.syx = (T)r.syx;
+                w.sxy = (T)r.sxy;
+                sv[i] = w;
+            }
+            __syncthreads();
+            for (int j = 0; j < nb; ++j) {
+                const SBeam<T> &b = sb[j];
+                T A[DPT], B[DPT], sr[DPT], si[DPT], mn[DPT];
+                bool useX[DPT], rare[DPT], near[DPT];
+#pragma unroll
+                for (int d = 0; d < DPT; ++d) {
+                    A[d] = fma(stT[d], b.a[0], fma(ctT[d], b.a[1], b.a[2]));
+                    B[d] = fma(stT[d], b.a[3], fma(ctT[d], b.a[4], b.a[5]));
+                    useX[d] = fabs(B[d]) > fabs(A[d]);
+                    near[d] = kF32 && (float)(A[d] * A[d] + B[d] * B[d]) <= b.nearr2;
+                    const bool cand = fabs(fma(A[d], b.slab[0], B[d] * b.slab[1])) <= T(1)
+                                   && fabs(fma(A[d], b.slab[2], B[d] * b.slab[3])) <= T(1);
+                    rare[d] = general[d] || near[d] || cand;
+                }
+                edge_sums<T, DPT>(sv + b.vs, b.nv, st, ct, A, B, useX, sr, si, mn);
+#pragma unroll
+                for (int d = 0; d < DPT; ++d) {
+                    if (!active[d])
+                        continue;
+                    T dj[8];
+                    bool ok;
+                    if (rare[d] || mn[d] <= eps) {
+                        ok = beam_rare<T>(P, bs + j, b, p, t[d], st[d], ct[d], cp, sp,
+                                          near[d] && !general[d], dj);
+                    } else {
+                        const T m = useX[d] ? rcp_t(B[d]) : -rcp_t(A[d]);
+                        const T s_r = sr[d] * m, s_i = si[d] * m;
+                        ok = !(s_r != s_r);
+                        // d = s x (P0 + cos t Pc + sin t Ps)
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const T rr = fma(stT[d], b.P[16 + 2 * e], fma(ctT[d], b.P[8 + 2 * e], b.P[2 * e]));
+                            const T ri = fma(stT[d], b.P[17 + 2 * e], fma(ctT[d], b.P[9 + 2 * e], b.P[2 * e + 1]));
+                            dj[2 * e] = fma(s_r, rr, -s_i * ri);
+                            dj[2 * e + 1] = fma(s_r, ri, s_i * rr);
+                        }
+                    }
+                    if (ok) {
+                        J[d].add(dj);
+                        if (NS && !(P.beams[bs + j].flags & MBS_PO_BEAM_EXTERNAL))
+                            Jn[d].add(dj);
+                    }
+                }
+                if (kF32 && ((j & (kFlushEvery - 1)) == kFlushEvery - 1 || j + 1 == nb)) {
+#pragma unroll
+                    for (int d = 0; d < DPT; ++d) {
+                        const int slot = d * TPB + threadIdx.x;
+                        kahan_fold(reinterpret_cast<float *>(J[d].b), Ksm + slot, Ksm + 8 * kDirs + slot, kDirs);
+                        if (NS)
+                            kahan_fold(reinterpret_cast<float *>(Jn[d].b), Ksm + 16 * kDirs + slot,
+                                       Ksm + 24 * kDirs + slot, kDirs);
+                    }
+                }
+            }
+            bs = be;
+        }
+        // Mueller of this orientation, weighted, added to the chunk's
+        // partial plane in global memory (coalesced: consecutive threads
+        // own consecutive directions; the first orientation initialises).
+        const double wgt = P.weight[o] * 0.25;
+#pragma unroll
+        for (int d = 0; d < DPT; ++d) {
+            if (!active[d])
+                continue;
+            const int slot = d * TPB + threadIdx.x;
+            const size_t g = (size_t)p * P.n_t + t[d];
+            for (int set = 0; set < kSets; ++set) {
+                double j[8];
+                if (kF32) {
+                    const float *s = Ksm + set * 16 * kDirs + slot;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        j[i] = (double)s[i * kDirs] - (double)s[(8 + i) * kDirs];
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        j[i] = (double)(set == 0 ? J[d].b[i] : Jn[NS ? d : 0].b[i]);
+                }
+                double m[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    m[i] = 0.0;
+                mueller_add(j, wgt, m);
+                double *out = (set == 0 ? P.partial : P.partial_ns) + (size_t)chunk * 16 * G + g;
+                if (o == o0) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        out[i * G] = m[i];
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        out[i * G] += m[i];
+                }
+            }
+        }
+    }
+}
+
+template <typename T, int TPB, int DPT, bool NS>
+constexpr size_t diffract_smem_bytes()
+{
+    return StageCfg<T, TPB>::kBytes
+         + (sizeof(T) == 4 ? (NS ? 2 : 1) * 16 * TPB * DPT * sizeof(float) : 0);
+}
+
+// Polar zenith rows (row_kind 1): every azimuth bin has the same direction
+// and polarisation basis there (Handler.h:147-160), so the row is evaluated
+// once per orientation in FP64 and written to all azimuth bins.  Grid:
+// x = orientation chunk, y = polar row index; threads stride over the
+// chunk's orientations, then a fixed-order tree sums them.
+template <bool NS>
+__global__ void __launch_bounds__(256) po_pole_kernel(KParams P, const int32_t *pole_rows)
+{
+    __shared__ double red[256];
+    const int chunk = blockIdx.x;
+    const int t = pole_rows[blockIdx.y];
+    const int o0 = chunk * P.orient_per_chunk;
+    const int o1 = min(P.n_orient, o0 + P.orient_per_chunk);
+    DirFull dc;
+    dir_full(P, 0, t, dc);
+    double M[16], Mn[NS ? 16 : 1];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) M[i] = 0.0;
+    if (NS) {
+#pragma unroll
+        for (int i = 0; i < (NS ? 16 : 1); ++i) Mn[i] = 0.0;
+    }
+    for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
+        double J[8] = {0, 0, 0, 0, 0, 0, 0, 0}, Jn[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int b = P.beam_off[o]; b < P.beam_off[o + 1]; ++b) {
+            double d[8];
+            if (beam_general(P.beams[b], P.verts, dc, P.wc, d)) {
+                for (int q = 0; q < 8; ++q) J[q] += d[q];
+                if (NS && !(P.beams[b].flags & MBS_PO_BEAM_EXTERNAL))
+                    for (int q = 0; q < 8; ++q) Jn[q] += d[q];
+            }
+        }
+        const double wgt = P.weight[o] * 0.25;
+        mueller_add(J, wgt, M);
+        if (NS)
+            mueller_add(Jn, wgt, Mn);
+    }
+    const size_t G = (size_t)P.n_az * P.n_t;
+    for (int set = 0; set < (NS ? 2 : 1); ++set) {
+        double *out = (set == 0 ? P.partial : P.partial_ns) + (size_t)chunk * 16 * G;
+        for (int i = 0; i < 16; ++i) {
+            red[threadIdx.x] = set == 0 ? M[i] : Mn[NS ? i : 0];
+            __syncthreads();
+            for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+                if ((int)threadIdx.x < s)
+                    red[threadIdx.x] += red[threadIdx.x + s];
+                __syncthreads();
+            }
+            const double v = red[0];
+            for (int pp = threadIdx.x; pp < P.n_az; pp += blockDim.x)
+                out[(size_t)i * G + (size_t)pp * P.n_t + t] = v;
+            __syncthreads();
+        }
+    }
+}
+
+// out[g*16+k] += sum_c partial[c][k][g], in chunk order (deterministic).
+__global__ void po_reduce_kernel(const double *__restrict__ partial, int n_chunks,
+                                 int64_t G, double *__restrict__ out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G * 16)
+        return;
+    const int64_t k = i / G, g = i - k * G;
+    double s = 0.0;
+    for (int c = 0; c < n_chunks; ++c)
+        s += partial[(int64_t)c * 16 * G + i];
+    out[g * 16 + k] += s;
+}
+
+// --------------------------------------------------------- extinction
+// One thread per orientation: HandlerPO::ComputeForwardExtinctionOt
+// (reference HandlerPO.cpp:1812-2009) at zenith 0, azimuth 0.
+__global__ void po_extinction_kernel(const DevBeam *beams, const DevVert *verts,
+                                     const int32_t *beam_off, const double *weight,
+                                     int n_orient, WaveConst wc, double *cext)
+{
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n_orient)
+        return;
+    const double k = wc.k;
+    DirFull dc;
+    dc.st = 0.0; dc.ct = 1.0; dc.cp = 1.0; dc.sp = 0.0;
+    dc.dir[0] = 0.0; dc.dir[1] = 0.0; dc.dir[2] = -1.0;
+    dc.vf[0] = 0.0; dc.vf[1] = 1.0; dc.vf[2] = 0.0;
+    cross3(dc.vf, dc.dir, dc.u);
+    dc.vt[0] = dc.u[0]; dc.vt[1] = dc.u[1]; dc.vt[2] = dc.u[2];
+    cross3(dc.vt, dc.dir, dc.w);
+    double f00r = 0, f00i = 0, f11r = 0, f11i = 0;
+    for (int b = beam_off[o]; b < beam_off[o + 1]; ++b) {
+        DevBeam g = beams[b];
+        const bool external = (g.flags & MBS_PO_BEAM_EXTERNAL) != 0;
+        if (wc.ot_phase_avg && !external)
+            continue;
+        // The extinction phase reference differs from the scattering one
+        // (HandlerPO.cpp:1965-1977): external beams take exp(-ik opticalPath),
+        // internal ones exp(-ik(cos t dp_cos + farReference)).  beam_general
+        // is run on a copy flagged external (no common phase), and the
+        // reference's factor is applied here.
+        const double ref = external ? g.opath : wc.ot_far_ref;
+        g.flags |= MBS_PO_BEAM_EXTERNAL;
+        // The reference drops beams whose 1/A or 1/B divisor is nearly
+        // singular at this direction (HandlerPO.cpp:1920-1921, 1945-1946).
+        const double A = g.h[2] + g.a0, B = g.v[2] + g.b0;
+        double dd[8], pr, pi;
+        const bool small = small_phase_factor(verts + g.vbeg, g.nv, A, B, k, pr, pi);
+        if (!small && ((fabs(B) > fabs(A)) ? fabs(B) <= wc.eps1 : fabs(A) <= wc.eps1))
+            continue;
+        if (!beam_general(g, verts, dc, wc, dd))
+            continue;
+        double ph = 0.0;
+        if (!external)
+            ph = -k * (1.0 * (-g.c[2]) + ref);
+        else if (ref != 0.0)
+            ph = -k * ref;
+        double s = 0.0, c = 1.0;
+        if (ph != 0.0)
+            sincos_rad(ph, s, c);
+        // the CPU rotation carries 0.5 (HandlerPO_fast.h:643-646)
+        f00r += 0.5 * (dd[0] * c - dd[1] * s); f00i += 0.5 * (dd[0] * s + dd[1] * c);
+        f11r += 0.5 * (dd[6] * c - dd[7] * s); f11i += 0.5 * (dd[6] * s + dd[7] * c);
+    }
+    const double fwr = f00r + f11r, fwi = f00i + f11i;
+    double amp = fwi;
+    if (wc.ot_ping != 0.0) {
+        double sn, cs;
+        sincos_rad(2.0 * k * wc.ot_ping, sn, cs);
+        amp = fwi * cs - fwr * sn;
+    }
+    const double cv = wc.wavelength * amp * weight[o];
+    cext[o] = isfinite(cv) ? cv : 0.0;
+}
+
+// ------------------------------------------------------------ peak probe
+// Independent FFMA chains: this device's FP32 FMA throughput, the
+// denominator of the diffraction kernels' roofline fraction.
+__global__ void __launch_bounds__(256) po_fp32_probe_kernel(float *out, int iters, float a, float b)
+{
+    float x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        x[i] = threadIdx.x * 1e-3f + i;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                x[i] = fmaf(x[i], a, b);
+        }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        s += x[i];
+    if (s == 1234.5f)
+        out[blockIdx.x] = s;
+}
+
+}  // namespace mbs

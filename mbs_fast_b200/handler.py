@@ -48,6 +48,8 @@ def lib() -> C.CDLL:
         L.mbs_po_select_batch.argtypes = [vp, C.POINTER(abi.Beams), C.c_int, C.c_int, C.c_double,
                                           C.POINTER(C.c_int)]
         L.mbs_po_probe_fp32_peak.argtypes = [vp, abi._dp]
+        L.mbs_po_autotune.argtypes = [vp, vp, C.c_int, C.c_int, C.POINTER(C.c_int), abi._dp, C.c_int]
+        L.mbs_po_set_variant.argtypes = [vp, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -147,6 +149,19 @@ class GpuHandlerPO:
         v = C.c_double()
         self._call(lib().mbs_po_probe_fp32_peak(self.ctx, C.byref(v)), "mbs_po_probe_fp32_peak")
         return v.value
+
+    def autotune(self, staged: "Staged", precision: int, max_orient: int = 256):
+        """Time every compiled launch shape on the staged batch; keep the
+        fastest.  Returns (best index, per-shape kernel ms)."""
+        best = C.c_int()
+        ms = np.zeros(16)
+        self._call(lib().mbs_po_autotune(self.ctx, staged.handle, precision, max_orient,
+                                         C.byref(best), abi.ptr(ms, C.c_double), len(ms)),
+                   "mbs_po_autotune")
+        return best.value, [m for m in ms if m > 0]
+
+    def set_variant(self, precision: int, variant: int) -> None:
+        self._call(lib().mbs_po_set_variant(self.ctx, precision, variant), "mbs_po_set_variant")
 
     # -- device-resident path -------------------------------------------------
     def stage(self, batch: BeamBatch) -> Staged:

@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 # reference reports 9.6e-10 CPU vs CUDA FP64 and gates at 1e-5,
 # tests/run_cuda_release_gate.sh:8).  FP32C: the FP32 path against the FP64
 # path on the same inputs.
-FP64_WL2 = 1e-8
+FP64_WL2 = 1e-8          # against the oracle (both evaluate sin/cos to < 1 ulp)
+FP64_REF_WL2 = 1e-7      # against the reference (its own AVX sin/cos polynomial)
 FP32C_WL2 = 2e-4
 
 
@@ -48,8 +49,8 @@ def test_fp64_matches_reference(hex_case):
     M_ref, Mns_ref, _, _ = oracle.ref_batch(cfg, (0.0, 180.0, 16, 180), batch)
     M, Mns = h.new_mueller(), h.new_mueller()
     assert h.handle_orientations_to_local_gpu(batch, M, Mns, precision=abi.FP64)
-    assert common.weighted_l2(M, M_ref, grid) < FP64_WL2
-    assert common.weighted_l2(Mns, Mns_ref, grid) < FP64_WL2
+    assert common.weighted_l2(M, M_ref, grid) < FP64_REF_WL2
+    assert common.weighted_l2(Mns, Mns_ref, grid) < FP64_REF_WL2
 
 
 def test_fp32c_against_fp64(hex_case):
