@@ -181,6 +181,32 @@ int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams,
                         int start, int max_count, double mem_fraction,
                         int *count_out);
 
+/* Allocation-free variant of mbs_po_diffract_staged (no counterpart in the
+ * reference).  For callers that cannot allocate device memory when they
+ * diffract: work recorded into a CUDA graph while a stream is captured,
+ * callers whose device memory belongs to an external pool or a fixed budget,
+ * and real-time loops that must not stall on cudaMalloc/cudaFree (both
+ * synchronise the device).  The orientation-chunk partials that
+ * mbs_po_diffract_staged keeps in context memory it allocates on demand live
+ * here in one fixed device array of MBS_PO_NOALLOC_SCRATCH_BYTES, which
+ * every GPU that loads the library holds until the process exits.
+ *   - Inputs (the staged batch, grid and wave constants of the context) and
+ *     outputs (M_accum_dev / Mns_accum_dev, device arrays of
+ *     [n_az*(n_zen+1)*16] doubles, accumulated +=) are the caller's.
+ *   - Grids whose partial plane (16 doubles per direction, twice with
+ *     Mns_accum_dev) exceeds the array are rejected with MBS_PO_ERANGE; when
+ *     the array holds fewer orientation chunks than the default plan uses,
+ *     the call runs fewer, larger chunks.
+ *   - The first call on a device resolves the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - Every call shares the array and overwrites what the last call left;
+ *     calls that overlap on the GPU (other streams, other host threads, other
+ *     contexts on the same device) race on it and must be serialised. */
+#define MBS_PO_NOALLOC_SCRATCH_BYTES (32u << 20)
+int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_staged *staged,
+                                   int precision, double *M_accum_dev,
+                                   double *Mns_accum_dev, void *stream);
+
 /* Launch-shape autotuner (project-written; no counterpart in the reference):
  * times each compiled shape of the diffraction kernel (threads per CTA,
  * directions per thread, register budget) on the first max_orient (<= 0:

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -848,5 +849,143 @@ extern "C" int mbs_po_probe_fp32_peak(mbs_po_ctx *ctx, double *tflops)
     }
     cudaFree(out);
     *tflops = best;
+    return MBS_PO_OK;
+}
+
+// ------------------------------------------------- allocation-free variant --
+// For callers that cannot allocate device memory at the time they diffract:
+// code running while a stream is being captured into a CUDA graph, callers
+// whose device memory is owned by an external pool or a fixed budget, and
+// real-time loops that must not block on cudaMalloc/cudaFree (both
+// synchronise the device).  mbs_po_diffract_staged keeps its chunk partials
+// in context memory that it allocates and grows on demand; this variant
+// keeps them in the fixed device array below instead.  The array is a
+// file-scope __device__ variable, so every GPU that loads this library holds
+// it (kNoAllocScratchBytes) until the process exits.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = MBS_PO_NOALLOC_SCRATCH_BYTES;
+constexpr size_t kNoAllocScratchDoubles = kNoAllocScratchBytes / sizeof(double);
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+// Device address of g_noalloc_scratch per device ordinal.  In host code the
+// symbol is only a host-side stand-in, never a device address: it must be
+// resolved with cudaGetSymbolAddress while that device is current.
+constexpr int kMaxDevices = 64;
+std::atomic<double *> g_noalloc_addr[kMaxDevices];
+
+int noalloc_scratch(mbs_po_ctx *ctx, double **out)
+{
+    if (ctx->device < 0 || ctx->device >= kMaxDevices)
+        return fail(ctx, MBS_PO_ERANGE, "device ordinal beyond the no-allocation table");
+    double *addr = g_noalloc_addr[ctx->device].load();
+    if (!addr) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return cuda_fail(ctx, e != cudaSuccess ? e : cudaErrorInvalidSymbol,
+                             "cudaGetSymbolAddress(no-allocation scratch)");
+        addr = static_cast<double *>(p);
+        g_noalloc_addr[ctx->device].store(addr);
+    }
+    *out = addr;
+    return MBS_PO_OK;
+}
+
+}  // namespace
+
+extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_staged *s,
+                                              int precision, double *M_dev, double *Mns_dev,
+                                              void *stream)
+{
+    if (!ctx || !s || !M_dev)
+        return fail(ctx, MBS_PO_EINVAL, "null argument");
+    if (!ctx->has_grid || !ctx->has_wave)
+        return fail(ctx, MBS_PO_ESTATE, "grid and wave constants must be set first");
+    if (precision != MBS_PO_FP64 && precision != MBS_PO_FP32C)
+        return fail(ctx, MBS_PO_EINVAL, "unknown precision");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    double *scratch = nullptr;
+    int rc = noalloc_scratch(ctx, &scratch);
+    if (rc)
+        return rc;
+    const int nAz = ctx->grid.n_az, nT = ctx->grid.n_zen + 1;
+    const int64_t G = (int64_t)nAz * nT;
+    if (s->n_orient == 0 || s->n_beams == 0 || G == 0)
+        return MBS_PO_OK;
+    const bool ns = Mns_dev != nullptr;
+    const size_t plane = (size_t)16 * G;
+    const size_t sets = ns ? 2 : 1;
+    // one partial plane per orientation chunk (and per output set) must fit
+    if (plane * sets > kNoAllocScratchDoubles)
+        return fail(ctx, MBS_PO_ERANGE,
+                    "grid of " + std::to_string(G) + " directions needs "
+                    + std::to_string(plane * sets * sizeof(double)) + " bytes of partials; the "
+                    "no-allocation scratch holds " + std::to_string(kNoAllocScratchBytes)
+                    + " bytes (use mbs_po_diffract_staged)");
+    const int pi = precision == MBS_PO_FP64 ? 0 : 1;
+    const int variant = ns ? 0 : ctx->variant[pi];
+    const Variant V = pi == 0 ? kVariantsF64[variant] : kVariantsF32[variant];
+    LaunchPlan L = plan_launch(nAz, nT, s->n_orient, V.tpb * V.dpt, V.minb);
+    // fewer, larger orientation chunks when the fixed scratch is short
+    const int max_chunks = (int)std::min<size_t>(kNoAllocScratchDoubles / (plane * sets), 64);
+    if (L.n_chunks > max_chunks) {
+        L.orient_per_chunk = (s->n_orient + max_chunks - 1) / max_chunks;
+        L.n_chunks = (s->n_orient + L.orient_per_chunk - 1) / L.orient_per_chunk;
+    }
+    // Every partial entry of chunks [0, n_chunks) is written (not added) by
+    // each call (first orientation of a chunk, polar rows), so the scratch
+    // left by an earlier call needs no clearing.
+    KParams P;
+    P.beams = s->beams;
+    P.verts = s->verts;
+    P.brec = s->brec;
+    P.vrec = s->vrec;
+    P.moments = s->moments;
+    P.vbeg = s->vbeg;
+    P.beam_off = s->beam_off;
+    P.weight = s->weight;
+    P.st = ctx->grid.st;
+    P.ct = ctx->grid.ct;
+    P.sphi = ctx->grid.sphi;
+    P.cphi = ctx->grid.cphi;
+    P.vf = ctx->grid.vf;
+    P.row_kind = ctx->grid.row_kind;
+    P.n_az = nAz;
+    P.n_t = nT;
+    P.n_orient = s->n_orient;
+    P.orient_per_chunk = L.orient_per_chunk;
+    P.tiles_per_row = L.tiles_per_row;
+    P.wc = ctx->wc;
+    P.partial = scratch;
+    P.partial_ns = ns ? scratch + plane * L.n_chunks : nullptr;
+    cudaStream_t st = (cudaStream_t)stream;
+    dim3 grid((unsigned)(nAz * L.tiles_per_row), (unsigned)L.n_chunks);
+    if (ctx->grid.n_pole > 0) {
+        CK(cudaEventRecord(ctx->ev[0], st), "event");
+        CK(cudaStreamWaitEvent(ctx->side, ctx->ev[0], 0), "side wait");
+        dim3 pg((unsigned)L.n_chunks, (unsigned)ctx->grid.n_pole);
+        if (ns)
+            po_pole_kernel<true><<<pg, 256, 0, ctx->side>>>(P, ctx->grid.pole_rows);
+        else
+            po_pole_kernel<false><<<pg, 256, 0, ctx->side>>>(P, ctx->grid.pole_rows);
+        CK(cudaGetLastError(), "pole kernel launch");
+        CK(cudaEventRecord(ctx->ev[6], ctx->side), "event");
+    }
+    const cudaError_t e = launch_diffract(precision, variant, ns, P, grid, st);
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "diffraction kernel launch");
+    if (ctx->grid.n_pole > 0)
+        CK(cudaStreamWaitEvent(st, ctx->ev[6], 0), "join side stream");
+    const int rb = 256;
+    const int rg = (int)((G * 16 + rb - 1) / rb);
+    po_reduce_kernel<<<rg, rb, 0, st>>>(P.partial, L.n_chunks, G, M_dev);
+    CK(cudaGetLastError(), "reduce launch");
+    if (ns) {
+        po_reduce_kernel<<<rg, rb, 0, st>>>(P.partial_ns, L.n_chunks, G, Mns_dev);
+        CK(cudaGetLastError(), "reduce launch");
+    }
     return MBS_PO_OK;
 }

@@ -50,6 +50,8 @@ def lib() -> C.CDLL:
         L.mbs_po_probe_fp32_peak.argtypes = [vp, abi._dp]
         L.mbs_po_autotune.argtypes = [vp, vp, C.c_int, C.c_int, C.POINTER(C.c_int), abi._dp, C.c_int]
         L.mbs_po_set_variant.argtypes = [vp, C.c_int, C.c_int]
+        L.mbs_po_diffract_staged_noalloc.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_void_p,
+                                                     C.c_void_p]
         _lib = L
     return _lib
 
@@ -149,6 +151,17 @@ class GpuHandlerPO:
         v = C.c_double()
         self._call(lib().mbs_po_probe_fp32_peak(self.ctx, C.byref(v)), "mbs_po_probe_fp32_peak")
         return v.value
+
+    def diffract_staged_noalloc(self, staged: Staged, m_dev_ptr: int,
+                                mns_dev_ptr: int | None = None, precision: int = abi.FP64,
+                                stream: int = 0) -> None:
+        """mbs_po_diffract_staged_noalloc: the same accumulation with the
+        chunk partials in the library's fixed device array (no allocation).
+        Calls sharing the array must not overlap on the GPU."""
+        self._call(lib().mbs_po_diffract_staged_noalloc(
+            self.ctx, staged.handle, precision, C.c_void_p(m_dev_ptr),
+            C.c_void_p(mns_dev_ptr) if mns_dev_ptr else None, C.c_void_p(stream)),
+            "mbs_po_diffract_staged_noalloc")
 
     def autotune(self, staged: "Staged", precision: int, max_orient: int = 256):
         """Time every compiled launch shape on the staged batch; keep the
