@@ -45,7 +45,8 @@ struct GridDev {
 struct Variant {
     int tpb, dpt, minb;
 };
-constexpr Variant kVariantsF32[] = {{128, 2, 4}, {128, 1, 6}, {256, 1, 3}, {128, 2, 3}, {128, 1, 4}};
+constexpr Variant kVariantsF32[] = {{128, 2, 4}, {96, 2, 5}, {96, 1, 8}, {128, 2, 3},
+                                    {128, 1, 4}, {128, 4, 2}, {64, 4, 4}, {96, 4, 2}};
 constexpr Variant kVariantsF64[] = {{128, 1, 4}, {128, 2, 3}, {128, 1, 3}};
 constexpr int kNumVariantsF32 = sizeof(kVariantsF32) / sizeof(Variant);
 constexpr int kNumVariantsF64 = sizeof(kVariantsF64) / sizeof(Variant);
@@ -501,10 +502,13 @@ cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &
     if (ns)
         return launch_one<float, 128, 2, true, 4>(P, grid, st);
     switch (variant) {
-    case 1: return launch_one<float, 128, 1, false, 6>(P, grid, st);
-    case 2: return launch_one<float, 256, 1, false, 3>(P, grid, st);
+    case 1: return launch_one<float, 96, 2, false, 5>(P, grid, st);
+    case 2: return launch_one<float, 96, 1, false, 8>(P, grid, st);
     case 3: return launch_one<float, 128, 2, false, 3>(P, grid, st);
     case 4: return launch_one<float, 128, 1, false, 4>(P, grid, st);
+    case 5: return launch_one<float, 128, 4, false, 2>(P, grid, st);
+    case 6: return launch_one<float, 64, 4, false, 4>(P, grid, st);
+    case 7: return launch_one<float, 96, 4, false, 2>(P, grid, st);
     default: return launch_one<float, 128, 2, false, 4>(P, grid, st);
     }
 }

@@ -443,51 +443,186 @@ __device__ __noinline__ void near_forward_s(const DevBeam &g, const double *mom,
 }
 
 // ----------------------------------------------- shared-memory records
-// Per (beam, azimuth of the CTA).
+// Per (beam, azimuth of the CTA), laid out for 16-byte vector loads: every
+// lane of a warp reads the same record (a broadcast), so a beam costs ten
+// (FP32C) or eighteen (FP64) shared loads per thread for all DPT directions.
+//   A(t) = sin t a[0] + cos t a[1] + a[2],  B(t) = sin t a[3] + cos t a[4] + a[5]
+//   P0, Pc, Ps: complWave (R J) parts, 4 complex entries each (see BeamRec)
+//   slab: small-phase candidate test, nearr2: FP32C near-forward zone
 
 template <typename T>
-struct __align__(16) SBeam {
-    T a[6];          // A(t) = sin t a[0] + cos t a[1] + a[2]; B likewise a[3..5]
-    T P[24];         // P0, Pc, Ps: 4 complex entries each (re, im)
-    T slab[4];       // small-phase candidate slabs
-    float nearr2;    // FP32C near-forward zone
-    int32_t gbeam;   // global beam index
-    int32_t vs;      // first vertex in the stage
-    int32_t nv;
+struct BeamRegs {
+    T a[6];
+    T slab[4];
+    float nearr2;
+    int nv, vs, gbeam;
 };
 
 template <typename T>
-struct __align__(16) SVert {
-    double ps, pc, p0;   // phase(t) = sin t ps + cos t pc + p0, in turns
-    T syx, sxy;
+struct SBeamRaw;
+
+template <>
+struct __align__(16) SBeamRaw<float> {
+    float4 q[10];   // a0-3 | a4 a5 slab0 slab1 | slab2 slab3 nearr2 nv | P[24] | gbeam vs
+};
+
+template <>
+struct __align__(16) SBeamRaw<double> {
+    double2 q[18];  // a0a1 a2a3 a4a5 | slab | slab | P[24] | (nearr2,nv) (gbeam,vs)
+};
+
+template <typename T>
+struct SVertRaw;
+
+template <>
+struct __align__(16) SVertRaw<float> {
+    double2 q[2];   // (ps, pc) (p0, slopes syx|sxy as two floats)
+};
+
+template <>
+struct __align__(16) SVertRaw<double> {
+    double2 q[3];   // (ps, pc) (p0, syx) (sxy, unused)
 };
 
 template <typename T, int TPB>
 struct StageCfg {
     static constexpr int kBeams = TPB;
     static constexpr int kVerts = 4 * TPB;
-    static constexpr size_t kBytes = kBeams * sizeof(SBeam<T>) + kVerts * sizeof(SVert<T>);
+    static constexpr size_t kBytes = kBeams * sizeof(SBeamRaw<T>) + kVerts * sizeof(SVertRaw<T>);
 };
 
-template <typename T>
-__device__ __forceinline__ void fill_beam(const BeamRec &r, double cp, double sp, int vs,
-                                          int gbeam, SBeam<T> &s)
+__device__ __forceinline__ void fill_beam(const BeamRec &r, double cp, double sp, int vs, int gbeam,
+                                          SBeamRaw<float> &s)
 {
-    s.a[0] = (T)(-(cp * r.ab[0] + sp * r.ab[1])); s.a[1] = (T)r.ab[2]; s.a[2] = (T)r.ab[3];
-    s.a[3] = (T)(-(cp * r.ab[4] + sp * r.ab[5])); s.a[4] = (T)r.ab[6]; s.a[5] = (T)r.ab[7];
+    float a[6], P[24];
+    a[0] = (float)(-(cp * r.ab[0] + sp * r.ab[1])); a[1] = (float)r.ab[2]; a[2] = (float)r.ab[3];
+    a[3] = (float)(-(cp * r.ab[4] + sp * r.ab[5])); a[4] = (float)r.ab[6]; a[5] = (float)r.ab[7];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
-        s.P[e] = (T)(sp * r.Q[e] + cp * r.Q[8 + e]);
-        s.P[8 + e] = (T)(-(cp * r.Q[16 + e] + sp * r.Q[24 + e]));
-        s.P[16 + e] = (T)r.Q[32 + e];
+        P[e] = (float)(sp * r.Q[e] + cp * r.Q[8 + e]);
+        P[8 + e] = (float)(-(cp * r.Q[16 + e] + sp * r.Q[24 + e]));
+        P[16 + e] = (float)r.Q[32 + e];
     }
+    s.q[0] = make_float4(a[0], a[1], a[2], a[3]);
+    s.q[1] = make_float4(a[4], a[5], (float)r.slab[0], (float)r.slab[1]);
+    s.q[2] = make_float4((float)r.slab[2], (float)r.slab[3], r.nearr2, __int_as_float(r.nv));
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-        s.slab[i] = (T)r.slab[i];
-    s.nearr2 = r.nearr2;
-    s.gbeam = gbeam;
-    s.vs = vs;
-    s.nv = r.nv;
+    for (int i = 0; i < 6; ++i)
+        s.q[3 + i] = make_float4(P[4 * i], P[4 * i + 1], P[4 * i + 2], P[4 * i + 3]);
+    s.q[9] = make_float4(__int_as_float(gbeam), __int_as_float(vs), 0.f, 0.f);
+}
+
+__device__ __forceinline__ void fill_beam(const BeamRec &r, double cp, double sp, int vs, int gbeam,
+                                          SBeamRaw<double> &s)
+{
+    s.q[0] = make_double2(-(cp * r.ab[0] + sp * r.ab[1]), r.ab[2]);
+    s.q[1] = make_double2(r.ab[3], -(cp * r.ab[4] + sp * r.ab[5]));
+    s.q[2] = make_double2(r.ab[6], r.ab[7]);
+    s.q[3] = make_double2(r.slab[0], r.slab[1]);
+    s.q[4] = make_double2(r.slab[2], r.slab[3]);
+#pragma unroll
+    for (int e = 0; e < 8; e += 2) {
+        s.q[5 + e / 2] = make_double2(sp * r.Q[e] + cp * r.Q[8 + e], sp * r.Q[e + 1] + cp * r.Q[9 + e]);
+        s.q[9 + e / 2] = make_double2(-(cp * r.Q[16 + e] + sp * r.Q[24 + e]),
+                                      -(cp * r.Q[17 + e] + sp * r.Q[25 + e]));
+        s.q[13 + e / 2] = make_double2(r.Q[32 + e], r.Q[33 + e]);
+    }
+    s.q[17] = make_double2(__hiloint2double(r.nv, __float_as_int(r.nearr2)),
+                           __hiloint2double(vs, gbeam));
+}
+
+__device__ __forceinline__ void fill_vert(const VertRec &r, double cp, double sp, SVertRaw<float> &w)
+{
+    w.q[0] = make_double2(-(cp * r.X + sp * r.Y), r.pc);
+    w.q[1] = make_double2(r.p0, __hiloint2double(__float_as_int((float)r.sxy), __float_as_int((float)r.syx)));
+}
+
+__device__ __forceinline__ void fill_vert(const VertRec &r, double cp, double sp, SVertRaw<double> &w)
+{
+    w.q[0] = make_double2(-(cp * r.X + sp * r.Y), r.pc);
+    w.q[1] = make_double2(r.p0, r.syx);
+    w.q[2] = make_double2(r.sxy, 0.0);
+}
+
+__device__ __forceinline__ void load_beam(const SBeamRaw<float> &s, BeamRegs<float> &b)
+{
+    const float4 q0 = s.q[0], q1 = s.q[1], q2 = s.q[2], q9 = s.q[9];
+    b.a[0] = q0.x; b.a[1] = q0.y; b.a[2] = q0.z; b.a[3] = q0.w; b.a[4] = q1.x; b.a[5] = q1.y;
+    b.slab[0] = q1.z; b.slab[1] = q1.w; b.slab[2] = q2.x; b.slab[3] = q2.y;
+    b.nearr2 = q2.z;
+    b.nv = __float_as_int(q2.w);
+    b.gbeam = __float_as_int(q9.x);
+    b.vs = __float_as_int(q9.y);
+}
+
+__device__ __forceinline__ void load_beam(const SBeamRaw<double> &s, BeamRegs<double> &b)
+{
+    const double2 q0 = s.q[0], q1 = s.q[1], q2 = s.q[2], q3 = s.q[3], q4 = s.q[4], q17 = s.q[17];
+    b.a[0] = q0.x; b.a[1] = q0.y; b.a[2] = q1.x; b.a[3] = q1.y; b.a[4] = q2.x; b.a[5] = q2.y;
+    b.slab[0] = q3.x; b.slab[1] = q3.y; b.slab[2] = q4.x; b.slab[3] = q4.y;
+    b.nearr2 = __int_as_float(__double2loint(q17.x));
+    b.nv = __double2hiint(q17.x);
+    b.vs = __double2hiint(q17.y);
+    b.gbeam = __double2loint(q17.y);
+}
+
+__device__ __forceinline__ void load_P(const SBeamRaw<float> &s, float *P)
+{
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const float4 q = s.q[3 + i];
+        P[4 * i] = q.x; P[4 * i + 1] = q.y; P[4 * i + 2] = q.z; P[4 * i + 3] = q.w;
+    }
+}
+
+__device__ __forceinline__ void load_P(const SBeamRaw<double> &s, double *P)
+{
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        const double2 q = s.q[5 + i];
+        P[2 * i] = q.x; P[2 * i + 1] = q.y;
+    }
+}
+
+// P0, Pc, Ps entries 2h and 2h+1 (re, im each) of a beam record.
+__device__ __forceinline__ void load_P_pair(const SBeamRaw<float> &s, int h, float *p0, float *pc,
+                                            float *ps)
+{
+    const float4 a = s.q[3 + h], b = s.q[5 + h], c = s.q[7 + h];
+    p0[0] = a.x; p0[1] = a.y; p0[2] = a.z; p0[3] = a.w;
+    pc[0] = b.x; pc[1] = b.y; pc[2] = b.z; pc[3] = b.w;
+    ps[0] = c.x; ps[1] = c.y; ps[2] = c.z; ps[3] = c.w;
+}
+
+__device__ __forceinline__ void load_P_pair(const SBeamRaw<double> &s, int h, double *p0, double *pc,
+                                            double *ps)
+{
+    const double2 a0 = s.q[5 + 2 * h], a1 = s.q[6 + 2 * h];
+    const double2 b0 = s.q[9 + 2 * h], b1 = s.q[10 + 2 * h];
+    const double2 c0 = s.q[13 + 2 * h], c1 = s.q[14 + 2 * h];
+    p0[0] = a0.x; p0[1] = a0.y; p0[2] = a1.x; p0[3] = a1.y;
+    pc[0] = b0.x; pc[1] = b0.y; pc[2] = b1.x; pc[3] = b1.y;
+    ps[0] = c0.x; ps[1] = c0.y; ps[2] = c1.x; ps[3] = c1.y;
+}
+
+struct VertRegs {
+    double ps, pc, p0;
+};
+
+__device__ __forceinline__ void load_vert(const SVertRaw<float> &w, VertRegs &v, float &syx, float &sxy)
+{
+    const double2 q0 = w.q[0], q1 = w.q[1];
+    v.ps = q0.x; v.pc = q0.y; v.p0 = q1.x;
+    syx = __int_as_float(__double2loint(q1.y));
+    sxy = __int_as_float(__double2hiint(q1.y));
+}
+
+__device__ __forceinline__ void load_vert(const SVertRaw<double> &w, VertRegs &v, double &syx, double &sxy)
+{
+    const double2 q0 = w.q[0], q1 = w.q[1], q2 = w.q[2];
+    v.ps = q0.x; v.pc = q0.y; v.p0 = q1.x;
+    syx = q1.y;
+    sxy = q2.x;
 }
 
 // Phasor (cos, sin) of 2 pi u.
@@ -517,17 +652,18 @@ __device__ __forceinline__ float rcp_t(float x) { return rcp32(x); }
 // interleave.  mn[d] receives the smallest |C_e| (nearly singular edges are
 // recomputed in FP64 by the caller).
 template <typename T, int DPT, int NV>
-__device__ __forceinline__ void edge_sums_fixed(const SVert<T> *v, const double *st, const double *ct,
+__device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const double *st, const double *ct,
                                                 const T *A, const T *B, const bool *useX,
                                                 T *sr, T *si, T *mn)
 {
-    T c[DPT][NV], s[DPT][NV];
+    T c[DPT][NV], s[DPT][NV], syx[NV], sxy[NV];
 #pragma unroll
     for (int e = 0; e < NV; ++e) {
-        const double ps = v[e].ps, pc = v[e].pc, p0 = v[e].p0;
+        VertRegs w;
+        load_vert(v[e], w, syx[e], sxy[e]);
 #pragma unroll
         for (int d = 0; d < DPT; ++d)
-            phasor(fma(st[d], ps, fma(ct[d], pc, p0)), s[d][e], c[d][e]);
+            phasor(fma(st[d], w.ps, fma(ct[d], w.pc, w.p0)), s[d][e], c[d][e]);
     }
 #pragma unroll
     for (int d = 0; d < DPT; ++d) {
@@ -538,10 +674,9 @@ __device__ __forceinline__ void edge_sums_fixed(const SVert<T> *v, const double 
 #pragma unroll
     for (int e = 0; e < NV; ++e) {
         const int en = (e + 1 < NV) ? e + 1 : 0;
-        const T syx = v[e].syx, sxy = v[e].sxy;
 #pragma unroll
         for (int d = 0; d < DPT; ++d) {
-            const T coef = useX[d] ? fma(syx, B[d], A[d]) : fma(sxy, A[d], B[d]);
+            const T coef = useX[d] ? fma(syx[e], B[d], A[d]) : fma(sxy[e], A[d], B[d]);
             const T inv = rcp_t(coef);
             mn[d] = fmin(mn[d], fabs(coef));
             sr[d] = fma(c[d][en] - c[d][e], inv, sr[d]);
@@ -551,14 +686,17 @@ __device__ __forceinline__ void edge_sums_fixed(const SVert<T> *v, const double 
 }
 
 template <typename T, int DPT>
-__device__ __forceinline__ void edge_sums_loop(const SVert<T> *v, int nv, const double *st,
+__device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, const double *st,
                                                const double *ct, const T *A, const T *B,
                                                const bool *useX, T *sr, T *si, T *mn)
 {
     T c0[DPT], s0[DPT], cp_[DPT], sp_[DPT];
+    T syx, sxy;
+    VertRegs w;
+    load_vert(v[0], w, syx, sxy);
 #pragma unroll
     for (int d = 0; d < DPT; ++d) {
-        phasor(fma(st[d], v[0].ps, fma(ct[d], v[0].pc, v[0].p0)), s0[d], c0[d]);
+        phasor(fma(st[d], w.ps, fma(ct[d], w.pc, w.p0)), s0[d], c0[d]);
         cp_[d] = c0[d];
         sp_[d] = s0[d];
         mn[d] = T(1e30);
@@ -567,19 +705,15 @@ __device__ __forceinline__ void edge_sums_loop(const SVert<T> *v, int nv, const 
     }
     for (int e = 0; e < nv; ++e) {
         const bool last = e + 1 == nv;
-        const int en = last ? 0 : e + 1;
-        const double ps = v[en].ps, pc = v[en].pc, p0 = v[en].p0;
-        const T syx = v[e].syx, sxy = v[e].sxy;
+        const T syx_e = syx, sxy_e = sxy;
+        if (!last)
+            load_vert(v[e + 1], w, syx, sxy);
 #pragma unroll
         for (int d = 0; d < DPT; ++d) {
-            T cn, sn;
-            if (last) {
-                cn = c0[d];
-                sn = s0[d];
-            } else {
-                phasor(fma(st[d], ps, fma(ct[d], pc, p0)), sn, cn);
-            }
-            const T coef = useX[d] ? fma(syx, B[d], A[d]) : fma(sxy, A[d], B[d]);
+            T cn = c0[d], sn = s0[d];
+            if (!last)
+                phasor(fma(st[d], w.ps, fma(ct[d], w.pc, w.p0)), sn, cn);
+            const T coef = useX[d] ? fma(syx_e, B[d], A[d]) : fma(sxy_e, A[d], B[d]);
             const T inv = rcp_t(coef);
             mn[d] = fmin(mn[d], fabs(coef));
             sr[d] = fma(cn - cp_[d], inv, sr[d]);
@@ -591,7 +725,7 @@ __device__ __forceinline__ void edge_sums_loop(const SVert<T> *v, int nv, const 
 }
 
 template <typename T, int DPT>
-__device__ __forceinline__ void edge_sums(const SVert<T> *v, int nv, const double *st,
+__device__ __forceinline__ void edge_sums(const SVertRaw<T> *v, int nv, const double *st,
                                           const double *ct, const T *A, const T *B,
                                           const bool *useX, T *sr, T *si, T *mn)
 {
@@ -606,25 +740,29 @@ __device__ __forceinline__ void edge_sums(const SVert<T> *v, int nv, const doubl
 
 // The rare pairs of one direction, in FP64: the near-forward moment
 // expansion (FP32C), or the complete general evaluation (small-phase
-// candidates, nearly singular edges, irregular polar rows).  Writes d[8];
+// candidates, nearly singular edges, irregular polar rows).  Writes the
+// Jones contribution to the thread's shared-memory slot out[0..7] (stride
+// `stride`), so the caller's registers never leave the register file;
 // returns false when the beam contributes nothing.
 template <typename T>
-__device__ __noinline__ bool beam_rare(const KParams &P, int gbeam, const SBeam<T> &b, int p, int t,
-                                       double st, double ct, double cp, double sp, bool near,
-                                       T *d)
+__device__ __noinline__ bool beam_rare(const KParams &P, int gbeam, const SBeamRaw<T> *sbr, int p,
+                                       int t, bool near, T *out, int stride)
 {
     constexpr bool kF32 = sizeof(T) == 4;
+    const double st = P.st[t], ct = P.ct[t], cp = P.cphi[p], sp = P.sphi[p];
     if (kF32 && near) {
         float sr, si;
         near_forward_s(P.beams[gbeam], P.moments + (size_t)gbeam * kNumMoments, st, ct, cp, sp,
                        P.wc, sr, si);
+        T Pm[24];
+        load_P(*sbr, Pm);
         const T stT = (T)st, ctT = (T)ct;
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-            const T rr = fma(stT, b.P[16 + 2 * e], fma(ctT, b.P[8 + 2 * e], b.P[2 * e]));
-            const T ri = fma(stT, b.P[17 + 2 * e], fma(ctT, b.P[9 + 2 * e], b.P[2 * e + 1]));
-            d[2 * e] = fma((T)sr, rr, -(T)si * ri);
-            d[2 * e + 1] = fma((T)sr, ri, (T)si * rr);
+            const T rr = fma(stT, Pm[16 + 2 * e], fma(ctT, Pm[8 + 2 * e], Pm[2 * e]));
+            const T ri = fma(stT, Pm[17 + 2 * e], fma(ctT, Pm[9 + 2 * e], Pm[2 * e + 1]));
+            out[(2 * e) * stride] = fma((T)sr, rr, -(T)si * ri);
+            out[(2 * e + 1) * stride] = fma((T)sr, ri, (T)si * rr);
         }
         return true;
     }
@@ -634,13 +772,14 @@ __device__ __noinline__ bool beam_rare(const KParams &P, int gbeam, const SBeam<
     const bool ok = beam_general(P.beams[gbeam], P.verts, dc, P.wc, dd);
 #pragma unroll
     for (int q = 0; q < 8; ++q)
-        d[q] = (T)dd[q];
+        out[q * stride] = (T)dd[q];
     return ok;
 }
 
-// Accumulators of the coherent Jones sum of one orientation.  FP32: plain
-// sums over blocks of kFlushEvery beams in registers, folded into a
-// Kahan-compensated running sum (kept in shared memory) at every block end.
+// Accumulator of the coherent Jones sum of one orientation for one
+// direction.  FP32: plain sums over blocks of kFlushEvery beams in
+// registers, folded into a Kahan-compensated running sum kept in shared
+// memory (s, c with stride) at every block end.  FP64: plain sums.
 constexpr int kFlushEvery = 16;
 
 template <typename T>
@@ -654,21 +793,18 @@ struct JonesAcc {
 #pragma unroll
         for (int i = 0; i < 8; ++i) b[i] += d[i];
     }
-};
-
-// Kahan fold of a block sum into (s, c) held in shared memory with stride.
-__device__ __forceinline__ void kahan_fold(float *b, float *s, float *c, int stride)
-{
+    __device__ __forceinline__ void fold(float *s, float *c, int stride) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const float si = s[i * stride], ci = c[i * stride];
-        const float y = __fsub_rn(b[i], ci);
-        const float t = __fadd_rn(si, y);
-        c[i * stride] = __fsub_rn(__fsub_rn(t, si), y);
-        s[i * stride] = t;
-        b[i] = 0.f;
+        for (int i = 0; i < 8; ++i) {
+            const float si = s[i * stride], ci = c[i * stride];
+            const float y = __fsub_rn((float)b[i], ci);
+            const float t = __fadd_rn(si, y);
+            c[i * stride] = __fsub_rn(__fsub_rn(t, si), y);
+            s[i * stride] = t;
+            b[i] = T(0);
+        }
     }
-}
+};
 
 // Fused diffraction kernel.  Grid: x = azimuth bin * zenith tiles, y =
 // orientation chunk.  Each thread owns DPT directions (zenith rows
@@ -681,10 +817,12 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
     constexpr bool kF32 = sizeof(T) == 4;
     constexpr int kSets = NS ? 2 : 1;        // full and no-shadow sums
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SBeam<T> *sb = reinterpret_cast<SBeam<T> *>(smem_raw);
-    SVert<T> *sv = reinterpret_cast<SVert<T> *>(smem_raw + Cfg::kBeams * sizeof(SBeam<T>));
+    SBeamRaw<T> *sb = reinterpret_cast<SBeamRaw<T> *>(smem_raw);
+    SVertRaw<T> *sv = reinterpret_cast<SVertRaw<T> *>(smem_raw + Cfg::kBeams * sizeof(SBeamRaw<T>));
+    // rare-path result slot per thread: [8][TPB]
+    T *rsm = reinterpret_cast<T *>(smem_raw + Cfg::kBytes);
     // FP32C: Kahan running sums of the Jones matrices, [kSets][s, c][8][kDirs]
-    float *Ksm = reinterpret_cast<float *>(smem_raw + Cfg::kBytes);
+    float *Ksm = reinterpret_cast<float *>(rsm + 8 * TPB);
 
     const int p = blockIdx.x / P.tiles_per_row;
     const int tile = blockIdx.x - p * P.tiles_per_row;
@@ -693,6 +831,7 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
     const int o1 = min(P.n_orient, o0 + P.orient_per_chunk);
     const double cp = P.cphi[p], sp = P.sphi[p];
     const T eps = (T)(kF32 ? P.wc.eps1_f32 : P.wc.eps1);
+    T *rslot = rsm + threadIdx.x;
 
     int t[DPT];
     bool active[DPT], general[DPT];
@@ -726,33 +865,29 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
         const int b0 = P.beam_off[o], b1 = P.beam_off[o + 1];
         for (int bs = b0; bs < b1;) {
             // stage [bs, be): at most kBeams beams and kVerts vertices
-            int lo = bs + 1, hi = min(b1, bs + Cfg::kBeams);
             const int vb0 = P.vbeg[bs];
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (P.vbeg[mid] - vb0 <= Cfg::kVerts) lo = mid; else hi = mid - 1;
+            int be = min(b1, bs + Cfg::kBeams);
+            if (P.vbeg[be] - vb0 > Cfg::kVerts) {
+                int lo = bs + 1, hi = be;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (P.vbeg[mid] - vb0 <= Cfg::kVerts) lo = mid; else hi = mid - 1;
+                }
+                be = lo;
             }
-            const int be = lo;
             const int nb = be - bs;
             const int nvs = P.vbeg[be] - vb0;
             __syncthreads();   // previous stage fully consumed
             for (int i = threadIdx.x; i < nb; i += TPB) {
                 const BeamRec &r = P.brec[bs + i];
-                fill_beam<T>(r, cp, sp, r.vbeg - vb0, bs + i, sb[i]);
+                fill_beam(r, cp, sp, r.vbeg - vb0, bs + i, sb[i]);
             }
-            for (int i = threadIdx.x; i < nvs; i += TPB) {
-                const VertRec &r = P.vrec[vb0 + i];
-                SVert<T> w;
-                w.ps = -(cp * r.X + sp * r.Y);
-                w.pc = r.pc;
-                w.p0 = r.p0;
-                w.syx = (T)r.syx;
-                w.sxy = (T)r.sxy;
-                sv[i] = w;
-            }
+            for (int i = threadIdx.x; i < nvs; i += TPB)
+                fill_vert(P.vrec[vb0 + i], cp, sp, sv[i]);
             __syncthreads();
             for (int j = 0; j < nb; ++j) {
-                const SBeam<T> &b = sb[j];
+                BeamRegs<T> b;
+                load_beam(sb[j], b);
                 T A[DPT], B[DPT], sr[DPT], si[DPT], mn[DPT];
                 bool useX[DPT], rare[DPT], near[DPT];
 #pragma unroll
@@ -766,42 +901,56 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                     rare[d] = general[d] || near[d] || cand;
                 }
                 edge_sums<T, DPT>(sv + b.vs, b.nv, st, ct, A, B, useX, sr, si, mn);
+                const bool internal = NS && !(P.beams[b.gbeam].flags & MBS_PO_BEAM_EXTERNAL);
+                T s_r[DPT], s_i[DPT];
+                bool ok[DPT];
+#pragma unroll
+                for (int d = 0; d < DPT; ++d) {
+                    const T m = useX[d] ? rcp_t(B[d]) : -rcp_t(A[d]);
+                    s_r[d] = sr[d] * m;
+                    s_i[d] = si[d] * m;
+                    ok[d] = !(s_r[d] != s_r[d]);
+                }
+                // d = s x (P0 + cos t Pc + sin t Ps), two complex entries at a time
+                T dj[DPT][8];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    T p0[4], pc[4], ps[4];
+                    load_P_pair(sb[j], h, p0, pc, ps);
+#pragma unroll
+                    for (int d = 0; d < DPT; ++d) {
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const T rr = fma(stT[d], ps[2 * e], fma(ctT[d], pc[2 * e], p0[2 * e]));
+                            const T ri = fma(stT[d], ps[2 * e + 1], fma(ctT[d], pc[2 * e + 1], p0[2 * e + 1]));
+                            dj[d][4 * h + 2 * e] = fma(s_r[d], rr, -s_i[d] * ri);
+                            dj[d][4 * h + 2 * e + 1] = fma(s_r[d], ri, s_i[d] * rr);
+                        }
+                    }
+                }
 #pragma unroll
                 for (int d = 0; d < DPT; ++d) {
                     if (!active[d])
                         continue;
-                    T dj[8];
-                    bool ok;
                     if (rare[d] || mn[d] <= eps) {
-                        ok = beam_rare<T>(P, bs + j, b, p, t[d], st[d], ct[d], cp, sp,
-                                          near[d] && !general[d], dj);
-                    } else {
-                        const T m = useX[d] ? rcp_t(B[d]) : -rcp_t(A[d]);
-                        const T s_r = sr[d] * m, s_i = si[d] * m;
-                        ok = !(s_r != s_r);
-                        // d = s x (P0 + cos t Pc + sin t Ps)
+                        ok[d] = beam_rare<T>(P, b.gbeam, &sb[j], p, t[d], near[d] && !general[d], rslot, TPB);
 #pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            const T rr = fma(stT[d], b.P[16 + 2 * e], fma(ctT[d], b.P[8 + 2 * e], b.P[2 * e]));
-                            const T ri = fma(stT[d], b.P[17 + 2 * e], fma(ctT[d], b.P[9 + 2 * e], b.P[2 * e + 1]));
-                            dj[2 * e] = fma(s_r, rr, -s_i * ri);
-                            dj[2 * e + 1] = fma(s_r, ri, s_i * rr);
-                        }
+                        for (int q = 0; q < 8; ++q)
+                            dj[d][q] = rslot[q * TPB];
                     }
-                    if (ok) {
-                        J[d].add(dj);
-                        if (NS && !(P.beams[bs + j].flags & MBS_PO_BEAM_EXTERNAL))
-                            Jn[d].add(dj);
+                    if (ok[d]) {
+                        J[d].add(dj[d]);
+                        if (NS && internal)
+                            Jn[d].add(dj[d]);
                     }
                 }
                 if (kF32 && ((j & (kFlushEvery - 1)) == kFlushEvery - 1 || j + 1 == nb)) {
 #pragma unroll
                     for (int d = 0; d < DPT; ++d) {
                         const int slot = d * TPB + threadIdx.x;
-                        kahan_fold(reinterpret_cast<float *>(J[d].b), Ksm + slot, Ksm + 8 * kDirs + slot, kDirs);
+                        J[d].fold(Ksm + slot, Ksm + 8 * kDirs + slot, kDirs);
                         if (NS)
-                            kahan_fold(reinterpret_cast<float *>(Jn[d].b), Ksm + 16 * kDirs + slot,
-                                       Ksm + 24 * kDirs + slot, kDirs);
+                            Jn[d].fold(Ksm + 16 * kDirs + slot, Ksm + 24 * kDirs + slot, kDirs);
                     }
                 }
             }
@@ -852,7 +1001,7 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
 template <typename T, int TPB, int DPT, bool NS>
 constexpr size_t diffract_smem_bytes()
 {
-    return StageCfg<T, TPB>::kBytes
+    return StageCfg<T, TPB>::kBytes + 8 * TPB * sizeof(T)
          + (sizeof(T) == 4 ? (NS ? 2 : 1) * 16 * TPB * DPT * sizeof(float) : 0);
 }
 
