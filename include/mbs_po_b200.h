@@ -168,6 +168,42 @@ int mbs_po_diffract_staged(mbs_po_ctx *ctx, const mbs_po_staged *staged,
                            double *Mns_accum_dev, void *stream,
                            mbs_po_stats *stats);
 
+/* Multi-size scan: the orientations of `beams` at n_scales particle sizes
+ * (size factor scales[i] relative to the traced particle), all in one
+ * diffraction launch.  Instance i is the batch with vertex coordinates and
+ * beam centres times scales[i], beam areas times scales[i]^2 and the Jones
+ * matrices re-phased from the unphased records,
+ *     J_phased = sign * absorption(s) * J * exp(i wave_index s path)
+ * (beam_raw is required; abs_offsets/abs_paths with the absorption
+ * coefficient of the wave constants give absorption(s)).  wave_index <= 0
+ * uses the context's wave number.  M_accum: n_scales consecutive Mueller
+ * planes of [n_az*(n_zen+1)*16] doubles (host), each accumulated +=.
+ * Replaces HandlerPO::HandleOrientationsToLocalGpuMultiK (reference
+ * GpuDiffraction.cu:3956-4158, src/handler/HandlerPO.h:132-137) and the scaled
+ * single-size call HandleOrientationsToLocalGpu(..., scale, waveIndex)
+ * (GpuDiffraction.cu:4323-4324). */
+int mbs_po_diffract_multisize(mbs_po_ctx *ctx, const mbs_po_beams *beams,
+                              const double *scales, int n_scales, double wave_index,
+                              int precision, double *M_accum, double *Mns_accum,
+                              mbs_po_stats *stats);
+/* Device-resident multi-size batch: mbs_po_diffract_staged on it writes
+ * mbs_po_staged_sets() consecutive Mueller planes (one per size). */
+int mbs_po_stage_multisize(mbs_po_ctx *ctx, const mbs_po_beams *beams,
+                           const double *scales, int n_scales, double wave_index,
+                           mbs_po_staged **out);
+int mbs_po_staged_sets(const mbs_po_staged *staged);
+
+/* Orientation-averaged M11 on a list of zenith angles (radians), summed over
+ * the context grid's n_az azimuth bins and over beams INCOHERENTLY:
+ *   m11_out[t] = sum_o w_o sum_beams sum_{p<n_az} 0.5 |d|^2 / (n_az + 1)
+ * with d the beam's GPU-convention Jones contribution (rotation without the
+ * 0.5 factor), zenith angles clamped 1e-6 away from the poles and the
+ * stable edge quotient off (zero for |C_e| <= eps1), in FP64.  m11_out[n]
+ * (host) is overwritten.  Replaces HandlerPO::DiffractThetasGpu (reference
+ * GpuDiffraction.cu:4780-4970, theta_m11_kernel). */
+int mbs_po_diffract_thetas(mbs_po_ctx *ctx, const mbs_po_beams *beams,
+                           const double *theta_rad, int n, double *m11_out);
+
 /* Optical-theorem extinction per orientation on the device (weighted by the
  * orientation weight), written to cext_out[n_orient] (host).  Replaces
  * HandlerPO::ComputeForwardExtinctionOt (reference HandlerPO.cpp:1812-2009). */

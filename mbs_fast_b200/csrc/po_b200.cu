@@ -69,9 +69,11 @@ struct mbs_po_staged {
     int32_t *vbeg = nullptr;
     int32_t *beam_off = nullptr;
     double *weight = nullptr;
-    int n_orient = 0;
+    int n_orient = 0;              // all instances: n_sets * orient_per_set
     int64_t n_beams = 0, n_verts = 0;
     int max_nv = 0;
+    int n_sets = 1;                // output planes (size instances)
+    int orient_per_set = 0;
 };
 
 struct mbs_po_ctx {
@@ -349,17 +351,39 @@ namespace {
 
 // Upload a batch and build the device records into `s` (capacity reused).
 // The records carry wave-dependent coefficients: a staged batch belongs to
-// the wave constants set when it was staged.
-int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStream_t st)
+// the wave constants set when it was staged.  With `scales` the batch is
+// staged once per size factor (instance i = scales[i]); instance i's
+// orientations are [i nO, (i+1) nO) and its results go to output set i.
+int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStream_t st,
+               const double *scales = nullptr, int n_scales = 0, double k_rephase = 0.0)
 {
     int rc = validate(ctx, b);
     if (rc)
         return rc;
     if (!ctx->has_wave)
         return fail(ctx, MBS_PO_ESTATE, "wave constants must be set before staging");
+    const int nI = scales ? n_scales : 1;
+    if (scales) {
+        if (n_scales < 1)
+            return fail(ctx, MBS_PO_EINVAL, "no size scale factors");
+        for (int i = 0; i < n_scales; ++i)
+            if (!(scales[i] > 0.0) || !std::isfinite(scales[i]))
+                return fail(ctx, MBS_PO_EINVAL, "size scale factors must be positive");
+        if (b->n_beams > 0 && !b->beam_raw)
+            return fail(ctx, MBS_PO_EINVAL, "size scaling needs the unphased Jones records (beam_raw)");
+        if (b->n_beams > 0 && (b->abs_offsets == nullptr) != (b->abs_paths == nullptr)
+            && b->abs_offsets && b->abs_offsets[b->n_beams] > 0)
+            return fail(ctx, MBS_PO_EINVAL, "abs_offsets given without abs_paths");
+    }
+    if ((int64_t)nI * b->n_beams >= ((int64_t)1 << 31) || (int64_t)nI * b->n_verts >= ((int64_t)1 << 31)
+        || (int64_t)nI * b->n_orient >= ((int64_t)1 << 31))
+        return fail(ctx, MBS_PO_ERANGE, "staged instances exceed 2^31 beams, vertices or orientations");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const int64_t nB = b->n_beams, nV = b->n_verts, nO = b->n_orient;
+    const bool has_abs = scales && b->abs_offsets && b->abs_paths && nB > 0 && b->abs_offsets[nB] > 0;
+    const int64_t nAbs = has_abs ? b->abs_offsets[nB] : 0;
     // raw upload area: vert_off, vx, vy, syx, sxy, geom, flags
+    // (+ scales, raw Jones records, absorption paths for size instances)
     const size_t off_vo = 0;
     const size_t off_vx = off_vo + align256((nB + 1) * 8);
     const size_t off_vy = off_vx + align256(nV * 8);
@@ -368,20 +392,25 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     const size_t off_g = off_sxy + align256(nV * 8);
     const size_t off_ef = off_g + align256(nB * MBS_PO_GEOM_STRIDE * 8);
     const size_t off_bf = off_ef + align256(nV);
-    const size_t raw_bytes = off_bf + align256(nB);
+    const size_t off_sc = off_bf + align256(nB);
+    const size_t off_raw = off_sc + align256(scales ? nI * 8 : 0);
+    const size_t off_ao = off_raw + align256(scales ? nB * MBS_PO_RAW_STRIDE * 8 : 0);
+    const size_t off_ap = off_ao + align256(has_abs ? (nB + 1) * 8 : 0);
+    const size_t raw_bytes = off_ap + align256(nAbs * 8);
     if ((rc = ensure_arena(ctx, ctx->raw, raw_bytes, "staging")))
         return rc;
     unsigned char *raw = (unsigned char *)ctx->raw.base;
-    // device records
+    // device records (nI instances)
+    const int64_t iB = nI * nB, iV = nI * nV, iO = nI * nO;
     const size_t o_beams = 0;
-    const size_t o_verts = o_beams + align256(nB * sizeof(DevBeam));
-    const size_t o_brec = o_verts + align256(nV * sizeof(DevVert));
-    const size_t o_vrec = o_brec + align256(nB * sizeof(BeamRec));
-    const size_t o_mom = o_vrec + align256(nV * sizeof(VertRec));
-    const size_t o_vbeg = o_mom + align256(nB * kNumMoments * sizeof(double));
-    const size_t o_boff = o_vbeg + align256((nB + 1) * sizeof(int32_t));
-    const size_t o_w = o_boff + align256((nO + 1) * sizeof(int32_t));
-    const size_t bytes = o_w + align256(std::max<int64_t>(nO, 1) * sizeof(double));
+    const size_t o_verts = o_beams + align256(iB * sizeof(DevBeam));
+    const size_t o_brec = o_verts + align256(iV * sizeof(DevVert));
+    const size_t o_vrec = o_brec + align256(iB * sizeof(BeamRec));
+    const size_t o_mom = o_vrec + align256(iV * sizeof(VertRec));
+    const size_t o_vbeg = o_mom + align256(iB * kNumMoments * sizeof(double));
+    const size_t o_boff = o_vbeg + align256((iB + 1) * sizeof(int32_t));
+    const size_t o_w = o_boff + align256((iO + 1) * sizeof(int32_t));
+    const size_t bytes = o_w + align256(std::max<int64_t>(iO, 1) * sizeof(double));
     if ((rc = ensure_arena(ctx, s->arena, bytes, "staged batch")))
         return rc;
     unsigned char *base = (unsigned char *)s->arena.base;
@@ -394,12 +423,14 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     s->beam_off = (int32_t *)(base + o_boff);
     s->weight = (double *)(base + o_w);
 
-    std::vector<int32_t> boff(nO + 1);
-    for (int64_t o = 0; o <= nO; ++o)
-        boff[o] = (int32_t)b->beam_offsets[o];
-    CK(cudaMemcpyAsync(s->beam_off, boff.data(), (nO + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, st), "H2D offsets");
-    if (nO > 0)
-        CK(cudaMemcpyAsync(s->weight, b->orient_weight, nO * sizeof(double), cudaMemcpyHostToDevice, st), "H2D weights");
+    std::vector<int32_t> boff(iO + 1);
+    for (int i = 0; i < nI; ++i)
+        for (int64_t o = 0; o < nO; ++o)
+            boff[i * nO + o] = (int32_t)(i * nB + b->beam_offsets[o]);
+    boff[iO] = (int32_t)iB;
+    CK(cudaMemcpyAsync(s->beam_off, boff.data(), (iO + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, st), "H2D offsets");
+    for (int i = 0; i < nI && nO > 0; ++i)
+        CK(cudaMemcpyAsync(s->weight + i * nO, b->orient_weight, nO * sizeof(double), cudaMemcpyHostToDevice, st), "H2D weights");
     if (nB > 0) {
         CK(cudaMemcpyAsync(raw + off_vo, b->vert_offsets, (nB + 1) * 8, cudaMemcpyHostToDevice, st), "H2D vert_offsets");
         CK(cudaMemcpyAsync(raw + off_vx, b->vx, nV * 8, cudaMemcpyHostToDevice, st), "H2D vx");
@@ -409,9 +440,24 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
         CK(cudaMemcpyAsync(raw + off_g, b->beam_geom, nB * MBS_PO_GEOM_STRIDE * 8, cudaMemcpyHostToDevice, st), "H2D geom");
         CK(cudaMemcpyAsync(raw + off_ef, b->edge_flags, nV, cudaMemcpyHostToDevice, st), "H2D edge_flags");
         CK(cudaMemcpyAsync(raw + off_bf, b->beam_flags, nB, cudaMemcpyHostToDevice, st), "H2D beam_flags");
+        if (scales) {
+            CK(cudaMemcpyAsync(raw + off_sc, scales, nI * 8, cudaMemcpyHostToDevice, st), "H2D scales");
+            CK(cudaMemcpyAsync(raw + off_raw, b->beam_raw, nB * MBS_PO_RAW_STRIDE * 8, cudaMemcpyHostToDevice, st), "H2D raw Jones");
+            if (has_abs) {
+                CK(cudaMemcpyAsync(raw + off_ao, b->abs_offsets, (nB + 1) * 8, cudaMemcpyHostToDevice, st), "H2D abs offsets");
+                CK(cudaMemcpyAsync(raw + off_ap, b->abs_paths, nAbs * 8, cudaMemcpyHostToDevice, st), "H2D abs paths");
+            }
+        }
         CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st), "memset status");
         PackParams P;
         P.n_beams = nB;
+        P.n_verts = nV;
+        P.sc.scales = scales ? (const double *)(raw + off_sc) : nullptr;
+        P.sc.raw = scales ? (const double *)(raw + off_raw) : nullptr;
+        P.sc.abs_off = has_abs ? (const int64_t *)(raw + off_ao) : nullptr;
+        P.sc.abs_paths = has_abs ? (const double *)(raw + off_ap) : nullptr;
+        P.sc.k_rephase = k_rephase > 0.0 ? k_rephase : ctx->wc.k;
+        P.sc.abs_coeff = ctx->wave.abs_coeff;
         P.vert_off = (const int64_t *)(raw + off_vo);
         P.vx = (const double *)(raw + off_vx);
         P.vy = (const double *)(raw + off_vy);
@@ -429,7 +475,7 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
         P.vbeg = s->vbeg;
         P.status = ctx->d_status;
         const int threads = 128;
-        const int blocks = (int)((nB + 1 + threads - 1) / threads);
+        const dim3 blocks((unsigned)((nB + 1 + threads - 1) / threads), (unsigned)nI);
         po_pack_kernel<<<blocks, threads, 0, st>>>(P);
         CK(cudaGetLastError(), "pack kernel launch");
         int status = 0;
@@ -438,9 +484,11 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
         if (status)
             return fail(ctx, MBS_PO_EBEAM, "malformed beam in batch");
     }
-    s->n_orient = (int)nO;
-    s->n_beams = nB;
-    s->n_verts = nV;
+    s->n_orient = (int)iO;
+    s->n_beams = iB;
+    s->n_verts = iV;
+    s->n_sets = nI;
+    s->orient_per_set = (int)nO;
     int mx = 0;
     for (int64_t i = 0; i < nB; ++i)
         mx = std::max<int>(mx, (int)(b->vert_offsets[i + 1] - b->vert_offsets[i]));
@@ -449,10 +497,14 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
 }
 
 struct LaunchPlan {
-    int tiles_per_row, n_chunks, orient_per_chunk;
+    int tiles_per_row, n_chunks, orient_per_chunk, chunks_per_set;
 };
 
-LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ctas_per_sm)
+// Orientation chunks per output set: about six waves of CTAs over the
+// whole launch, at most 64 chunks per set (each chunk owns a partial plane).
+// n_orient is per set; n_chunks counts all sets.
+LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ctas_per_sm,
+                       int n_sets = 1)
 {
     LaunchPlan L;
     L.tiles_per_row = (n_t + dirs_per_cta - 1) / dirs_per_cta;
@@ -464,13 +516,15 @@ LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ct
             && cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
             sms = v;
     }
+    n_sets = std::max(1, n_sets);
     const long long target = (long long)sms * ctas_per_sm * 6;   // ~6 waves
-    long long chunks = (target + ctas_per_chunk - 1) / ctas_per_chunk;
+    long long chunks = (target + ctas_per_chunk * n_sets - 1) / (ctas_per_chunk * n_sets);
     chunks = std::max<long long>(1, std::min<long long>(chunks, std::max(1, n_orient)));
     chunks = std::min<long long>(chunks, 64);
     L.orient_per_chunk = (int)((n_orient + chunks - 1) / chunks);
-    L.n_chunks = (int)((n_orient + L.orient_per_chunk - 1) / std::max(1, L.orient_per_chunk));
-    if (L.n_chunks < 1) L.n_chunks = 1;
+    L.chunks_per_set = (int)((n_orient + L.orient_per_chunk - 1) / std::max(1, L.orient_per_chunk));
+    if (L.chunks_per_set < 1) L.chunks_per_set = 1;
+    L.n_chunks = L.chunks_per_set * n_sets;
     return L;
 }
 
@@ -539,8 +593,11 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     if (ns)
         variant = 0;
     const Variant V = pi == 0 ? kVariantsF64[variant] : kVariantsF32[variant];
-    const int n_orient = orient_limit > 0 ? std::min(orient_limit, s->n_orient) : s->n_orient;
-    const LaunchPlan L = plan_launch(nAz, nT, n_orient, V.tpb * V.dpt, V.minb);
+    // the autotuner's slice: the first orient_limit orientations of set 0
+    const int n_sets = orient_limit > 0 ? 1 : s->n_sets;
+    const int per_set = orient_limit > 0 ? std::min(orient_limit, s->orient_per_set) : s->orient_per_set;
+    const int n_orient = n_sets * per_set;
+    const LaunchPlan L = plan_launch(nAz, nT, per_set, V.tpb * V.dpt, V.minb, n_sets);
     const size_t plane = (size_t)16 * G;
     int rc;
     if ((rc = ensure(ctx, ctx->partial, ctx->partial_cap, plane * L.n_chunks * (ns ? 2 : 1), "partials")))
@@ -565,6 +622,8 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     P.n_orient = n_orient;
     P.orient_per_chunk = L.orient_per_chunk;
     P.tiles_per_row = L.tiles_per_row;
+    P.orient_per_set = per_set;
+    P.chunks_per_set = L.chunks_per_set;
     P.wc = ctx->wc;
     P.partial = ctx->partial;
     P.partial_ns = ns ? ctx->partial + plane * L.n_chunks : nullptr;
@@ -591,12 +650,12 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
         CK(cudaStreamWaitEvent(st, ctx->ev[6], 0), "join side stream");
     CK(cudaEventRecord(ctx->ev[1], st), "event");
     const int rb = 256;
-    const int rg = (int)((G * 16 + rb - 1) / rb);
-    po_reduce_kernel<<<rg, rb, 0, st>>>(ctx->partial, L.n_chunks, G, M_dev);
+    const dim3 rg((unsigned)((G * 16 + rb - 1) / rb), (unsigned)n_sets);
+    po_reduce_kernel<<<rg, rb, 0, st>>>(ctx->partial, L.chunks_per_set, G, M_dev);
     CK(cudaGetLastError(), "reduce launch");
     ++launches;
     if (ns) {
-        po_reduce_kernel<<<rg, rb, 0, st>>>(P.partial_ns, L.n_chunks, G, Mns_dev);
+        po_reduce_kernel<<<rg, rb, 0, st>>>(P.partial_ns, L.chunks_per_set, G, Mns_dev);
         CK(cudaGetLastError(), "reduce launch");
         ++launches;
     }
@@ -709,20 +768,29 @@ extern "C" int mbs_po_diffract_staged(mbs_po_ctx *ctx, const mbs_po_staged *s, i
     return run_diffract(ctx, s, precision, M_dev, Mns_dev, (cudaStream_t)stream, stats);
 }
 
-extern "C" int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
-                               double *M_accum, double *Mns_accum, mbs_po_stats *stats)
+namespace {
+
+// Host-buffer path shared by mbs_po_diffract and mbs_po_diffract_multisize:
+// stage (one size instance per scale, or the batch as is), diffract into
+// device accumulators, copy back, add into the caller's planes.
+int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scales, int n_scales,
+                  double k_rephase, int precision, double *M_accum, double *Mns_accum,
+                  mbs_po_stats *stats)
 {
     if (!ctx || !beams || !M_accum)
         return fail(ctx, MBS_PO_EINVAL, "null argument");
     if (!ctx->has_grid || !ctx->has_wave)
         return fail(ctx, MBS_PO_ESTATE, "grid and wave constants must be set first");
+    if (scales && n_scales < 1)
+        return fail(ctx, MBS_PO_EINVAL, "no size scale factors");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const int64_t G = (int64_t)ctx->grid.n_az * (ctx->grid.n_zen + 1);
     if (beams->n_orient == 0 || beams->n_beams == 0 || G == 0)
         return validate(ctx, beams);
     cudaStream_t st = ctx->stream;
     const bool ns = Mns_accum != nullptr;
-    const size_t n = (size_t)G * 16;
+    const size_t sets = scales ? (size_t)n_scales : 1;
+    const size_t n = (size_t)G * 16 * sets;
     int rc;
     if ((rc = ensure(ctx, ctx->macc, ctx->macc_cap, n * 2, "accumulators")))
         return rc;
@@ -734,7 +802,7 @@ extern "C" int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int p
         ctx->hres_cap = n * 2;
     }
     CK(cudaEventRecord(ctx->ev[3], st), "event");
-    if ((rc = stage_into(ctx, beams, &ctx->host_staged, st)))
+    if ((rc = stage_into(ctx, beams, &ctx->host_staged, st, scales, n_scales, k_rephase)))
         return rc;
     CK(cudaEventRecord(ctx->ev[4], st), "event");
     CK(cudaMemsetAsync(ctx->macc, 0, n * (ns ? 2 : 1) * sizeof(double), st), "memset acc");
@@ -758,6 +826,117 @@ extern "C" int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int p
         stats->d2h_ms = d2h;
         stats->launches += 1;   // pack kernel
     }
+    return MBS_PO_OK;
+}
+
+}  // namespace
+
+extern "C" int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
+                               double *M_accum, double *Mns_accum, mbs_po_stats *stats)
+{
+    return diffract_host(ctx, beams, nullptr, 0, 0.0, precision, M_accum, Mns_accum, stats);
+}
+
+extern "C" int mbs_po_diffract_multisize(mbs_po_ctx *ctx, const mbs_po_beams *beams,
+                                         const double *scales, int n_scales, double wave_index,
+                                         int precision, double *M_accum, double *Mns_accum,
+                                         mbs_po_stats *stats)
+{
+    if (!scales)
+        return fail(ctx, MBS_PO_EINVAL, "null scales");
+    return diffract_host(ctx, beams, scales, n_scales, wave_index, precision, M_accum, Mns_accum, stats);
+}
+
+extern "C" int mbs_po_stage_multisize(mbs_po_ctx *ctx, const mbs_po_beams *beams,
+                                      const double *scales, int n_scales, double wave_index,
+                                      mbs_po_staged **out)
+{
+    if (!ctx || !out || !scales)
+        return fail(ctx, MBS_PO_EINVAL, "null argument");
+    *out = nullptr;
+    mbs_po_staged *s = new mbs_po_staged();
+    int rc = stage_into(ctx, beams, s, ctx->stream, scales, n_scales, wave_index);
+    if (rc) {
+        staged_release(s);
+        delete s;
+        return rc;
+    }
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        staged_release(s);
+        delete s;
+        return cuda_fail(ctx, e, "stage sync");
+    }
+    *out = s;
+    return MBS_PO_OK;
+}
+
+extern "C" int mbs_po_staged_sets(const mbs_po_staged *s)
+{
+    return s ? s->n_sets : 0;
+}
+
+extern "C" int mbs_po_diffract_thetas(mbs_po_ctx *ctx, const mbs_po_beams *beams,
+                                      const double *theta_rad, int n, double *m11_out)
+{
+    if (!ctx || !beams || (n > 0 && (!theta_rad || !m11_out)) || n < 0)
+        return fail(ctx, MBS_PO_EINVAL, "bad arguments");
+    if (!ctx->has_grid || !ctx->has_wave)
+        return fail(ctx, MBS_PO_ESTATE, "grid and wave constants must be set first");
+    if (n == 0)
+        return validate(ctx, beams);
+    for (int i = 0; i < n; ++i)
+        m11_out[i] = 0.0;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = ctx->stream;
+    int rc = stage_into(ctx, beams, &ctx->host_staged, st);
+    if (rc)
+        return rc;
+    const mbs_po_staged &s = ctx->host_staged;
+    if (s.n_beams == 0 || s.n_orient == 0)
+        return MBS_PO_OK;
+    // zenith angles clamped off the poles (GpuDiffraction.cu:4856-4866)
+    constexpr double kPi = 3.14159265358979323846;
+    std::vector<double> tab(2 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        double th = theta_rad[i];
+        if (th <= 1e-14)
+            th = 1e-6;
+        else if (th >= kPi - 1e-14)
+            th = kPi - 1e-6;
+        tab[i] = std::sin(th);
+        tab[n + i] = std::cos(th);
+    }
+    const int nAz = ctx->grid.n_az;
+    const int64_t pairs = s.n_beams * nAz;
+    // chunks of about 64 (beam, azimuth) pairs per thread, at most 4096
+    int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(4096, pairs / (256 * 64)));
+    const int bpc = (int)((s.n_beams + chunks - 1) / chunks);
+    chunks = (s.n_beams + bpc - 1) / bpc;
+    double *buf = nullptr;
+    size_t cap = 0;
+    const size_t need = 2 * (size_t)n + (size_t)chunks * n + n;
+    if ((rc = ensure(ctx, buf, cap, need, "theta scan")))
+        return rc;
+    double *d_st = buf, *d_ct = buf + n, *part = buf + 2 * n, *d_m11 = part + (size_t)chunks * n;
+    cudaError_t e = cudaMemcpyAsync(buf, tab.data(), 2 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        po_thetas_kernel<<<dim3((unsigned)n, (unsigned)chunks), 256, 0, st>>>(
+            s.beams, s.verts, s.beam_off, s.weight, s.n_orient, s.n_beams, bpc, d_st, d_ct,
+            ctx->grid.sphi, ctx->grid.cphi, nAz, n, ctx->wc, part);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        po_thetas_sum_kernel<<<(n + 127) / 128, 128, 0, st>>>(part, (int)chunks, n, d_m11);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m11_out, d_m11, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    cudaFree(buf);
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "theta scan");
     return MBS_PO_OK;
 }
 
@@ -915,6 +1094,8 @@ extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_stag
     int rc = noalloc_scratch(ctx, &scratch);
     if (rc)
         return rc;
+    if (s->n_sets != 1)
+        return fail(ctx, MBS_PO_EINVAL, "multi-size staged batches use mbs_po_diffract_staged");
     const int nAz = ctx->grid.n_az, nT = ctx->grid.n_zen + 1;
     const int64_t G = (int64_t)nAz * nT;
     if (s->n_orient == 0 || s->n_beams == 0 || G == 0)
@@ -938,6 +1119,7 @@ extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_stag
     if (L.n_chunks > max_chunks) {
         L.orient_per_chunk = (s->n_orient + max_chunks - 1) / max_chunks;
         L.n_chunks = (s->n_orient + L.orient_per_chunk - 1) / L.orient_per_chunk;
+        L.chunks_per_set = L.n_chunks;
     }
     // Every partial entry of chunks [0, n_chunks) is written (not added) by
     // each call (first orientation of a chunk, polar rows), so the scratch
@@ -962,6 +1144,8 @@ extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_stag
     P.n_orient = s->n_orient;
     P.orient_per_chunk = L.orient_per_chunk;
     P.tiles_per_row = L.tiles_per_row;
+    P.orient_per_set = s->n_orient;
+    P.chunks_per_set = L.n_chunks;
     P.wc = ctx->wc;
     P.partial = scratch;
     P.partial_ns = ns ? scratch + plane * L.n_chunks : nullptr;

@@ -75,20 +75,54 @@ struct KParams {
     int n_orient;
     int orient_per_chunk;
     int tiles_per_row;
+    // Output sets (size instances of a multi-size batch): set s owns the
+    // orientations [s*orient_per_set, (s+1)*orient_per_set) and the chunks
+    // [s*chunks_per_set, (s+1)*chunks_per_set).  One set: the whole batch.
+    int orient_per_set;
+    int chunks_per_set;
     WaveConst wc;
     double *partial;           // [n_chunks][16][G]
     double *partial_ns;        // [n_chunks][16][G] or null
 };
 
+// Orientation range [o0, o1) of an orientation chunk; chunks never span
+// two output sets.
+__device__ __forceinline__ void chunk_range(const KParams &P, int chunk, int &o0, int &o1)
+{
+    const int set = chunk / P.chunks_per_set;
+    const int base = set * P.orient_per_set;
+    o0 = base + (chunk - set * P.chunks_per_set) * P.orient_per_chunk;
+    o1 = min(min(base + P.orient_per_set, P.n_orient), o0 + P.orient_per_chunk);
+}
+
 // ------------------------------------------------------------ pack kernel
 
+// Size scaling of a staged instance (multi-size scan): the reference's
+// ScalePreparedOrientation (TracerPOTotal.cpp:2682-2747) and the scaled
+// packing of pack_prepared_gpu_beam (GpuDiffraction.cu:281-357): vertex
+// coordinates and the beam centre times s, area times s^2, and the Jones
+// matrix re-phased from the unphased one,
+//   J_phased = sign * absorption(s) * J * exp(i k s path),
+//   absorption(s) = mean over absorption paths L of (L > DBL_EPSILON ?
+//                   exp(cAbs L s) : 1)   (GpuDiffraction.cu:257-271).
+struct ScaleParams {
+    const double *scales;       // [n_inst] or null (one instance, s = 1, no re-phasing)
+    const double *raw;          // [n_beams][MBS_PO_RAW_STRIDE]
+    const int64_t *abs_off;     // [n_beams+1] or null
+    const double *abs_paths;
+    double k_rephase;           // wave number of the re-phasing
+    double abs_coeff;
+};
+
 struct PackParams {
-    int64_t n_beams;
+    int64_t n_beams;            // beams of one instance
+    int64_t n_verts;            // vertices of one instance
     const int64_t *vert_off;
     const double *vx, *vy, *syx, *sxy;
     const uint8_t *eflags;
     const double *geom;
     const uint8_t *bflags;
+    ScaleParams sc;
     WaveConst wc;
     DevBeam *beams;
     DevVert *verts;
@@ -99,31 +133,53 @@ struct PackParams {
     int *status;   // set to 1 on a malformed beam
 };
 
-__device__ __forceinline__ double binom(int n, int k)
-{
-    double r = 1.0;
-    for (int i = 1; i <= k; ++i)
-        r = r * (n - k + i) / i;
-    return r;
-}
+// Binomial coefficients C(n, k), n, k <= 2 kMomentOrder (zero for k > n).
+__constant__ double kBinom[13][13] = {
+    {1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0, 2.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0, 3.0, 3.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0, 4.0, 6.0, 4.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0, 5.0, 10.0, 10.0, 5.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0, 6.0, 15.0, 20.0, 15.0, 6.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0, 7.0, 21.0, 35.0, 35.0, 21.0, 7.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0, 8.0, 28.0, 56.0, 70.0, 56.0, 28.0, 8.0, 1.0, 0.0, 0.0, 0.0, 0.0},
+    {1.0, 9.0, 36.0, 84.0, 126.0, 126.0, 84.0, 36.0, 9.0, 1.0, 0.0, 0.0, 0.0},
+    {1.0, 10.0, 45.0, 120.0, 210.0, 252.0, 210.0, 120.0, 45.0, 10.0, 1.0, 0.0, 0.0},
+    {1.0, 11.0, 55.0, 165.0, 330.0, 462.0, 462.0, 330.0, 165.0, 55.0, 11.0, 1.0, 0.0},
+    {1.0, 12.0, 66.0, 220.0, 495.0, 792.0, 924.0, 792.0, 495.0, 220.0, 66.0, 12.0, 1.0}};
 
+// Grid: x over the beams of one instance (+1 for the terminal vertex
+// offset), y = instance.  Instance i writes beams [i n_beams, (i+1) n_beams)
+// and vertices [i n_verts, (i+1) n_verts) of the record arrays.
 __global__ void po_pack_kernel(PackParams P)
 {
-    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b > P.n_beams)
+    const int64_t bl = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (bl > P.n_beams)
         return;
-    const int64_t v0 = P.vert_off[b];
-    P.vbeg[b] = (int32_t)v0;
-    if (b == P.n_beams)
+    const int inst = blockIdx.y;
+    const int64_t ob = (int64_t)inst * P.n_beams, ov = (int64_t)inst * P.n_verts;
+    const int64_t v0l = P.vert_off[bl];
+    P.vbeg[ob + bl] = (int32_t)(ov + v0l);
+    if (bl == P.n_beams)
         return;
-    const int nv = (int)(P.vert_off[b + 1] - v0);
+    const int64_t b = ob + bl;
+    const int64_t v0 = ov + v0l;
+    const int nv = (int)(P.vert_off[bl + 1] - v0l);
     if (nv < 3 || nv > kMaxNv) {
         atomicExch(P.status, 1);
         return;
     }
     const WaveConst &wc = P.wc;
     const double k = wc.k, kt = wc.k * kInvTwoPi;
-    const double *g = P.geom + b * MBS_PO_GEOM_STRIDE;
+    const double *g = P.geom + bl * MBS_PO_GEOM_STRIDE;
+    const double scl = P.sc.scales ? P.sc.scales[inst] : 1.0;
+    // scaled vertex coordinates (x s, y s)
+    double vx[kMaxNv], vy[kMaxNv];
+    for (int e = 0; e < nv; ++e) {
+        vx[e] = P.vx[v0l + e] * scl;
+        vy[e] = P.vy[v0l + e] * scl;
+    }
     DevBeam d;
     // a0 = bd.hor, b0 = bd.ver (GpuDiffraction.cu:301-302)
     d.a0 = g[MBS_PO_G_BD] * g[MBS_PO_G_HOR] + g[MBS_PO_G_BD + 1] * g[MBS_PO_G_HOR + 1]
@@ -133,40 +189,64 @@ __global__ void po_pack_kernel(PackParams P)
     for (int i = 0; i < 3; ++i) {
         d.h[i] = g[MBS_PO_G_HOR + i];
         d.v[i] = g[MBS_PO_G_VER + i];
-        d.c[i] = g[MBS_PO_G_CEN + i];
+        d.c[i] = g[MBS_PO_G_CEN + i] * scl;
     }
-    d.area = g[MBS_PO_G_AREA];
+    d.area = g[MBS_PO_G_AREA] * (scl * scl);
     for (int i = 0; i < 12; ++i)
         d.rot[i] = g[MBS_PO_G_NT + i];
-    for (int i = 0; i < 8; ++i)
-        d.jp[i] = g[MBS_PO_G_JP + i];
-    d.opath = g[MBS_PO_G_OPATH];
+    if (P.sc.scales) {
+        const double *raw = P.sc.raw + bl * MBS_PO_RAW_STRIDE;
+        double sn, cs;
+        sincos(P.sc.k_rephase * raw[MBS_PO_R_PATH] * scl, &sn, &cs);
+        double absorption = 1.0;
+        if (P.sc.abs_off) {
+            const int64_t a0 = P.sc.abs_off[bl], a1 = P.sc.abs_off[bl + 1];
+            if (a1 > a0) {
+                double sum = 0.0;
+                for (int64_t a = a0; a < a1; ++a) {
+                    const double path = P.sc.abs_paths[a];
+                    sum += (path > 2.220446049250313e-16) ? exp(P.sc.abs_coeff * path * scl) : 1.0;
+                }
+                absorption = sum / (double)(a1 - a0);
+            }
+        }
+        const double f = raw[MBS_PO_R_SIGN] * absorption;
+        for (int i = 0; i < 4; ++i) {
+            const double jr = raw[MBS_PO_R_J + 2 * i], ji = raw[MBS_PO_R_J + 2 * i + 1];
+            d.jp[2 * i] = f * (jr * cs - ji * sn);
+            d.jp[2 * i + 1] = f * (jr * sn + ji * cs);
+        }
+    } else {
+        for (int i = 0; i < 8; ++i)
+            d.jp[i] = g[MBS_PO_G_JP + i];
+    }
+    d.opath = g[MBS_PO_G_OPATH] * scl;
     d.vbeg = (int32_t)v0;
     d.nv = nv;
-    d.flags = P.bflags[b];
+    d.flags = P.bflags[bl];
     const bool internal = !(d.flags & MBS_PO_BEAM_EXTERNAL);
 
     // vertices: general records, phase coefficients, second moments
     double sxx = 0, sxy = 0, syy = 0, rmax2 = 0;
     const double nan = __longlong_as_double(0x7ff8000000000000LL);
     for (int e = 0; e < nv; ++e) {
-        const double x = P.vx[v0 + e], y = P.vy[v0 + e];
+        const double x = vx[e], y = vy[e];
         sxx += x * x; sxy += x * y; syy += y * y;
         rmax2 = fmax(rmax2, x * x + y * y);
-        const uint8_t f = P.eflags[v0 + e];
+        const uint8_t f = P.eflags[v0l + e];
         DevVert dv;
         dv.x = x;
         dv.y = y;
-        dv.syx = (f & MBS_PO_EDGE_VALID_X) ? P.syx[v0 + e] : nan;
-        dv.sxy = (f & MBS_PO_EDGE_VALID_Y) ? P.sxy[v0 + e] : nan;
+        dv.syx = (f & MBS_PO_EDGE_VALID_X) ? P.syx[v0l + e] : nan;
+        dv.sxy = (f & MBS_PO_EDGE_VALID_Y) ? P.sxy[v0l + e] : nan;
         P.verts[v0 + e] = dv;
         VertRec vr;
         vr.X = kt * (d.h[0] * x + d.v[0] * y) + (internal ? kt * d.c[0] : 0.0);
         vr.Y = kt * (d.h[1] * x + d.v[1] * y) + (internal ? kt * d.c[1] : 0.0);
         vr.pc = kt * (d.h[2] * x + d.v[2] * y) + (internal ? kt * d.c[2] : 0.0);
         vr.p0 = kt * (d.a0 * x + d.b0 * y);
-        vr.syx = (f & MBS_PO_EDGE_VALID_X) ? P.syx[v0 + e] : kInvalidSlope;
-        vr.sxy = (f & MBS_PO_EDGE_VALID_Y) ? P.sxy[v0 + e] : kInvalidSlope;
+        vr.syx = (f & MBS_PO_EDGE_VALID_X) ? P.syx[v0l + e] : kInvalidSlope;
+        vr.sxy = (f & MBS_PO_EDGE_VALID_Y) ? P.sxy[v0l + e] : kInvalidSlope;
         P.vrec[v0 + e] = vr;
     }
     // Small-phase candidates.  The reference's moment branch needs every
@@ -177,21 +257,17 @@ __global__ void po_pack_kernel(PackParams P)
     // apertures; candidates take the exact FP64 test.
     int ia = 0;
     for (int e = 1; e < nv; ++e) {
-        const double x = P.vx[v0 + e], y = P.vy[v0 + e];
-        if (x * x + y * y > P.vx[v0 + ia] * P.vx[v0 + ia] + P.vy[v0 + ia] * P.vy[v0 + ia])
+        if (vx[e] * vx[e] + vy[e] * vy[e] > vx[ia] * vx[ia] + vy[ia] * vy[ia])
             ia = e;
     }
-    const double xa = P.vx[v0 + ia], ya = P.vy[v0 + ia];
+    const double xa = vx[ia], ya = vy[ia];
     int ib = ia == 0 ? 1 : 0;
     for (int e = 0; e < nv; ++e) {
-        const double x = P.vx[v0 + e], y = P.vy[v0 + e];
-        const double xb = P.vx[v0 + ib], yb = P.vy[v0 + ib];
-        if (fabs(xa * y - ya * x) > fabs(xa * yb - ya * xb))
+        if (fabs(xa * vy[e] - ya * vx[e]) > fabs(xa * vy[ib] - ya * vx[ib]))
             ib = e;
     }
     const double slab_scale = k / (1.25 * kSmallPhase);
-    double slab[4] = {xa * slab_scale, ya * slab_scale,
-                      P.vx[v0 + ib] * slab_scale, P.vy[v0 + ib] * slab_scale};
+    double slab[4] = {xa * slab_scale, ya * slab_scale, vx[ib] * slab_scale, vy[ib] * slab_scale};
     (void)sxx; (void)sxy; (void)syy;
     d.sp_thr2 = 0.0;
     // FP32C near-forward zone: |q| rmax <= kNearPhase, so every vertex phase
@@ -234,21 +310,52 @@ __global__ void po_pack_kernel(PackParams P)
 
     // Polygon moments I(p,q) = integral of x^p y^q over the aperture, by
     // Green's theorem over the edges (exact for polygons), normalised by
-    // the signed area: c_pq = <x^p y^q> / (p! q!).
+    // the signed area: c_pq = <x^p y^q> / (p! q!).  Per edge (i -> j):
+    //   I(p,q) += p! q!/(p+q+2)! (x_i y_j - x_j y_i)
+    //             sum_{a<=p, c<=q} C(a+c, c) C(p+q-a-c, q-c) x_i^a x_j^(p-a) y_i^c y_j^(q-c)
     double *mom = P.moments + b * kNumMoments;
     double area2 = 0.0, minX = 1e300, maxX = -1e300, minY = 1e300, maxY = -1e300;
     for (int e = 0; e < nv; ++e) {
         const int en = (e + 1 < nv) ? e + 1 : 0;
-        area2 += P.vx[v0 + e] * P.vy[v0 + en] - P.vx[v0 + en] * P.vy[v0 + e];
-        minX = fmin(minX, P.vx[v0 + e]); maxX = fmax(maxX, P.vx[v0 + e]);
-        minY = fmin(minY, P.vy[v0 + e]); maxY = fmax(maxY, P.vy[v0 + e]);
+        area2 += vx[e] * vy[en] - vx[en] * vy[e];
+        minX = fmin(minX, vx[e]); maxX = fmax(maxX, vx[e]);
+        minY = fmin(minY, vy[e]); maxY = fmax(maxY, vy[e]);
     }
     const bool degenerate = fabs(area2) <= 0x1p-40 * fmax((maxX - minX) * (maxY - minY), 2.2250738585072014e-308);
-    int idx = 0;
     double fact[kMomentOrder + 3];
     fact[0] = 1.0;
     for (int i = 1; i < kMomentOrder + 3; ++i)
         fact[i] = fact[i - 1] * i;
+    double I[kNumMoments];
+    for (int i = 0; i < kNumMoments; ++i)
+        I[i] = 0.0;
+    if (!degenerate) {
+        for (int e = 0; e < nv; ++e) {
+            const int en = (e + 1 < nv) ? e + 1 : 0;
+            double pxi[kMomentOrder + 1], pxj[kMomentOrder + 1], pyi[kMomentOrder + 1], pyj[kMomentOrder + 1];
+            pxi[0] = pxj[0] = pyi[0] = pyj[0] = 1.0;
+            for (int a = 1; a <= kMomentOrder; ++a) {
+                pxi[a] = pxi[a - 1] * vx[e];
+                pxj[a] = pxj[a - 1] * vx[en];
+                pyi[a] = pyi[a - 1] * vy[e];
+                pyj[a] = pyj[a - 1] * vy[en];
+            }
+            const double cross = vx[e] * vy[en] - vx[en] * vy[e];
+            int idx = 0;
+            for (int n = 0; n <= kMomentOrder; ++n) {
+                for (int p = n; p >= 0; --p, ++idx) {
+                    const int q = n - p;
+                    double t = 0.0;
+                    for (int a = 0; a <= p; ++a)
+                        for (int c = 0; c <= q; ++c)
+                            t += kBinom[a + c][c] * kBinom[p + q - a - c][q - c]
+                               * pxi[a] * pxj[p - a] * pyi[c] * pyj[q - c];
+                    I[idx] += cross * t;
+                }
+            }
+        }
+    }
+    int idx = 0;
     for (int n = 0; n <= kMomentOrder; ++n) {
         for (int p = n; p >= 0; --p, ++idx) {
             const int q = n - p;
@@ -256,21 +363,8 @@ __global__ void po_pack_kernel(PackParams P)
                 mom[idx] = (n == 0) ? 1.0 : 0.0;
                 continue;
             }
-            double s = 0.0;
-            for (int e = 0; e < nv; ++e) {
-                const int en = (e + 1 < nv) ? e + 1 : 0;
-                const double xi = P.vx[v0 + e], yi = P.vy[v0 + e];
-                const double xj = P.vx[v0 + en], yj = P.vy[v0 + en];
-                const double cross = xi * yj - xj * yi;
-                double t = 0.0;
-                for (int a = 0; a <= p; ++a)
-                    for (int c = 0; c <= q; ++c)
-                        t += binom(a + c, c) * binom(p + q - a - c, q - c)
-                           * pow(xi, a) * pow(xj, p - a) * pow(yi, c) * pow(yj, q - c);
-                s += cross * t;
-            }
-            const double I = s * fact[p] * fact[q] / fact[p + q + 2];
-            mom[idx] = (I / (0.5 * area2)) / (fact[p] * fact[q]);
+            const double In = I[idx] * fact[p] * fact[q] / fact[p + q + 2];
+            mom[idx] = (In / (0.5 * area2)) / (fact[p] * fact[q]);
         }
     }
 }
@@ -314,8 +408,10 @@ __device__ __forceinline__ void dir_full(const KParams &P, int p, int t, DirFull
 
 // One beam's Jones contribution d[8] to one direction in FP64.  Returns
 // false when the reference would skip the beam (NaN integral).
+// `singular` = false drops nearly singular edges (|C_e| <= eps1) instead of
+// taking their stable quotient, the reference's singularCorrection = 0.
 __device__ __noinline__ bool beam_general(const DevBeam &g, const DevVert *gv, const DirFull &dc,
-                                          const WaveConst &wc, double *d)
+                                          const WaveConst &wc, double *d, bool singular = true)
 {
     const double k = wc.k;
     const double a_sin = -dc.cp * g.h[0] - dc.sp * g.h[1];
@@ -356,7 +452,7 @@ __device__ __noinline__ bool beam_general(const DevBeam &g, const DevVert *gv, c
                 const double inv = 1.0 / coef;
                 sr = fma(cn - cprev, inv, sr);
                 si = fma(sn - sprev, inv, si);
-            } else if (ac <= wc.eps1) {   // valid, nearly singular edge (NaN: invalid edge)
+            } else if (singular && ac <= wc.eps1) {   // valid, nearly singular edge (NaN: invalid edge)
                 const double delta = useX ? (v[en].x - v[e].x) : (v[en].y - v[e].y);
                 stable_edge(cprev, sprev, delta, coef, k, sr, si);
             }
@@ -827,8 +923,8 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
     const int p = blockIdx.x / P.tiles_per_row;
     const int tile = blockIdx.x - p * P.tiles_per_row;
     const int chunk = blockIdx.y;
-    const int o0 = chunk * P.orient_per_chunk;
-    const int o1 = min(P.n_orient, o0 + P.orient_per_chunk);
+    int o0, o1;
+    chunk_range(P, chunk, o0, o1);
     const double cp = P.cphi[p], sp = P.sphi[p];
     const T eps = (T)(kF32 ? P.wc.eps1_f32 : P.wc.eps1);
     T *rslot = rsm + threadIdx.x;
@@ -1016,8 +1112,8 @@ __global__ void __launch_bounds__(256) po_pole_kernel(KParams P, const int32_t *
     __shared__ double red[256];
     const int chunk = blockIdx.x;
     const int t = pole_rows[blockIdx.y];
-    const int o0 = chunk * P.orient_per_chunk;
-    const int o1 = min(P.n_orient, o0 + P.orient_per_chunk);
+    int o0, o1;
+    chunk_range(P, chunk, o0, o1);
     DirFull dc;
     dir_full(P, 0, t, dc);
     double M[16], Mn[NS ? 16 : 1];
@@ -1061,18 +1157,95 @@ __global__ void __launch_bounds__(256) po_pole_kernel(KParams P, const int32_t *
     }
 }
 
-// out[g*16+k] += sum_c partial[c][k][g], in chunk order (deterministic).
-__global__ void po_reduce_kernel(const double *__restrict__ partial, int n_chunks,
+// out[set][g*16+k] += sum_c partial[set chunks c][k][g], in chunk order
+// (deterministic).  Grid: x over 16 G, y = output set.
+__global__ void po_reduce_kernel(const double *__restrict__ partial, int chunks_per_set,
                                  int64_t G, double *__restrict__ out)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= G * 16)
         return;
+    const int set = blockIdx.y;
+    partial += (int64_t)set * chunks_per_set * 16 * G;
+    out += (int64_t)set * 16 * G;
     const int64_t k = i / G, g = i - k * G;
     double s = 0.0;
-    for (int c = 0; c < n_chunks; ++c)
+    for (int c = 0; c < chunks_per_set; ++c)
         s += partial[(int64_t)c * 16 * G + i];
     out[g * 16 + k] += s;
+}
+
+// ------------------------------------------------------------ theta scan
+// Incoherent, azimuth-summed M11 on a list of zenith angles (reference
+// theta_m11_kernel, GpuDiffraction.cu:1909-1956, called by DiffractThetasGpu
+// :4780-4970).  Grid: x = zenith point, y = beam chunk; the CTA strides over
+// (beam, azimuth bin) pairs of its chunk and sums in a fixed-order tree, so
+// out_partial[chunk][t] is deterministic.
+__global__ void __launch_bounds__(256) po_thetas_kernel(
+    const DevBeam *beams, const DevVert *verts, const int32_t *beam_off, const double *weight,
+    int n_orient, int64_t n_beams, int beams_per_chunk, const double *st, const double *ct,
+    const double *sphi, const double *cphi, int n_az, int n_points, WaveConst wc,
+    double *out_partial)
+{
+    __shared__ double red[256];
+    const int t = blockIdx.x;
+    const int64_t b0 = (int64_t)blockIdx.y * beams_per_chunk;
+    const int64_t b1 = min(n_beams, b0 + beams_per_chunk);
+    const int64_t pairs = (b1 - b0) * n_az;
+    double acc = 0.0;
+    for (int64_t i = threadIdx.x; i < pairs; i += blockDim.x) {
+        const int64_t b = b0 + i / n_az;
+        const int p = (int)(i - (b - b0) * n_az);
+        // orientation of beam b: last o with beam_off[o] <= b
+        int lo = 0, hi = n_orient;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (beam_off[mid] <= b) lo = mid; else hi = mid;
+        }
+        DirFull dc;
+        dc.st = st[t];
+        dc.ct = ct[t];
+        dc.cp = cphi[p];
+        dc.sp = sphi[p];
+        dc.dir[0] = dc.st * dc.cp;
+        dc.dir[1] = dc.st * dc.sp;
+        dc.dir[2] = -dc.ct;
+        dc.vf[0] = -dc.sp; dc.vf[1] = dc.cp; dc.vf[2] = 0.0;
+        cross3(dc.vf, dc.dir, dc.u);
+        const double l2 = dc.u[0] * dc.u[0] + dc.u[1] * dc.u[1] + dc.u[2] * dc.u[2];
+        const double il = (l2 > 1e-30) ? rsqrt(l2) : 1.0;
+        dc.vt[0] = dc.u[0] * il; dc.vt[1] = dc.u[1] * il; dc.vt[2] = dc.u[2] * il;
+        cross3(dc.vt, dc.dir, dc.w);
+        double d[8];
+        if (beam_general(beams[b], verts, dc, wc, d, false)) {
+            double e = 0.0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                e = fma(d[q], d[q], e);
+            acc += 0.5 * e * weight[lo] / (double)(n_az + 1);
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        out_partial[(size_t)blockIdx.y * n_points + t] = red[0];
+}
+
+// m11[t] = sum over chunks of partial[c][t], chunk order.
+__global__ void po_thetas_sum_kernel(const double *partial, int n_chunks, int n_points, double *m11)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_points)
+        return;
+    double s = 0.0;
+    for (int c = 0; c < n_chunks; ++c)
+        s += partial[(size_t)c * n_points + t];
+    m11[t] = s;
 }
 
 // --------------------------------------------------------- extinction

@@ -52,6 +52,13 @@ def lib() -> C.CDLL:
         L.mbs_po_set_variant.argtypes = [vp, C.c_int, C.c_int]
         L.mbs_po_diffract_staged_noalloc.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_void_p,
                                                      C.c_void_p]
+        L.mbs_po_diffract_multisize.argtypes = [vp, C.POINTER(abi.Beams), abi._dp, C.c_int,
+                                                C.c_double, C.c_int, abi._dp, abi._dp,
+                                                C.POINTER(abi.Stats)]
+        L.mbs_po_stage_multisize.argtypes = [vp, C.POINTER(abi.Beams), abi._dp, C.c_int,
+                                             C.c_double, C.POINTER(vp)]
+        L.mbs_po_staged_sets.argtypes = [vp]
+        L.mbs_po_diffract_thetas.argtypes = [vp, C.POINTER(abi.Beams), abi._dp, C.c_int, abi._dp]
         _lib = L
     return _lib
 
@@ -62,9 +69,10 @@ class Staged:
     def __init__(self, handler: "GpuHandlerPO", handle: C.c_void_p, batch: BeamBatch):
         self._h = handler
         self.handle = handle
-        self.n_orient = batch.n_orient
-        self.n_beams = batch.n_beams
-        self.n_verts = batch.n_verts
+        self.n_sets = int(lib().mbs_po_staged_sets(handle))
+        self.n_orient = batch.n_orient * self.n_sets
+        self.n_beams = batch.n_beams * self.n_sets
+        self.n_verts = batch.n_verts * self.n_sets
 
     def free(self) -> None:
         if self.handle:
@@ -128,6 +136,63 @@ class GpuHandlerPO:
             return False
         self._call(rc, "mbs_po_diffract")
         return True
+
+    # -- HandlerPO::HandleOrientationsToLocalGpuMultiK ----------------------
+    def handle_orientations_to_local_gpu_multik(self, prepared: BeamBatch, start: int, count: int,
+                                                scales, wave_index: float,
+                                                local_ms: list[np.ndarray] | np.ndarray,
+                                                precision: int = abi.FP64) -> bool:
+        """Adds the Mueller sums of orientations [start, start+count) at every
+        size factor in ``scales`` into ``local_ms[i]`` (reference
+        GpuDiffraction.cu:3956-4158).  The batch must carry the unphased
+        Jones records (traced with raw output).  Returns False where the
+        reference does (invalid beams)."""
+        if start < 0 or count < 0 or start > prepared.n_orient:
+            return False
+        sc = np.ascontiguousarray(np.asarray(scales, dtype=np.float64))
+        if count == 0 or len(sc) == 0:
+            return True
+        if len(local_ms) < len(sc):
+            return False
+        batch = prepared if (start == 0 and count >= prepared.n_orient) else prepared.select(start, count)
+        if batch.beam_raw is None:
+            raise ValueError("multi-size diffraction needs the unphased Jones records (beam_raw)")
+        shape = (self.grid.n_az, self.grid.n_zen + 1, 16)
+        out = np.zeros((len(sc),) + shape)
+        b = batch.as_c(with_raw=True)
+        rc = lib().mbs_po_diffract_multisize(self.ctx, C.byref(b), abi.ptr(sc, C.c_double), len(sc),
+                                             float(wave_index), precision,
+                                             abi.ptr(out, C.c_double), None,
+                                             C.byref(self.last_stats))
+        if rc == -2:
+            return False
+        self._call(rc, "mbs_po_diffract_multisize")
+        for i in range(len(sc)):
+            local_ms[i] += out[i]
+        return True
+
+    def stage_multisize(self, batch: BeamBatch, scales, wave_index: float = 0.0) -> "Staged":
+        sc = np.ascontiguousarray(np.asarray(scales, dtype=np.float64))
+        h = C.c_void_p()
+        b = batch.as_c(with_raw=True)
+        self._call(lib().mbs_po_stage_multisize(self.ctx, C.byref(b), abi.ptr(sc, C.c_double),
+                                                len(sc), float(wave_index), C.byref(h)),
+                   "mbs_po_stage_multisize")
+        return Staged(self, h, batch)
+
+    # -- HandlerPO::DiffractThetasGpu ----------------------------------------
+    def diffract_thetas_gpu(self, prepared: BeamBatch, theta_rads) -> np.ndarray | None:
+        """Incoherent azimuth-summed M11 at the given zenith angles (reference
+        GpuDiffraction.cu:4780-4970); None where the reference returns false."""
+        th = np.ascontiguousarray(np.asarray(theta_rads, dtype=np.float64))
+        out = np.zeros(len(th))
+        b = prepared.as_c(with_raw=False)
+        rc = lib().mbs_po_diffract_thetas(self.ctx, C.byref(b), abi.ptr(th, C.c_double), len(th),
+                                          abi.ptr(out, C.c_double))
+        if rc == -2:
+            return None
+        self._call(rc, "mbs_po_diffract_thetas")
+        return out
 
     # -- HandlerPO::SelectGpuOrientationBatchSize ---------------------------
     def select_gpu_orientation_batch_size(self, prepared: BeamBatch, start: int, max_count: int,

@@ -260,6 +260,66 @@ static bool diffract_range(HandlerPO &h, const ScatteringRange &sphere,
     return true;
 }
 
+// Size-scaled diffraction of prepared[start, start+count) at every factor of
+// `scales` in one call (mbs_po_diffract_multisize): Mueller sums added into
+// *Ms[i], the no-shadow sums into *Mns[i] when Mns is given.
+static bool diffract_scaled(HandlerPO &h, const ScatteringRange &sphere,
+                            const std::vector<PreparedOrientation> &prepared, int start,
+                            int count, const std::vector<double> &scales, double waveIndex,
+                            const std::vector<Arr2D *> &Ms, const std::vector<Arr2D *> *Mns,
+                            int device)
+{
+    const int nAz = sphere.nAzimuth, nZen = sphere.nZenith;
+    MbsPackedBeams packed;
+    std::string err;
+    const int prc = mbs_pack_prepared(prepared, start, count, true, packed, &err);
+    if (prc != MBS_PO_OK)
+        return false;   // reference: failMultiK("bad-edge-data")
+    const mbs_po_beams view = packed.view(true);
+    if (view.n_beams == 0)
+        return true;
+    if (!HandlerPOBoundary::Prepare(h, sphere, HandlerPOWaveAccess::Get(h, 0.0), device))
+        return false;
+    BoundaryContext &c = g_ctx;
+    const size_t plane = (size_t)nAz * (nZen + 1) * 16;
+    const size_t n = plane * scales.size();
+    c.M.assign(n, 0.0);
+    if (Mns)
+        c.Mns.assign(n, 0.0);
+    mbs_po_stats st;
+    std::memset(&st, 0, sizeof(st));
+    const int rc = mbs_po_diffract_multisize(c.ctx, &view, scales.data(), (int)scales.size(),
+                                             waveIndex, precision_from_env(), c.M.data(),
+                                             Mns ? c.Mns.data() : nullptr, &st);
+    if (rc == MBS_PO_EBEAM)
+        return false;
+    if (!report(rc, "multi-size diffraction"))
+        return false;
+    for (size_t s = 0; s < scales.size(); ++s)
+        for (int p = 0; p < nAz; ++p)
+            for (int t = 0; t <= nZen; ++t)
+            {
+                const size_t off = s * plane + ((size_t)p * (nZen + 1) + t) * 16;
+                double *cell = Ms[s]->RawCell(p, t);
+                for (int q = 0; q < 16; ++q)
+                    cell[q] += c.M[off + q];
+                if (Mns)
+                {
+                    double *cn = (*Mns)[s]->RawCell(p, t);
+                    for (int q = 0; q < 16; ++q)
+                        cn[q] += c.Mns[off + q];
+                }
+            }
+    if (env_is("MBS_GPU_TIMING", "1"))
+        std::fprintf(stderr,
+                     "GPU timing multik path=b200-%s orient=%d sizes=%zu beams=%lld nAz=%d nZen=%d "
+                     "h2d+stage=%.3fms kernels=%.3fms reduce=%.3fms\n",
+                     precision_from_env() == MBS_PO_FP32C ? "fp32c" : "fp64", view.n_orient,
+                     scales.size(), (long long)view.n_beams, nAz, nZen, st.h2d_ms, st.kernel_ms,
+                     st.reduce_ms);
+    return true;
+}
+
 bool HandlerPO::HandleOrientationsToLocalGpu(const std::vector<PreparedOrientation> &prepared,
                                              int start, int count, Arr2D &localM,
                                              Arr2D &localM_noshadow, double scale,
@@ -271,16 +331,12 @@ bool HandlerPO::HandleOrientationsToLocalGpu(const std::vector<PreparedOrientati
         return false;
     if (std::fabs(scale - 1.0) > 1e-15)
     {
-        std::vector<Arr2D> ms;
-        ms.emplace_back(m_sphere.nAzimuth + 1, m_sphere.nZenith + 1, 4, 4);
-        ms.back().ClearArr();
-        std::vector<double> scales(1, scale);
-        if (!HandleOrientationsToLocalGpuMultiK(prepared, start, count, scales, waveIndex, ms))
-            return false;
-        for (int p = 0; p < m_sphere.nAzimuth; ++p)
-            for (int t = 0; t <= m_sphere.nZenith; ++t)
-                localM.insert(p, t, ms[0](p, t));
-        return true;
+        // scaled packing (GpuDiffraction.cu:4323-4324): one size instance
+        const std::vector<double> scales(1, scale);
+        const std::vector<Arr2D *> Ms(1, &localM), Mns(1, &localM_noshadow);
+        return diffract_scaled(*this, m_sphere, prepared, start, count, scales,
+                               waveIndex > 0.0 ? waveIndex : 0.0, Ms,
+                               ComputeNoShadow() ? &Mns : nullptr, current_device());
     }
     return diffract_range(*this, m_sphere, prepared, start, count, localM, localM_noshadow,
                           ComputeNoShadow(), current_device());
@@ -302,13 +358,8 @@ bool HandlerPO::HandleOrientationsToLocalGpuOnDevice(
     cudaGetDevice(&saved);
     if (cudaSetDevice(device) != cudaSuccess)
         return false;
-    bool ok;
-    if (std::fabs(scale - 1.0) > 1e-15)
-        ok = HandleOrientationsToLocalGpu(prepared, start, count, localM, localM_noshadow,
-                                          scale, waveIndex);
-    else
-        ok = isCoh && diffract_range(*this, m_sphere, prepared, start, count, localM,
-                                     localM_noshadow, ComputeNoShadow(), device);
+    const bool ok = HandleOrientationsToLocalGpu(prepared, start, count, localM,
+                                                 localM_noshadow, scale, waveIndex);
     cudaSetDevice(saved);
     return ok;
 }
@@ -331,13 +382,28 @@ bool HandlerPO::HandleOrientationsToLocalGpuFftPhi(const std::vector<PreparedOri
                                         scale, waveIndex);
 }
 
-bool HandlerPO::HandleOrientationsToLocalGpuMultiK(const std::vector<PreparedOrientation> & /*prepared*/,
-                                                   int /*start*/, int /*count*/,
-                                                   const std::vector<double> & /*scales*/,
-                                                   double /*waveIndex*/,
-                                                   std::vector<Arr2D> & /*localMs*/)
+bool HandlerPO::HandleOrientationsToLocalGpuMultiK(const std::vector<PreparedOrientation> &prepared,
+                                                   int start, int count,
+                                                   const std::vector<double> &scales,
+                                                   double waveIndex,
+                                                   std::vector<Arr2D> &localMs)
 {
-    return false;
+    // Same refusals as the reference (GpuDiffraction.cu:3970-3975); the fused
+    // path is on by default here, MBS_GPU_MULTI_K_FULL=0 turns it off so the
+    // caller falls back to per-size calls.
+    if (env_is("MBS_GPU_MULTI_K_FULL", "0"))
+        return false;
+    if (!isCoh || ComputeNoShadow())
+        return false;
+    if (count <= 0 || scales.empty())
+        return true;
+    if (localMs.size() < scales.size() || start < 0 || start > (int)prepared.size())
+        return false;
+    std::vector<Arr2D *> Ms;
+    for (size_t s = 0; s < scales.size(); ++s)
+        Ms.push_back(&localMs[s]);
+    return diffract_scaled(*this, m_sphere, prepared, start, count, scales, waveIndex, Ms,
+                           nullptr, current_device());
 }
 
 bool HandlerPO::HandleOrientationsToLocalGpuFftPhiMultiK(
@@ -347,11 +413,28 @@ bool HandlerPO::HandleOrientationsToLocalGpuFftPhiMultiK(
     return HandleOrientationsToLocalGpuMultiK(prepared, start, count, scales, waveIndex, localMs);
 }
 
-bool HandlerPO::DiffractThetasGpu(const std::vector<PreparedOrientation> & /*prepared*/,
-                                  const double * /*theta_rads*/, int /*nPoints*/,
-                                  std::vector<double> & /*m11_out*/)
+bool HandlerPO::DiffractThetasGpu(const std::vector<PreparedOrientation> &prepared,
+                                  const double *theta_rads, int nPoints,
+                                  std::vector<double> &m11_out)
 {
-    return false;
+    if (nPoints <= 0)
+        return true;
+    if (prepared.empty() || m_sphere.nAzimuth <= 0)
+        return true;
+    MbsPackedBeams packed;
+    if (mbs_pack_prepared(prepared, 0, (int)prepared.size(), false, packed, nullptr) != MBS_PO_OK)
+        return false;
+    m11_out.assign(nPoints, 0.0);
+    const mbs_po_beams view = packed.view(false);
+    if (view.n_beams == 0)
+        return true;
+    if (!HandlerPOBoundary::Prepare(*this, m_sphere, HandlerPOWaveAccess::Get(*this, 0.0),
+                                    current_device()))
+        return false;
+    const int rc = mbs_po_diffract_thetas(g_ctx.ctx, &view, theta_rads, nPoints, m11_out.data());
+    if (rc == MBS_PO_EBEAM)
+        return false;
+    return report(rc, "theta scan");
 }
 
 int HandlerPO::SelectGpuOrientationBatchSize(const std::vector<PreparedOrientation> &prepared,

@@ -52,6 +52,8 @@ def _po_lib():
         _po.po_oracle_extinction.restype = C.c_double
         _po.po_oracle_phi_average.argtypes = [abi._dp, C.c_int, C.c_int, abi._dp, abi._dp,
                                               abi._dp, abi._dp, abi._dp]
+        _po.po_oracle_thetas_m11.argtypes = [C.POINTER(abi.Beams), C.POINTER(abi.Wave), C.c_int,
+                                             C.c_double, abi._dp, C.c_int, C.c_int, abi._dp]
     return _po
 
 
@@ -206,3 +208,63 @@ def ref_jones_kat(jones: np.ndarray, weights: np.ndarray):
     lib.mbs_ref_jones_kat(n, abi.ptr(jones, C.c_double), abi.ptr(weights, C.c_double),
                           abi.ptr(direct, C.c_double), abi.ptr(legacy, C.c_double))
     return direct, legacy
+
+
+def scale_batch(batch: BeamBatch, scale: float, wave_index: float, abs_coeff: float) -> BeamBatch:
+    """The batch of a particle `scale` times larger, restating the
+    reference's ScalePreparedOrientation (src/scattering/TracerPOTotal.cpp:
+    2682-2747): vertex coordinates, beam centre and optical path times s, area
+    times s^2, and J_phased rebuilt from the unphased Jones matrix,
+        J_phased = sign * absorption(s) * J * exp(i k s path),
+        absorption(s) = mean over paths L of (L > DBL_EPSILON ? exp(cAbs L s) : 1).
+    Needs the batch's raw records (beam_raw, abs_offsets, abs_paths)."""
+    if batch.beam_raw is None:
+        raise ValueError("scale_batch needs beam_raw")
+    s = float(scale)
+    out = batch.select(0, batch.n_orient)
+    out.vx = batch.vx * s
+    out.vy = batch.vy * s
+    g = batch.beam_geom.copy()
+    g[:, abi.G_CEN:abi.G_CEN + 3] *= s
+    g[:, abi.G_AREA] *= s * s
+    g[:, abi.G_OPATH] *= s
+    raw = batch.beam_raw
+    arg = wave_index * raw[:, abi.R_PATH] * s
+    cs, sn = np.cos(arg), np.sin(arg)
+    absorption = np.ones(batch.n_beams)
+    ao, ap = batch.abs_offsets, batch.abs_paths
+    if ao is not None and ap is not None and len(ap):
+        for b in range(batch.n_beams):
+            a0, a1 = int(ao[b]), int(ao[b + 1])
+            if a1 > a0:
+                L = ap[a0:a1]
+                absorption[b] = np.mean(np.where(L > np.finfo(float).eps, np.exp(abs_coeff * L * s), 1.0))
+    f = raw[:, abi.R_SIGN] * absorption
+    for i in range(4):
+        jr, ji = raw[:, abi.R_J + 2 * i], raw[:, abi.R_J + 2 * i + 1]
+        g[:, abi.G_JP + 2 * i] = f * (jr * cs - ji * sn)
+        g[:, abi.G_JP + 2 * i + 1] = f * (jr * sn + ji * cs)
+    out.beam_geom = np.ascontiguousarray(g)
+    return out
+
+
+def thetas_m11(batch: BeamBatch, grid_n_az: int, az_step: float, theta_rad, wave: abi.Wave,
+               singular: bool = False):
+    """Incoherent azimuth-summed M11 on a zenith list, restating
+    HandlerPO::DiffractThetasGpu and theta_m11_kernel (reference
+    src/cuda/GpuDiffraction.cu:1909-1956, 4780-4970) on the oracle's
+    per-beam Jones: sum_o w_o sum_beams sum_{p<n_az} 0.5 |d|^2 / (n_az + 1),
+    d with the GPU rotation convention (no 0.5 factor), zenith angles clamped
+    1e-6 off the poles, nearly singular edges dropped (singular=False, as the
+    reference does there) or given their stable quotient (singular=True)."""
+    th = np.asarray(theta_rad, dtype=np.float64).copy()
+    th = np.where(th <= 1e-14, 1e-6, np.where(th >= np.pi - 1e-14, np.pi - 1e-6, th))
+    L = _po_lib()
+    n = len(th)
+    out = np.zeros(n)
+    b = batch.as_c(with_raw=False)
+    w = wave
+    L.po_oracle_thetas_m11(C.byref(b), C.byref(w), grid_n_az, az_step,
+                           abi.ptr(np.ascontiguousarray(th), C.c_double), n,
+                           1 if singular else 0, abi.ptr(out, C.c_double))
+    return out

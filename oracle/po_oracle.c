@@ -107,7 +107,7 @@ static inline void stable_edge(double pr, double pi, double delta, double c,
  * else the edge sum over precomputed vertex phasors (HandlerPO.cpp:2675-2739). */
 static cplx aperture(const mbs_po_beams *b, int64_t v0, int nv, double A, double B,
                      const double *vc, const double *vs, double area,
-                     const mbs_po_wave *w)
+                     const mbs_po_wave *w, int singular)
 {
     const double k = w->wave_index;
     double fr, fi;
@@ -132,7 +132,7 @@ static cplx aperture(const mbs_po_beams *b, int64_t v0, int nv, double A, double
             const double inv = (fabs(Ci) > w->eps1) ? 1.0 / Ci : 0.0;
             sr += (vc[en] - vc[e]) * inv;
             si += (vs[en] - vs[e]) * inv;
-            if (fabs(Ci) <= w->eps1)
+            if (singular && fabs(Ci) <= w->eps1)
                 stable_edge(vc[e], vs[e], b->vx[v0 + en] - b->vx[v0 + e], Ci, k, &sr, &si);
         }
         const double invB = 1.0 / B;
@@ -150,7 +150,7 @@ static cplx aperture(const mbs_po_beams *b, int64_t v0, int nv, double A, double
             const double inv = (fabs(Ei) > w->eps1) ? 1.0 / Ei : 0.0;
             sr += (vc[en] - vc[e]) * inv;
             si += (vs[en] - vs[e]) * inv;
-            if (fabs(Ei) <= w->eps1)
+            if (singular && fabs(Ei) <= w->eps1)
                 stable_edge(vc[e], vs[e], b->vy[v0 + en] - b->vy[v0 + e], Ei, k, &sr, &si);
         }
         const double invNA = -1.0 / A;
@@ -262,7 +262,7 @@ static void orientation_jones(const mbs_po_beams *b, const mbs_po_grid *g,
                     const double arg = -k * (st[t] * (cp * cen[0] + sp * cen[1]) + ct[t] * (-cen[2]));
                     sincos(arg, &dp.im, &dp.re);
                 }
-                const cplx F = aperture(b, v0, nv, A, B, vc, vs, gm[MBS_PO_G_AREA], w);
+                const cplx F = aperture(b, v0, nv, A, B, vc, vs, gm[MBS_PO_G_AREA], w, 1);
                 if (isnan(F.re))
                     continue;
                 const double dir[3] = { st[t] * cp, st[t] * sp, -ct[t] };
@@ -558,4 +558,69 @@ int po_oracle_phi_average(const double *M, int n_az, int n_zen,
     if (asym)
         *asym = cs != 0.0 ? cg / cs : 0.0;
     return MBS_PO_OK;
+}
+
+int po_oracle_thetas_m11(const mbs_po_beams *b, const mbs_po_wave *w, int n_az, double az_step,
+                         const double *theta, int n, int singular, double *m11)
+{   /* theta_m11_kernel (GpuDiffraction.cu:1909-1956) over DiffractThetasGpu's
+       tables (:4780-4970): per beam and azimuth bin p < n_az the squared
+       norm of the GPU-convention Jones contribution (rotation without the
+       0.5, i.e. twice this file's); the reference drops nearly singular
+       edges there (singular = 0). */
+    const double k = w->wave_index;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int t = 0; t < n; ++t)
+    {
+        double st, ct, vc[32], vs[32], acc = 0.0;
+        sincos(theta[t], &st, &ct);
+        for (int o = 0; o < b->n_orient; ++o)
+        {
+            const double wo = b->orient_weight[o];
+            for (int64_t i = b->beam_offsets[o]; i < b->beam_offsets[o + 1]; ++i)
+            {
+                const int64_t v0 = b->vert_offsets[i];
+                const int nv = (int)(b->vert_offsets[i + 1] - v0);
+                const double *gm = b->beam_geom + (size_t)i * MBS_PO_GEOM_STRIDE;
+                const double *hor = gm + MBS_PO_G_HOR, *ver = gm + MBS_PO_G_VER;
+                const double *bd = gm + MBS_PO_G_BD, *cen = gm + MBS_PO_G_CEN;
+                const int external = (b->beam_flags[i] & MBS_PO_BEAM_EXTERNAL) != 0;
+                const double a0 = bd[0] * hor[0] + bd[1] * hor[1] + bd[2] * hor[2];
+                const double b0 = bd[0] * ver[0] + bd[1] * ver[1] + bd[2] * ver[2];
+                for (int p = 0; p < n_az; ++p)
+                {
+                    double sp, cp;
+                    sincos(p * az_step, &sp, &cp);
+                    const double a_sin = -cp * hor[0] - sp * hor[1], a_cos = hor[2];
+                    const double b_sin = -cp * ver[0] - sp * ver[1], b_cos = ver[2];
+                    const double A = st * a_sin + ct * a_cos + a0;
+                    const double B = st * b_sin + ct * b_cos + b0;
+                    for (int v = 0; v < nv; ++v)
+                    {
+                        const double x = b->vx[v0 + v], y = b->vy[v0 + v];
+                        sincos(k * (A * x + B * y), &vs[v], &vc[v]);
+                    }
+                    cplx dp = { 1.0, 0.0 };
+                    if (!external)
+                    {
+                        const double arg = -k * (st * (cp * cen[0] + sp * cen[1]) + ct * (-cen[2]));
+                        sincos(arg, &dp.im, &dp.re);
+                    }
+                    const cplx F = aperture(b, v0, nv, A, B, vc, vs, gm[MBS_PO_G_AREA], w, singular);
+                    if (isnan(F.re))
+                        continue;
+                    const double dir[3] = { st * cp, st * sp, -ct };
+                    const double vf[3] = { -sp, cp, 0.0 };
+                    double r[4], d[8];
+                    rotate_jones(gm, vf, dir, r);
+                    beam_jones(F, dp, r, gm + MBS_PO_G_JP, d);
+                    double e = 0.0;
+                    for (int q = 0; q < 8; ++q)
+                        e += d[q] * d[q];
+                    acc += 0.5 * (4.0 * e) * wo / (double)(n_az + 1);
+                }
+            }
+        }
+        m11[t] = acc;
+    }
+    return 0;
 }

@@ -49,6 +49,15 @@ int po_oracle_phi_average(const double *M, int n_az, int n_zen,
                           const double *theta, const double *dcos2pi,
                           double *rows, double *csca, double *asym);
 
+/* Incoherent azimuth-summed M11 on a zenith list (already clamped off the
+ * poles), the quantity of HandlerPO::DiffractThetasGpu (reference
+ * src/cuda/GpuDiffraction.cu:1909-1956, 4780-4970); m11[n] overwritten.
+ * singular = 0 drops nearly singular edges as that reference path does;
+ * 1 takes their stable quotient like the Mueller path. */
+int po_oracle_thetas_m11(const mbs_po_beams *b, const mbs_po_wave *w, int n_az,
+                         double az_step, const double *theta, int n, int singular,
+                         double *m11);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,8 +33,41 @@ def sobol_batch(cfg_key: str, n: int, seed: int = 42) -> B.BeamBatch:
     return B.trace(cfg, beta, gamma, w)
 
 
+# Absorbing column for the multi-size re-phasing (absorption paths present).
+HEX_COLUMN_ABSORBING_10x20 = B.ParticleConfig(particle_type=1, p=(20.0, 10.0), ri_re=1.3116,
+                                              ri_im=0.002, absorption=True, wavelength=0.532,
+                                              max_reflections=4)
+# configs[3] plate family: length 0.2 x diameter, traced at D = 10 um and
+# scaled (--particle 1 L D).
+PLATE_D10 = B.ParticleConfig(particle_type=1, p=(2.0, 10.0), ri_re=1.3116, ri_im=0.0,
+                             wavelength=0.532, max_reflections=4)
+
 CASES = {"hex40x100": HEX_COLUMN_40x100, "hex10x20": HEX_COLUMN_10x20,
-         "concave": CONCAVE_ABSORBING}
+         "concave": CONCAVE_ABSORBING, "hexabs10x20": HEX_COLUMN_ABSORBING_10x20,
+         "plate10": PLATE_D10}
+
+
+def size_scan_diameters(n: int = 16, d_min: float = 10.0, d_max: float = 200.0) -> np.ndarray:
+    """plate diameters log-spaced from d_min to d_max (um)."""
+    return np.geomspace(d_min, d_max, n)
+
+
+def size_scan_theta_deg() -> np.ndarray:
+    """configs[3] zenith grid: 0.05 deg steps over 0-10 deg (201 rows), then
+    0.5 deg steps over 10.5-180 deg (340 rows)."""
+    return np.concatenate([np.arange(201) * 0.05, 10.5 + np.arange(340) * 0.5])
+
+
+def single_beam_orientations(batch: B.BeamBatch) -> B.BeamBatch:
+    """Every beam of `batch` as an orientation of its own, with its original
+    orientation's weight: coherent and incoherent sums coincide there."""
+    out = batch.select(0, batch.n_orient)
+    w = np.repeat(batch.orient_weight, np.diff(batch.beam_offsets))
+    out.beam_offsets = np.arange(batch.n_beams + 1, dtype=np.int64)
+    out.orient_weight = np.ascontiguousarray(w, dtype=np.float64)
+    if getattr(out, "extinction_ot", None) is not None:
+        out.extinction_ot = None
+    return out
 
 
 def weighted_l2(Ma: np.ndarray, Mb: np.ndarray, grid: B.GridTables) -> float:

@@ -93,3 +93,48 @@ def test_phi_average_rows():
     np.testing.assert_allclose(rows[:, 0], 1.0)
     assert abs(csca - 4 * np.pi) < 1e-12
     assert abs(asym) < 1e-12
+
+
+@pytest.mark.parametrize("scale", [0.6, 2.3])
+def test_scale_batch_matches_direct_trace(scale):
+    """The multi-size rescaling (ScalePreparedOrientation restated in
+    oracle.scale_batch) equals tracing the particle at the scaled size with
+    the reference tracer: geometry scales exactly, and the re-phased,
+    re-absorbed Jones matrices agree up to the reference's fast_exp_im."""
+    import dataclasses
+    cfg = common.HEX_COLUMN_ABSORBING_10x20
+    bs, gs, _ = B.symmetry(cfg)
+    beta, gamma, w = B.sobol_orientations(4, bs, gs)
+    base = B.trace(cfg, beta, gamma, w)
+    big = dataclasses.replace(cfg, p=(cfg.p[0] * scale, cfg.p[1] * scale))
+    direct = B.trace(big, beta, gamma, w)
+    wave = B.wave(cfg)
+    assert base.abs_paths is not None and len(base.abs_paths) > 0
+    scaled = oracle.scale_batch(base, scale, wave.wave_index, wave.abs_coeff)
+    assert scaled.n_beams == direct.n_beams
+    np.testing.assert_allclose(scaled.vx, direct.vx, atol=1e-9 * scale * 20)
+    g = B.grid(0.0, 180.0, 8, 90)
+    M1 = oracle.po_diffract(scaled, g, wave)
+    M2 = oracle.po_diffract(direct, g, B.wave(big))
+    assert common.weighted_l2(M1, M2, g) < 1e-9
+
+
+def test_thetas_oracle_matches_reference_single_beam():
+    """DiffractThetasGpu's incoherent azimuth sum, pinned through orientations
+    of one beam each (coherent = incoherent there): per zenith row,
+    m11(t) = 4/(n_az+1) * sum_p M11_ref(p, t) with the reference's CPU
+    HandleBeamsToLocal (CPU rotation carries the 0.5 the GPU one omits).
+    The Mueller path takes the stable quotient of nearly singular edges, so
+    the pin runs the restatement with it on; the reference's theta scan
+    drops those edges (checked on the GPU against singular=False)."""
+    cfg = common.HEX_COLUMN_10x20
+    batch = common.single_beam_orientations(common.sobol_batch("hex10x20", 2))
+    spec = (0.0, 180.0, 12, 60)
+    g = B.grid(*spec)
+    wave = B.wave(cfg)
+    M_ref, _, _, _ = oracle.ref_batch(cfg, spec, batch)
+    th = g.theta[1:-1]          # off the poles (the clamp moves them by 1e-6 rad)
+    m11 = oracle.thetas_m11(batch, g.n_az, g.az_step, th, wave, singular=True)
+    want = 4.0 / (g.n_az + 1) * M_ref[:, 1:-1, 0].sum(axis=0)
+    # the reference evaluates sin/cos with its own polynomial (as above)
+    np.testing.assert_allclose(m11, want, rtol=1e-6)
