@@ -204,6 +204,21 @@ int mbs_po_staged_sets(const mbs_po_staged *staged);
 int mbs_po_diffract_thetas(mbs_po_ctx *ctx, const mbs_po_beams *beams,
                            const double *theta_rad, int n, double *m11_out);
 
+/* Post-step on the device: the azimuth-averaged rows of a Mueller grid held
+ * in device memory (M_dev, [n_az*(n_zen+1)*16], e.g. the accumulator of
+ * mbs_po_diffract_staged), as HandlerPOTotal::WriteMatricesToFile writes them
+ * (reference src/handler/HandlerPOTotal.cpp:49-96): per zenith row the mean
+ * over azimuth bins of M(p, t) L(2 az_p), az_p = -2 pi p / n_az, polar rows
+ * unrotated and projected (PoleMueller ApplyForward / ApplyBackward).
+ * rows_out[(n_zen+1)*16] (host).  Also the scattering cross-section
+ * C_sca = sum_t M11(t) dcos2pi(t) (dcos2pi[n_zen+1], host: the grid's
+ * Compute2PiDcos weights) and the asymmetry parameter
+ * g = sum_t cos(theta_t) M11(t) dcos2pi(t) / C_sca, which the reference does
+ * not compute.  Only (n_zen+1)*16 doubles cross PCIe instead of the grid. */
+int mbs_po_phi_average(mbs_po_ctx *ctx, const double *M_dev, const double *dcos2pi,
+                       double *rows_out, double *csca_out, double *asym_out,
+                       void *stream);
+
 /* Optical-theorem extinction per orientation on the device (weighted by the
  * orientation weight), written to cext_out[n_orient] (host).  Replaces
  * HandlerPO::ComputeForwardExtinctionOt (reference HandlerPO.cpp:1812-2009). */

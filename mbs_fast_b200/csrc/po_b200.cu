@@ -32,6 +32,7 @@ struct GridDev {
     double *st = nullptr, *ct = nullptr;      // [n_zen+1]
     double *sphi = nullptr, *cphi = nullptr;  // [n_az]
     double *vf = nullptr;                     // [n_az*(n_zen+1)*3]
+    double *theta = nullptr;                  // [n_zen+1] zenith angles
     int8_t *row_kind = nullptr;               // [n_zen+1]
     int32_t *pole_rows = nullptr;             // [n_pole]
     int n_pole = 0;
@@ -188,7 +189,7 @@ int validate(mbs_po_ctx *ctx, const mbs_po_beams *b)
 void grid_release(GridDev &d)
 {
     cudaFree(d.st); cudaFree(d.ct); cudaFree(d.sphi); cudaFree(d.cphi); cudaFree(d.vf);
-    cudaFree(d.row_kind); cudaFree(d.pole_rows);
+    cudaFree(d.row_kind); cudaFree(d.pole_rows); cudaFree(d.theta);
     d = GridDev();
 }
 
@@ -307,6 +308,8 @@ extern "C" int mbs_po_set_grid(mbs_po_ctx *ctx, const mbs_po_grid *g)
     CK(cudaMalloc((void **)&d.sphi, nAz * sizeof(double)), "cudaMalloc grid");
     CK(cudaMalloc((void **)&d.cphi, nAz * sizeof(double)), "cudaMalloc grid");
     CK(cudaMalloc((void **)&d.vf, nvf * sizeof(double)), "cudaMalloc grid");
+    CK(cudaMalloc((void **)&d.theta, nT * sizeof(double)), "cudaMalloc grid");
+    CK(cudaMemcpy(d.theta, g->theta, nT * sizeof(double), cudaMemcpyHostToDevice), "grid copy");
     CK(cudaMalloc((void **)&d.row_kind, nT * sizeof(int8_t)), "cudaMalloc grid");
     CK(cudaMalloc((void **)&d.pole_rows, std::max<size_t>(poles.size(), 1) * sizeof(int32_t)), "cudaMalloc grid");
     CK(cudaMemcpy(d.st, st.data(), nT * sizeof(double), cudaMemcpyHostToDevice), "grid copy");
@@ -874,6 +877,50 @@ extern "C" int mbs_po_stage_multisize(mbs_po_ctx *ctx, const mbs_po_beams *beams
 extern "C" int mbs_po_staged_sets(const mbs_po_staged *s)
 {
     return s ? s->n_sets : 0;
+}
+
+extern "C" int mbs_po_phi_average(mbs_po_ctx *ctx, const double *M_dev, const double *dcos2pi,
+                                  double *rows_out, double *csca_out, double *asym_out,
+                                  void *stream)
+{
+    if (!ctx || !M_dev || !dcos2pi || !rows_out)
+        return fail(ctx, MBS_PO_EINVAL, "null argument");
+    if (!ctx->has_grid)
+        return fail(ctx, MBS_PO_ESTATE, "grid must be set first");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const int nT = ctx->grid.n_zen + 1, nAz = ctx->grid.n_az;
+    cudaStream_t st = (cudaStream_t)stream;
+    double *buf = nullptr;
+    size_t cap = 0;
+    int rc;
+    // [dcos2pi nT][rows nT*16][C_sca, g]
+    if ((rc = ensure(ctx, buf, cap, (size_t)nT * 17 + 2, "azimuth average")))
+        return rc;
+    double *d_dc = buf, *d_rows = buf + nT, *d_out = d_rows + (size_t)nT * 16;
+    cudaError_t e = cudaMemcpyAsync(d_dc, dcos2pi, nT * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        po_phi_average_kernel<<<nT, 128, 0, st>>>(M_dev, nAz, nT, ctx->grid.theta, d_rows);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        po_csca_kernel<<<1, 256, 0, st>>>(d_rows, nT, ctx->grid.theta, d_dc, d_out);
+        e = cudaGetLastError();
+    }
+    double res[2] = {0.0, 0.0};
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(rows_out, d_rows, (size_t)nT * 16 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(res, d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    cudaFree(buf);
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "azimuth average");
+    if (csca_out)
+        *csca_out = res[0];
+    if (asym_out)
+        *asym_out = res[1];
+    return MBS_PO_OK;
 }
 
 extern "C" int mbs_po_diffract_thetas(mbs_po_ctx *ctx, const mbs_po_beams *beams,

@@ -22,6 +22,7 @@ namespace mbs {
 constexpr int kMaxNv = 31;              // BeamEdgeData::MAX_EDGES - 1 (Handler.h:374)
 constexpr double kSmallPhase = 1e-3;    // HandlerPO_fast.h:170
 constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double kPi = 3.14159265358979323846264338327950;
 constexpr double kInvTwoPi = 0.15915494309189533576888376337251;
 constexpr double kMagic52 = 6755399441055744.0;   // 1.5 * 2^52
 constexpr double kMagic29 = 805306368.0;          // 1.5 * 2^29 (ulp 2^-23)

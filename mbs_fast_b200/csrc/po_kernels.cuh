@@ -1175,6 +1175,104 @@ __global__ void po_reduce_kernel(const double *__restrict__ partial, int chunks_
     out[g * 16 + k] += s;
 }
 
+// ------------------------------------------------------- azimuth average
+// Per zenith row t the azimuth average of M(p, t) L(2 az_p), az_p = -p 2 pi / n_az
+// (L the Stokes rotation [1 0 0 0; 0 c s 0; 0 -s c 0; 0 0 0 1]), the polar
+// rows unrotated and projected (PoleMueller ApplyForward / ApplyBackward),
+// as HandlerPOTotal::WriteMatricesToFile writes them (reference
+// src/handler/HandlerPOTotal.cpp:49-96).  One CTA per row; threads stride
+// over azimuth bins, fixed-order tree sum (deterministic).  rows[t][16].
+__global__ void __launch_bounds__(128) po_phi_average_kernel(const double *__restrict__ M, int n_az,
+                                                            int n_t, const double *__restrict__ theta,
+                                                            double *__restrict__ rows)
+{
+    __shared__ double red[16][128];
+    const int t = blockIdx.x;
+    const double th = theta[t];
+    const double tol = 256.0 * 2.220446049250313e-16;   // PoleMueller angular tolerance
+    const bool fwd = fabs(th) <= tol;
+    const bool bwd = fabs(th - kPi) <= tol;
+    double S[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+        S[q] = 0.0;
+    for (int p = threadIdx.x; p < n_az; p += blockDim.x) {
+        const double *m = M + ((size_t)p * n_t + t) * 16;
+        if (fwd || bwd) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q)
+                S[q] += m[q];
+            continue;
+        }
+        double sn, c;
+        sincos(2.0 * (-p * (2.0 * kPi / n_az)), &sn, &c);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const double m0 = m[4 * r], m1 = m[4 * r + 1], m2 = m[4 * r + 2], m3 = m[4 * r + 3];
+            S[4 * r + 0] += m0;
+            S[4 * r + 1] += m1 * c - m2 * sn;
+            S[4 * r + 2] += m1 * sn + m2 * c;
+            S[4 * r + 3] += m3;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+        red[q][threadIdx.x] = S[q];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int q = 0; q < 16; ++q)
+                red[q][threadIdx.x] += red[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double R[16];
+        for (int q = 0; q < 16; ++q)
+            R[q] = red[q][0] / n_az;
+        if (fwd || bwd) {
+            const double M00 = R[0], M33 = R[15], M03 = R[3];
+            const double M11 = bwd ? 0.5 * (R[5] - R[10]) : 0.5 * (R[5] + R[10]);
+            for (int q = 0; q < 16; ++q)
+                R[q] = 0.0;
+            R[0] = M00; R[5] = M11; R[10] = bwd ? -M11 : M11; R[15] = M33;
+            R[3] = M03; R[12] = M03;
+        }
+        for (int q = 0; q < 16; ++q)
+            rows[(size_t)t * 16 + q] = R[q];
+    }
+}
+
+// Scattering cross-section sum_t M11(t) dcos2pi(t) and the asymmetry
+// parameter g = sum_t cos(theta_t) M11(t) dcos2pi(t) / that sum over the
+// averaged rows.  One CTA, fixed-order tree sum; out[0] = C_sca, out[1] = g.
+__global__ void __launch_bounds__(256) po_csca_kernel(const double *__restrict__ rows, int n_t,
+                                                     const double *__restrict__ theta,
+                                                     const double *__restrict__ dcos2pi,
+                                                     double *__restrict__ out)
+{
+    __shared__ double a[256], b[256];
+    double sa = 0.0, sb = 0.0;
+    for (int t = threadIdx.x; t < n_t; t += blockDim.x) {
+        const double v = rows[(size_t)t * 16] * dcos2pi[t];
+        sa += v;
+        sb += cos(theta[t]) * v;
+    }
+    a[threadIdx.x] = sa;
+    b[threadIdx.x] = sb;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            a[threadIdx.x] += a[threadIdx.x + w];
+            b[threadIdx.x] += b[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = a[0];
+        out[1] = a[0] != 0.0 ? b[0] / a[0] : 0.0;
+    }
+}
+
 // ------------------------------------------------------------ theta scan
 // Incoherent, azimuth-summed M11 on a list of zenith angles (reference
 // theta_m11_kernel, GpuDiffraction.cu:1909-1956, called by DiffractThetasGpu

@@ -59,6 +59,8 @@ def lib() -> C.CDLL:
                                              C.c_double, C.POINTER(vp)]
         L.mbs_po_staged_sets.argtypes = [vp]
         L.mbs_po_diffract_thetas.argtypes = [vp, C.POINTER(abi.Beams), abi._dp, C.c_int, abi._dp]
+        L.mbs_po_phi_average.argtypes = [vp, C.c_void_p, abi._dp, abi._dp, abi._dp, abi._dp,
+                                         C.c_void_p]
         _lib = L
     return _lib
 
@@ -193,6 +195,18 @@ class GpuHandlerPO:
             return None
         self._call(rc, "mbs_po_diffract_thetas")
         return out
+
+    # -- HandlerPOTotal::WriteMatricesToFile rows, on the device ----------------
+    def phi_average_gpu(self, m_dev_ptr: int, stream: int = 0):
+        """Azimuth-averaged rows [(n_zen+1), 16], C_sca and the asymmetry
+        parameter g of a device-resident Mueller grid."""
+        rows = np.zeros((self.grid.n_zen + 1, 16))
+        csca, g = C.c_double(), C.c_double()
+        dc = np.ascontiguousarray(self.grid.dcos2pi, dtype=np.float64)
+        self._call(lib().mbs_po_phi_average(self.ctx, C.c_void_p(m_dev_ptr), abi.ptr(dc, C.c_double),
+                                            abi.ptr(rows, C.c_double), C.byref(csca), C.byref(g),
+                                            C.c_void_p(stream)), "mbs_po_phi_average")
+        return rows, csca.value, g.value
 
     # -- HandlerPO::SelectGpuOrientationBatchSize ---------------------------
     def select_gpu_orientation_batch_size(self, prepared: BeamBatch, start: int, max_count: int,

@@ -175,3 +175,27 @@ def test_edge_cases(hex_case):
     M = h.new_mueller()
     assert not h.handle_orientations_to_local_gpu(bad, M)
     assert not M.any()
+
+
+def test_phi_average_on_device(hex_case):
+    """Azimuth-averaged rows, C_sca and g computed on the device from the
+    device accumulator equal the oracle's writer restatement on the copied grid."""
+    import torch
+    cfg, batch, grid, wave, h, M_ref, _ = hex_case
+    st = h.stage(batch)
+    dev = torch.zeros(grid.n_az * (grid.n_zen + 1) * 16, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    h.diffract_staged(st, dev.data_ptr(), precision=abi.FP64)
+    torch.cuda.synchronize()
+    rows, csca, g = h.phi_average_gpu(dev.data_ptr())
+    M = dev.cpu().numpy().reshape(grid.n_az, grid.n_zen + 1, 16)
+    want, csca_w, g_w = oracle.phi_average(M, grid)
+    scale = np.max(np.abs(want[:, 0]))
+    assert np.max(np.abs(rows - want)) <= 1e-13 * scale
+    assert abs(csca - csca_w) <= 1e-12 * abs(csca_w)
+    assert abs(g - g_w) <= 1e-12
+    # and against the oracle's own Mueller grid (parity of C_sca and g)
+    _, csca_o, g_o = oracle.phi_average(M_ref, grid)
+    assert abs(csca - csca_o) <= 1e-8 * abs(csca_o)
+    assert abs(g - g_o) <= 1e-8
+    st.free()
