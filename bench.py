@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=48, help="orientations in the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error reference")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="column", choices=["column", "proposal"],
+                    help="column: the headline line (default); proposal: the learned "
+                         "orientation proposal against plain Sobol at equal error")
     return ap.parse_args()
 
 
@@ -212,10 +215,80 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_proposal(args):
+    """Learned orientation proposal (FP32C, importance-weighted) against plain
+    Sobol (FP64) on the D=40 um, L=100 um column: errors of the backscattering rows
+    (170-179.5 deg) and of all rows at several orientation counts against a
+    65536-orientation plain FP64 reference, the power-law fit of error vs N,
+    and the projected wall time (host tracing + device diffraction, plus the
+    pilot and training for the proposal) to 1 % RMS relative M11 error."""
+    import torch
+    from mbs_fast_b200 import abi, beams as B, proposal as PR
+    from mbs_fast_b200.handler import GpuHandlerPO
+    torch.cuda.set_device(0)
+    cfg = B.ParticleConfig(particle_type=1, p=(100.0, 40.0), ri_re=1.3116, ri_im=1e-9,
+                           wavelength=0.532, max_reflections=4)
+    bs, gs, _ = B.symmetry(cfg)
+    grid = B.grid(0.0, 180.0, args.n_phi, 180)
+    h = GpuHandlerPO(grid, B.wave(cfg))
+    th = np.rad2deg(grid.theta)
+    regions = {"backscatter": (th >= 170) & (th < 179.5), "all": (th > 0.5) & (th < 179.5)}
+
+    def rows_of(u, v, w, prec):
+        t0 = time.perf_counter()
+        b = PR.orientation_sample_batch(cfg, u, v, w, bs, gs)
+        t1 = time.perf_counter()
+        r = PR.averaged_rows(h, b, prec)[0]
+        torch.cuda.synchronize()
+        return r, t1 - t0, time.perf_counter() - t1
+
+    ref, _, _ = rows_of(*PR.plain_sobol(65536, seed=4242), abi.FP64)
+    prop, r2, t_train = PR.train_proposal(h, cfg, 2048, rows_mask=regions["backscatter"])
+    Ns = [1024, 2048, 4096, 8192]
+    err = {m: {k: [] for k in regions} for m in ("plain_fp64", "learned_fp32c")}
+    tper = {"plain_fp64": [], "learned_fp32c": []}
+    for N in Ns:
+        acc = {m: {k: [] for k in regions} for m in err}
+        for seed in (1, 2):
+            for m, (u, v, w), prec in (("plain_fp64", PR.plain_sobol(N, seed=seed), abi.FP64),
+                                       ("learned_fp32c", prop.sample(N, seed=seed), abi.FP32C)):
+                r, tt, td = rows_of(u, v, w, prec)
+                tper[m].append((tt + td) / N)
+                for k, mask in regions.items():
+                    acc[m][k].append(PR.row_errors(r, ref, mask)["M11_rms_rel"])
+        for m in err:
+            for k in regions:
+                err[m][k].append(float(np.sqrt(np.mean(np.square(acc[m][k])))))
+    out = {"metric": "wall time to 1% RMS relative error of orientation-averaged M11",
+           "unit": "s", "higher_is_better": False, "impl": "b200", "n_gpus": 1,
+           "config": {"workload": "hexagonal column D=40um L=100um, 1 deg zenith rows x %d azimuth bins; learned "
+                                  "proposal (MLP 4-128-128-128-1, BF16 tensor-core training) on "
+                                  "the backscattering rows; 2 scrambles per N" % args.n_phi,
+                      "orientations": Ns, "reference_orientations": 65536},
+           "fit_r2": r2, "proposal_train_s": t_train, "errors": err,
+           "seconds_per_orientation": {m: float(np.median(v)) for m, v in tper.items()}}
+    proj = {}
+    for k in regions:
+        proj[k] = {}
+        for m in err:
+            b, a = np.polyfit(np.log(Ns), np.log(err[m][k]), 1)
+            n1 = float(np.exp((np.log(0.01) - a) / b)) if b < 0 else float("inf")
+            t = n1 * out["seconds_per_orientation"][m] + (t_train if m == "learned_fp32c" else 0.0)
+            proj[k][m] = {"slope": float(b), "orientations_to_1pct": n1, "wall_s": t}
+        proj[k]["speedup"] = proj[k]["plain_fp64"]["wall_s"] / proj[k]["learned_fp32c"]["wall_s"]
+    out["to_1pct"] = proj
+    out["value"] = proj["backscatter"]["learned_fp32c"]["wall_s"]
+    h.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "proposal":
+        run_proposal(args)
         return
     rank, world, local = dist_env()
     import torch

@@ -219,6 +219,15 @@ int mbs_po_phi_average(mbs_po_ctx *ctx, const double *M_dev, const double *dcos2
                        double *rows_out, double *csca_out, double *asym_out,
                        void *stream);
 
+/* Azimuth-averaged rows of every orientation alone (the per-orientation
+ * results the learned orientation proposal trains on; no counterpart in the
+ * reference): rows_out[n_orient][(n_zen+1)*16] (host, overwritten), each
+ * orientation's Mueller grid times its orientation weight, averaged over
+ * azimuth as mbs_po_phi_average does.  The batch runs in groups of
+ * orientations whose grids fit about 1 GiB of device memory. */
+int mbs_po_orientation_rows(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
+                            double *rows_out);
+
 /* Optical-theorem extinction per orientation on the device (weighted by the
  * orientation weight), written to cext_out[n_orient] (host).  Replaces
  * HandlerPO::ComputeForwardExtinctionOt (reference HandlerPO.cpp:1812-2009). */

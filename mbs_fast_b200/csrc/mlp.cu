@@ -1,0 +1,625 @@
+// mlp.cu — the learned orientation proposal network (include/mbs_mlp.h).
+//
+// 4 -> 128 -> 128 -> 128 -> 1 with erf GELU.  Every layer product runs on
+// the tensor cores as BF16 x BF16 -> FP32 (mma.sync m16n8k16, one 64 x 64
+// output tile per CTA, operands staged through shared memory with arbitrary
+// strides so transposed operands of the backward pass need no copies).  The
+// 128 -> 1 head is a per-sample dot product in FP32.  Master parameters,
+// gradients and Adam moments are FP32; the BF16 weight copies are refreshed
+// after every update.  All reductions (bias gradients, loss) run in a fixed
+// order, so training is bitwise repeatable for a given seed.
+#include "mbs_mlp.h"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace mlp {
+
+constexpr int kH = MBS_MLP_HIDDEN;   // 128
+constexpr int kIn = MBS_MLP_IN;      // 4
+constexpr int kInPad = 16;           // K of the first layer, padded for the MMA
+constexpr int kTile = 64;
+
+// Flat parameter offsets (include/mbs_mlp.h)
+constexpr int oW1 = 0, ob1 = oW1 + kH * kIn, oW2 = ob1 + kH, ob2 = oW2 + kH * kH;
+constexpr int oW3 = ob2 + kH, ob3 = oW3 + kH * kH, ow4 = ob3 + kH, ob4 = ow4 + kH;
+constexpr int kNParams = ob4 + 1;
+static_assert(kNParams == MBS_MLP_N_PARAMS, "parameter layout");
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ float gelu(float z)
+{
+    return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+}
+
+__device__ __forceinline__ float gelu_grad(float z)
+{
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f))
+         + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+// Logical matrix view: X[r][c] = p[r * sr + c * sc].
+struct Mat {
+    const bf16 *p;
+    long sr, sc;
+};
+
+enum { kModeFwd = 0, kModeBwd = 1, kModeF32 = 2 };
+
+struct GemmOut {
+    const float *bias;   // kModeFwd: [N]
+    const float *zin;    // kModeBwd: pre-activation of the layer below [M][ldo]
+    float *z;            // kModeFwd: pre-activation out
+    bf16 *h;             // kModeFwd: activation out; kModeBwd: gradient out
+    float *f;            // kModeF32: plain product out
+    int ldo;
+};
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// C[M][N] = A[M][K] B[K][N] with the epilogue of MODE.  Grid: x over N
+// tiles, y over M tiles; 128 threads = 2 x 2 warps of 32 x 32 outputs.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, Mat A, Mat B, GemmOut o)
+{
+    // [row][k] with a pad of 8 so the 32-bit fragment loads spread over banks
+    __shared__ __align__(16) bf16 sA[kTile][kInPad + 8];
+    __shared__ __align__(16) bf16 sB[kTile][kInPad + 8];
+    const int m0 = blockIdx.y * kTile, n0 = blockIdx.x * kTile;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                acc[i][j][q] = 0.f;
+    const bf16 zero = __float2bfloat16(0.f);
+    for (int k0 = 0; k0 < K; k0 += kInPad) {
+        for (int i = threadIdx.x; i < kTile * kInPad; i += blockDim.x) {
+            const int r = i >> 4, c = i & 15;
+            const int gk = k0 + c;
+            const int gm = m0 + r, gn = n0 + r;
+            sA[r][c] = (gm < M && gk < K) ? A.p[gm * A.sr + gk * A.sc] : zero;
+            sB[r][c] = (gn < N && gk < K) ? B.p[gk * B.sr + gn * B.sc] : zero;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+            const int rb = wm + mi * 16;
+            const uint32_t a0 = *reinterpret_cast<const uint32_t *>(&sA[rb + gid][tig * 2]);
+            const uint32_t a1 = *reinterpret_cast<const uint32_t *>(&sA[rb + gid + 8][tig * 2]);
+            const uint32_t a2 = *reinterpret_cast<const uint32_t *>(&sA[rb + gid][tig * 2 + 8]);
+            const uint32_t a3 = *reinterpret_cast<const uint32_t *>(&sA[rb + gid + 8][tig * 2 + 8]);
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) {
+                const int cb = wn + ni * 8;
+                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&sB[cb + gid][tig * 2]);
+                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&sB[cb + gid][tig * 2 + 8]);
+                mma_bf16(acc[mi][ni], a0, a1, a2, a3, b0, b1);
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = m0 + wm + mi * 16 + gid + (q >= 2 ? 8 : 0);
+                const int c = n0 + wn + ni * 8 + tig * 2 + (q & 1);
+                if (r >= M || c >= N)
+                    continue;
+                const long idx = (long)r * o.ldo + c;
+                const float v = acc[mi][ni][q];
+                if (MODE == kModeFwd) {
+                    const float z = v + o.bias[c];
+                    o.z[idx] = z;
+                    o.h[idx] = __float2bfloat16(gelu(z));
+                } else if (MODE == kModeBwd) {
+                    o.h[idx] = __float2bfloat16(v * gelu_grad(o.zin[idx]));
+                } else {
+                    o.f[idx] = v;
+                }
+            }
+}
+
+// X0[b][0..15] (BF16): the quaternion in columns 0..3, zeros elsewhere and
+// on padding rows.
+__global__ void k_input(const float *q, int n, int bpad, bf16 *x0)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= bpad * kInPad)
+        return;
+    const int b = i / kInPad, c = i - b * kInPad;
+    x0[i] = __float2bfloat16((b < n && c < kIn) ? q[b * kIn + c] : 0.f);
+}
+
+// y[b] = sum_j H3[b][j] w4[j] + b4: one warp per sample, fixed lane order.
+__global__ void k_head_fwd(const bf16 *h3, const float *params, int n, float *y)
+{
+    const int b = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= n)
+        return;
+    float s = 0.f;
+    for (int j = lane; j < kH; j += 32)
+        s = fmaf(__bfloat162float(h3[(long)b * kH + j]), params[ow4 + j], s);
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1)
+        s += __shfl_xor_sync(0xffffffffu, s, w);
+    if (lane == 0)
+        y[b] = s + params[ob4];
+}
+
+// dy[b] = 2 (y_b - t_b) / n (0 on padding rows);
+// dZ3[b][j] = dy_b w4[j] gelu'(Z3[b][j]).
+__global__ void k_head_bwd(const float *y, const float *t, int n, int bpad, const float *params,
+                           const float *z3, float *dy, bf16 *dz3)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= bpad * kH)
+        return;
+    const int b = i / kH, j = i - b * kH;
+    const float d = b < n ? 2.f * (y[b] - t[b]) / (float)n : 0.f;
+    if (j == 0)
+        dy[b] = d;
+    dz3[i] = __float2bfloat16(d * params[ow4 + j] * gelu_grad(z3[i]));
+}
+
+// Column sums of a [rows][cols] BF16 matrix, fixed row order: out[c].
+__global__ void k_colsum_bf16(const bf16 *x, int rows, int cols, float *out)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols)
+        return;
+    float s = 0.f;
+    for (int r = 0; r < rows; ++r)
+        s += __bfloat162float(x[(long)r * cols + c]);
+    out[c] = s;
+}
+
+// Head gradients: gw4[j] = sum_b dy_b H3[b][j] (j < 128), gb4 = sum_b dy_b.
+__global__ void k_head_grad(const float *dy, const bf16 *h3, int bpad, float *grad)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > kH)
+        return;
+    float s = 0.f;
+    for (int b = 0; b < bpad; ++b)
+        s += j < kH ? dy[b] * __bfloat162float(h3[(long)b * kH + j]) : dy[b];
+    grad[j < kH ? ow4 + j : ob4] = s;
+}
+
+// W1 gradient: the first kIn columns of the padded [128][16] product.
+__global__ void k_pack_w1_grad(const float *gw1p, float *grad)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kH * kIn)
+        return;
+    const int r = i / kIn, c = i - r * kIn;
+    grad[oW1 + i] = gw1p[r * kInPad + c];
+}
+
+// BF16 copies of the weights (W1 padded to [128][16]).
+__global__ void k_refresh(const float *params, bf16 *w1p, bf16 *w2, bf16 *w3)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kH * kInPad) {
+        const int r = i / kInPad, c = i - r * kInPad;
+        w1p[i] = __float2bfloat16(c < kIn ? params[oW1 + r * kIn + c] : 0.f);
+    }
+    if (i < kH * kH) {
+        w2[i] = __float2bfloat16(params[oW2 + i]);
+        w3[i] = __float2bfloat16(params[oW3 + i]);
+    }
+}
+
+__global__ void k_adam(float *p, const float *g, float *m, float *v, int n, float lr, float bc1,
+                       float bc2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float gi = g[i];
+    const float mi = 0.9f * m[i] + 0.1f * gi;
+    const float vi = 0.999f * v[i] + 0.001f * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
+}
+
+// Mean-squared loss of n samples, one CTA, fixed-order tree sum.
+__global__ void __launch_bounds__(256) k_loss(const float *y, const float *t, int n, float *out)
+{
+    __shared__ float red[256];
+    float s = 0.f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float d = y[i] - t[i];
+        s = fmaf(d, d, s);
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        *out = red[0] / (float)max(n, 1);
+}
+
+// q_b[i] = q[idx[i]], t_b[i] = t[idx[i]].
+__global__ void k_gather(const float *q, const float *t, const int *idx, int n, float *qb, float *tb)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int s = idx[i];
+    for (int c = 0; c < kIn; ++c)
+        qb[i * kIn + c] = q[s * kIn + c];
+    tb[i] = t[s];
+}
+
+inline int pad64(int n) { return (n + kTile - 1) / kTile * kTile; }
+
+}  // namespace mlp
+
+using namespace mlp;
+
+struct mbs_mlp {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    float *params = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
+    bf16 *w1p = nullptr, *w2 = nullptr, *w3 = nullptr;
+    int step = 0;
+    // activations for up to `cap` padded rows
+    int cap = 0;
+    bf16 *x0 = nullptr, *h1 = nullptr, *h2 = nullptr, *h3 = nullptr;
+    bf16 *dz1 = nullptr, *dz2 = nullptr, *dz3 = nullptr;
+    float *z1 = nullptr, *z2 = nullptr, *z3 = nullptr;
+    float *y = nullptr, *t = nullptr, *dy = nullptr, *q = nullptr;
+    float *gw1p = nullptr, *scalar = nullptr;
+};
+
+namespace {
+
+int mfail(mbs_mlp *net, int code, const std::string &msg)
+{
+    if (net)
+        net->err = msg;
+    return code;
+}
+
+#define MK(expr, where)                                                          \
+    do {                                                                         \
+        cudaError_t e_ = (expr);                                                 \
+        if (e_ != cudaSuccess)                                                   \
+            return mfail(net, -3, std::string(where) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+void free_acts(mbs_mlp *net)
+{
+    void *ps[] = {net->x0, net->h1, net->h2, net->h3, net->dz1, net->dz2, net->dz3, net->z1,
+                  net->z2, net->z3, net->y, net->t, net->dy, net->q};
+    for (void *p : ps)
+        cudaFree(p);
+    net->x0 = net->h1 = net->h2 = net->h3 = net->dz1 = net->dz2 = net->dz3 = nullptr;
+    net->z1 = net->z2 = net->z3 = net->y = net->t = net->dy = net->q = nullptr;
+    net->cap = 0;
+}
+
+int ensure_acts(mbs_mlp *net, int rows)
+{
+    const int need = pad64(std::max(rows, 1));
+    if (need <= net->cap)
+        return 0;
+    free_acts(net);
+    const size_t hb = (size_t)need * kH;
+    MK(cudaMalloc((void **)&net->x0, (size_t)need * kInPad * sizeof(bf16)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->h1, hb * sizeof(bf16)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->h2, hb * sizeof(bf16)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->h3, hb * sizeof(bf16)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->dz1, hb * sizeof(bf16)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->dz2, hb * sizeof(bf16)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->dz3, hb * sizeof(bf16)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->z1, hb * sizeof(float)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->z2, hb * sizeof(float)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->z3, hb * sizeof(float)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->y, need * sizeof(float)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->t, need * sizeof(float)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->dy, need * sizeof(float)), "cudaMalloc mlp");
+    MK(cudaMalloc((void **)&net->q, (size_t)need * kIn * sizeof(float)), "cudaMalloc mlp");
+    net->cap = need;
+    return 0;
+}
+
+dim3 tiles(int M, int N) { return dim3((N + kTile - 1) / kTile, (M + kTile - 1) / kTile); }
+
+// Forward pass of n samples already in net->q (device); train keeps the
+// pre-activations for the backward pass.
+int forward_dev(mbs_mlp *net, int n)
+{
+    const int bp = pad64(n);
+    cudaStream_t s = net->stream;
+    k_input<<<(bp * kInPad + 255) / 256, 256, 0, s>>>(net->q, n, bp, net->x0);
+    GemmOut o{};
+    o.ldo = kH;
+    o.bias = net->params + ob1; o.z = net->z1; o.h = net->h1;
+    k_gemm<kModeFwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kInPad, Mat{net->x0, kInPad, 1},
+                                                   Mat{net->w1p, 1, kInPad}, o);
+    o.bias = net->params + ob2; o.z = net->z2; o.h = net->h2;
+    k_gemm<kModeFwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kH, Mat{net->h1, kH, 1},
+                                                   Mat{net->w2, 1, kH}, o);
+    o.bias = net->params + ob3; o.z = net->z3; o.h = net->h3;
+    k_gemm<kModeFwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kH, Mat{net->h2, kH, 1},
+                                                   Mat{net->w3, 1, kH}, o);
+    k_head_fwd<<<(n + 7) / 8, 256, 0, s>>>(net->h3, net->params, n, net->y);
+    MK(cudaGetLastError(), "mlp forward launch");
+    return 0;
+}
+
+// Backward pass after forward_dev (targets in net->t): net->grad (flat).
+int backward_dev(mbs_mlp *net, int n)
+{
+    const int bp = pad64(n);
+    cudaStream_t s = net->stream;
+    k_head_bwd<<<(bp * kH + 255) / 256, 256, 0, s>>>(net->y, net->t, n, bp, net->params, net->z3,
+                                                     net->dy, net->dz3);
+    k_head_grad<<<1, 160, 0, s>>>(net->dy, net->h3, bp, net->grad);
+    GemmOut o{};
+    // layer 3: dW3 = dZ3^T H2, db3 = colsum dZ3, dZ2 = (dZ3 W3) * gelu'(Z2)
+    o.ldo = kH; o.f = net->grad + oW3;
+    k_gemm<kModeF32><<<tiles(kH, kH), 128, 0, s>>>(kH, kH, bp, Mat{net->dz3, 1, kH},
+                                                   Mat{net->h2, kH, 1}, o);
+    k_colsum_bf16<<<1, kH, 0, s>>>(net->dz3, bp, kH, net->grad + ob3);
+    o = GemmOut{}; o.ldo = kH; o.zin = net->z2; o.h = net->dz2;
+    k_gemm<kModeBwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kH, Mat{net->dz3, kH, 1},
+                                                   Mat{net->w3, kH, 1}, o);
+    // layer 2
+    o = GemmOut{}; o.ldo = kH; o.f = net->grad + oW2;
+    k_gemm<kModeF32><<<tiles(kH, kH), 128, 0, s>>>(kH, kH, bp, Mat{net->dz2, 1, kH},
+                                                   Mat{net->h1, kH, 1}, o);
+    k_colsum_bf16<<<1, kH, 0, s>>>(net->dz2, bp, kH, net->grad + ob2);
+    o = GemmOut{}; o.ldo = kH; o.zin = net->z1; o.h = net->dz1;
+    k_gemm<kModeBwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kH, Mat{net->dz2, kH, 1},
+                                                   Mat{net->w2, kH, 1}, o);
+    // layer 1
+    o = GemmOut{}; o.ldo = kInPad; o.f = net->gw1p;
+    k_gemm<kModeF32><<<tiles(kH, kInPad), 128, 0, s>>>(kH, kInPad, bp, Mat{net->dz1, 1, kH},
+                                                       Mat{net->x0, kInPad, 1}, o);
+    k_pack_w1_grad<<<(kH * kIn + 127) / 128, 128, 0, s>>>(net->gw1p, net->grad);
+    k_colsum_bf16<<<1, kH, 0, s>>>(net->dz1, bp, kH, net->grad + ob1);
+    MK(cudaGetLastError(), "mlp backward launch");
+    return 0;
+}
+
+int refresh(mbs_mlp *net)
+{
+    k_refresh<<<(kH * kH + 255) / 256, 256, 0, net->stream>>>(net->params, net->w1p, net->w2, net->w3);
+    MK(cudaGetLastError(), "mlp refresh launch");
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int mbs_mlp_create(mbs_mlp **out, int device, uint64_t seed)
+{
+    if (!out)
+        return -1;
+    *out = nullptr;
+    mbs_mlp *net = new mbs_mlp();
+    net->device = device;
+    auto bail = [&](int rc) { mbs_mlp_destroy(net); return rc; };
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(-3);
+    const size_t np = kNParams;
+    if (cudaMalloc((void **)&net->params, np * 4) || cudaMalloc((void **)&net->grad, np * 4)
+        || cudaMalloc((void **)&net->m, np * 4) || cudaMalloc((void **)&net->v, np * 4)
+        || cudaMalloc((void **)&net->w1p, kH * kInPad * sizeof(bf16))
+        || cudaMalloc((void **)&net->w2, kH * kH * sizeof(bf16))
+        || cudaMalloc((void **)&net->w3, kH * kH * sizeof(bf16))
+        || cudaMalloc((void **)&net->gw1p, kH * kInPad * 4) || cudaMalloc((void **)&net->scalar, 16))
+        return bail(-4);
+    // uniform +-sqrt(6 / fan_in) weights, zero biases
+    std::vector<float> p(np, 0.f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int off, int count, int fan_in) {
+        std::uniform_real_distribution<float> u(-std::sqrt(6.f / fan_in), std::sqrt(6.f / fan_in));
+        for (int i = 0; i < count; ++i)
+            p[off + i] = u(rng);
+    };
+    fill(oW1, kH * kIn, kIn);
+    fill(oW2, kH * kH, kH);
+    fill(oW3, kH * kH, kH);
+    fill(ow4, kH, kH);
+    const int rc = mbs_mlp_set_params(net, p.data());
+    if (rc)
+        return bail(rc);
+    *out = net;
+    return 0;
+}
+
+extern "C" int mbs_mlp_destroy(mbs_mlp *net)
+{
+    if (!net)
+        return -1;
+    cudaSetDevice(net->device);
+    free_acts(net);
+    void *ps[] = {net->params, net->grad, net->m, net->v, net->w1p, net->w2, net->w3, net->gw1p,
+                  net->scalar};
+    for (void *p : ps)
+        cudaFree(p);
+    if (net->stream)
+        cudaStreamDestroy(net->stream);
+    delete net;
+    return 0;
+}
+
+extern "C" const char *mbs_mlp_last_error(const mbs_mlp *net)
+{
+    return net ? net->err.c_str() : "null network";
+}
+
+extern "C" int mbs_mlp_get_params(mbs_mlp *net, float *params)
+{
+    if (!net || !params)
+        return mfail(net, -1, "null argument");
+    MK(cudaSetDevice(net->device), "cudaSetDevice");
+    MK(cudaMemcpyAsync(params, net->params, kNParams * 4, cudaMemcpyDeviceToHost, net->stream), "D2H params");
+    MK(cudaStreamSynchronize(net->stream), "sync");
+    return 0;
+}
+
+extern "C" int mbs_mlp_set_params(mbs_mlp *net, const float *params)
+{
+    if (!net || !params)
+        return mfail(net, -1, "null argument");
+    MK(cudaSetDevice(net->device), "cudaSetDevice");
+    MK(cudaMemcpyAsync(net->params, params, kNParams * 4, cudaMemcpyHostToDevice, net->stream), "H2D params");
+    MK(cudaMemsetAsync(net->m, 0, kNParams * 4, net->stream), "memset");
+    MK(cudaMemsetAsync(net->v, 0, kNParams * 4, net->stream), "memset");
+    net->step = 0;
+    int rc = refresh(net);
+    if (rc)
+        return rc;
+    MK(cudaStreamSynchronize(net->stream), "sync");
+    return 0;
+}
+
+extern "C" int mbs_mlp_forward(mbs_mlp *net, const float *q, int n, float *y)
+{
+    if (!net || n < 0 || (n > 0 && (!q || !y)))
+        return mfail(net, -1, "bad arguments");
+    if (n == 0)
+        return 0;
+    MK(cudaSetDevice(net->device), "cudaSetDevice");
+    int rc = ensure_acts(net, n);
+    if (rc)
+        return rc;
+    MK(cudaMemcpyAsync(net->q, q, (size_t)n * kIn * 4, cudaMemcpyHostToDevice, net->stream), "H2D q");
+    if ((rc = forward_dev(net, n)))
+        return rc;
+    MK(cudaMemcpyAsync(y, net->y, (size_t)n * 4, cudaMemcpyDeviceToHost, net->stream), "D2H y");
+    MK(cudaStreamSynchronize(net->stream), "sync");
+    return 0;
+}
+
+extern "C" int mbs_mlp_loss_grad(mbs_mlp *net, const float *q, const float *t, int n, float *loss,
+                                 float *grad)
+{
+    if (!net || n <= 0 || !q || !t)
+        return mfail(net, -1, "bad arguments");
+    MK(cudaSetDevice(net->device), "cudaSetDevice");
+    int rc = ensure_acts(net, n);
+    if (rc)
+        return rc;
+    MK(cudaMemcpyAsync(net->q, q, (size_t)n * kIn * 4, cudaMemcpyHostToDevice, net->stream), "H2D q");
+    MK(cudaMemcpyAsync(net->t, t, (size_t)n * 4, cudaMemcpyHostToDevice, net->stream), "H2D t");
+    if ((rc = forward_dev(net, n)) || (rc = backward_dev(net, n)))
+        return rc;
+    k_loss<<<1, 256, 0, net->stream>>>(net->y, net->t, n, net->scalar);
+    MK(cudaGetLastError(), "loss launch");
+    float l = 0.f;
+    MK(cudaMemcpyAsync(&l, net->scalar, 4, cudaMemcpyDeviceToHost, net->stream), "D2H loss");
+    if (grad)
+        MK(cudaMemcpyAsync(grad, net->grad, kNParams * 4, cudaMemcpyDeviceToHost, net->stream), "D2H grad");
+    MK(cudaStreamSynchronize(net->stream), "sync");
+    if (loss)
+        *loss = l;
+    return 0;
+}
+
+extern "C" int mbs_mlp_train(mbs_mlp *net, const float *q, const float *t, int n, int epochs,
+                             int batch, float lr, uint64_t seed, float *final_loss)
+{
+    if (!net || n <= 0 || !q || !t || epochs < 0 || batch <= 0 || !(lr > 0.f))
+        return mfail(net, -1, "bad arguments");
+    MK(cudaSetDevice(net->device), "cudaSetDevice");
+    batch = std::min(batch, n);
+    int rc = ensure_acts(net, std::max(batch, n));
+    if (rc)
+        return rc;
+    cudaStream_t s = net->stream;
+    float *dq = nullptr, *dt = nullptr;
+    int *didx = nullptr;
+    auto cleanup = [&]() { cudaFree(dq); cudaFree(dt); cudaFree(didx); };
+    if (cudaMalloc((void **)&dq, (size_t)n * kIn * 4) || cudaMalloc((void **)&dt, (size_t)n * 4)
+        || cudaMalloc((void **)&didx, (size_t)epochs * n * 4 + 4)) {
+        cleanup();
+        return mfail(net, -4, "cudaMalloc training set");
+    }
+    // the shuffled order of every epoch, uploaded once
+    std::vector<int> order((size_t)epochs * n);
+    std::mt19937_64 rng(seed);
+    std::vector<int> perm(n);
+    for (int e = 0; e < epochs; ++e) {
+        for (int i = 0; i < n; ++i)
+            perm[i] = i;
+        std::shuffle(perm.begin(), perm.end(), rng);
+        std::copy(perm.begin(), perm.end(), order.begin() + (size_t)e * n);
+    }
+    cudaError_t e = cudaMemcpyAsync(dq, q, (size_t)n * kIn * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dt, t, (size_t)n * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && epochs > 0)
+        e = cudaMemcpyAsync(didx, order.data(), order.size() * 4, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        cleanup();
+        return mfail(net, -3, std::string("training upload: ") + cudaGetErrorString(e));
+    }
+    for (int ep = 0; ep < epochs && rc == 0; ++ep) {
+        for (int b0 = 0; b0 < n && rc == 0; b0 += batch) {
+            const int nb = std::min(batch, n - b0);
+            k_gather<<<(nb + 127) / 128, 128, 0, s>>>(dq, dt, didx + (size_t)ep * n + b0, nb, net->q, net->t);
+            if ((rc = forward_dev(net, nb)) || (rc = backward_dev(net, nb)))
+                break;
+            ++net->step;
+            const float bc1 = 1.f - std::pow(0.9f, (float)net->step);
+            const float bc2 = 1.f - std::pow(0.999f, (float)net->step);
+            k_adam<<<(kNParams + 255) / 256, 256, 0, s>>>(net->params, net->grad, net->m, net->v,
+                                                          kNParams, lr, bc1, bc2);
+            rc = refresh(net);
+        }
+    }
+    if (rc == 0 && final_loss) {
+        // loss over the whole set with the trained parameters
+        e = cudaMemcpyAsync(net->q, dq, (size_t)n * kIn * 4, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(net->t, dt, (size_t)n * 4, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess && (rc = forward_dev(net, n)) == 0) {
+            k_loss<<<1, 256, 0, s>>>(net->y, net->t, n, net->scalar);
+            e = cudaMemcpyAsync(final_loss, net->scalar, 4, cudaMemcpyDeviceToHost, s);
+        }
+    }
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    cleanup();
+    if (rc)
+        return rc;
+    if (e != cudaSuccess)
+        return mfail(net, -3, std::string("training: ") + cudaGetErrorString(e));
+    return 0;
+}

@@ -923,6 +923,96 @@ extern "C" int mbs_po_phi_average(mbs_po_ctx *ctx, const double *M_dev, const do
     return MBS_PO_OK;
 }
 
+extern "C" int mbs_po_orientation_rows(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
+                                       double *rows_out)
+{
+    if (!ctx || !beams || (beams->n_orient > 0 && !rows_out))
+        return fail(ctx, MBS_PO_EINVAL, "null argument");
+    if (!ctx->has_grid || !ctx->has_wave)
+        return fail(ctx, MBS_PO_ESTATE, "grid and wave constants must be set first");
+    int rc = validate(ctx, beams);
+    if (rc)
+        return rc;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const int nO = beams->n_orient, nT = ctx->grid.n_zen + 1, nAz = ctx->grid.n_az;
+    const size_t plane = (size_t)nAz * nT * 16;
+    const size_t nrow = (size_t)nT * 16;
+    std::memset(rows_out, 0, sizeof(double) * nrow * nO);
+    if (nO == 0 || beams->n_beams == 0)
+        return MBS_PO_OK;
+    // orientation groups: one Mueller grid per orientation, about 1 GiB of
+    // grids per group
+    const int group = (int)std::max<size_t>(
+        1, std::min<size_t>(std::min<size_t>(nO, 16384), ((size_t)1 << 27) / plane));
+    double *grids = nullptr, *drows = nullptr;
+    size_t gcap = 0, rcap = 0;
+    if ((rc = ensure(ctx, grids, gcap, plane * group, "orientation grids")))
+        return rc;
+    if ((rc = ensure(ctx, drows, rcap, nrow * group, "orientation rows"))) {
+        cudaFree(grids);
+        return rc;
+    }
+    cudaStream_t st = ctx->stream;
+    std::vector<int64_t> boff, voff;
+    for (int o0 = 0; o0 < nO && rc == 0; o0 += group) {
+        const int n = std::min(group, nO - o0);
+        // the sub-batch [o0, o0+n) with rebased offsets
+        const int64_t b0 = beams->beam_offsets[o0], b1 = beams->beam_offsets[o0 + n];
+        const int64_t v0 = beams->vert_offsets[b0], v1 = beams->vert_offsets[b1];
+        boff.resize(n + 1);
+        for (int o = 0; o <= n; ++o)
+            boff[o] = beams->beam_offsets[o0 + o] - b0;
+        voff.resize(b1 - b0 + 1);
+        for (int64_t b = b0; b <= b1; ++b)
+            voff[b - b0] = beams->vert_offsets[b] - v0;
+        mbs_po_beams sub = *beams;
+        sub.n_orient = n;
+        sub.n_beams = b1 - b0;
+        sub.n_verts = v1 - v0;
+        sub.beam_offsets = boff.data();
+        sub.orient_weight = beams->orient_weight + o0;
+        sub.vert_offsets = voff.data();
+        sub.vx = beams->vx + v0;
+        sub.vy = beams->vy + v0;
+        sub.slope_yx = beams->slope_yx + v0;
+        sub.slope_xy = beams->slope_xy + v0;
+        sub.edge_flags = beams->edge_flags + v0;
+        sub.beam_geom = beams->beam_geom + b0 * MBS_PO_GEOM_STRIDE;
+        sub.beam_flags = beams->beam_flags + b0;
+        sub.beam_raw = nullptr;
+        sub.abs_offsets = nullptr;
+        sub.abs_paths = nullptr;
+        if ((rc = stage_into(ctx, &sub, &ctx->host_staged, st)))
+            break;
+        if (sub.n_beams == 0)
+            continue;
+        // every orientation its own output set
+        ctx->host_staged.n_sets = n;
+        ctx->host_staged.orient_per_set = 1;
+        cudaError_t e = cudaMemsetAsync(grids, 0, plane * n * sizeof(double), st);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(ctx, e, "memset grids");
+            break;
+        }
+        if ((rc = run_diffract(ctx, &ctx->host_staged, precision, grids, nullptr, st, nullptr)))
+            break;
+        po_phi_average_kernel<<<dim3((unsigned)nT, (unsigned)n), 128, 0, st>>>(grids, nAz, nT,
+                                                                               ctx->grid.theta, drows);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(rows_out + nrow * o0, drows, nrow * n * sizeof(double),
+                                cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+            rc = cuda_fail(ctx, e, "orientation rows");
+    }
+    ctx->host_staged.n_sets = 1;
+    cudaFree(grids);
+    cudaFree(drows);
+    return rc;
+}
+
 extern "C" int mbs_po_diffract_thetas(mbs_po_ctx *ctx, const mbs_po_beams *beams,
                                       const double *theta_rad, int n, double *m11_out)
 {

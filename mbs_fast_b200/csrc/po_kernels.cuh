@@ -1180,14 +1180,18 @@ __global__ void po_reduce_kernel(const double *__restrict__ partial, int chunks_
 // (L the Stokes rotation [1 0 0 0; 0 c s 0; 0 -s c 0; 0 0 0 1]), the polar
 // rows unrotated and projected (PoleMueller ApplyForward / ApplyBackward),
 // as HandlerPOTotal::WriteMatricesToFile writes them (reference
-// src/handler/HandlerPOTotal.cpp:49-96).  One CTA per row; threads stride
-// over azimuth bins, fixed-order tree sum (deterministic).  rows[t][16].
+// src/handler/HandlerPOTotal.cpp:49-96).  One CTA per row (grid y: one
+// Mueller grid after another); threads stride over azimuth bins, fixed-order
+// tree sum (deterministic).  rows[y][t][16].
 __global__ void __launch_bounds__(128) po_phi_average_kernel(const double *__restrict__ M, int n_az,
                                                             int n_t, const double *__restrict__ theta,
                                                             double *__restrict__ rows)
 {
     __shared__ double red[16][128];
     const int t = blockIdx.x;
+    // y: independent grids (one per orientation for per-orientation rows)
+    M += (size_t)blockIdx.y * n_az * n_t * 16;
+    rows += (size_t)blockIdx.y * n_t * 16;
     const double th = theta[t];
     const double tol = 256.0 * 2.220446049250313e-16;   // PoleMueller angular tolerance
     const bool fwd = fabs(th) <= tol;

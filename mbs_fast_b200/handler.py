@@ -61,6 +61,7 @@ def lib() -> C.CDLL:
         L.mbs_po_diffract_thetas.argtypes = [vp, C.POINTER(abi.Beams), abi._dp, C.c_int, abi._dp]
         L.mbs_po_phi_average.argtypes = [vp, C.c_void_p, abi._dp, abi._dp, abi._dp, abi._dp,
                                          C.c_void_p]
+        L.mbs_po_orientation_rows.argtypes = [vp, C.POINTER(abi.Beams), C.c_int, abi._dp]
         _lib = L
     return _lib
 
@@ -207,6 +208,16 @@ class GpuHandlerPO:
                                             abi.ptr(rows, C.c_double), C.byref(csca), C.byref(g),
                                             C.c_void_p(stream)), "mbs_po_phi_average")
         return rows, csca.value, g.value
+
+    def orientation_rows(self, batch: BeamBatch, precision: int = abi.FP64) -> np.ndarray:
+        """Azimuth-averaged rows of every orientation alone (times its
+        weight): [n_orient, n_zen+1, 16]."""
+        out = np.zeros((batch.n_orient, self.grid.n_zen + 1, 16))
+        b = batch.as_c(with_raw=False)
+        self._call(lib().mbs_po_orientation_rows(self.ctx, C.byref(b), precision,
+                                                 abi.ptr(out, C.c_double)),
+                   "mbs_po_orientation_rows")
+        return out
 
     # -- HandlerPO::SelectGpuOrientationBatchSize ---------------------------
     def select_gpu_orientation_batch_size(self, prepared: BeamBatch, start: int, max_count: int,

@@ -1,8 +1,8 @@
 """Shared cases and error measures for the tests.
 
 Particle cases follow the reference's configurations and tests:
-  HEX_COLUMN_40x100   configs[1] particle (--particle 1 100 40, m=1.3116+1e-9i)
-  HEX_COLUMN_10x20    configs[0] particle (--particle 1 20 10, m=1.3116)
+  HEX_COLUMN_40x100   orientation-averaged column (--particle 1 100 40, m=1.3116+1e-9i)
+  HEX_COLUMN_10x20    fixed-orientation column (--particle 1 20 10, m=1.3116)
   CONCAVE_ABSORBING   the CUDA release-gate particle of the reference
                       (tests/run_cuda_release_gate.sh:31-44: --particle 10 1.0
                       0.7 43.4114540493, m=1.3116+0.01i, --absorption,
@@ -37,7 +37,7 @@ def sobol_batch(cfg_key: str, n: int, seed: int = 42) -> B.BeamBatch:
 HEX_COLUMN_ABSORBING_10x20 = B.ParticleConfig(particle_type=1, p=(20.0, 10.0), ri_re=1.3116,
                                               ri_im=0.002, absorption=True, wavelength=0.532,
                                               max_reflections=4)
-# configs[3] plate family: length 0.2 x diameter, traced at D = 10 um and
+# Size-scan plate family: length 0.2 x diameter, traced at D = 10 um and
 # scaled (--particle 1 L D).
 PLATE_D10 = B.ParticleConfig(particle_type=1, p=(2.0, 10.0), ri_re=1.3116, ri_im=0.0,
                              wavelength=0.532, max_reflections=4)
@@ -48,12 +48,12 @@ CASES = {"hex40x100": HEX_COLUMN_40x100, "hex10x20": HEX_COLUMN_10x20,
 
 
 def size_scan_diameters(n: int = 16, d_min: float = 10.0, d_max: float = 200.0) -> np.ndarray:
-    """plate diameters log-spaced from d_min to d_max (um)."""
+    """Size scan: plate diameters log-spaced from d_min to d_max (um)."""
     return np.geomspace(d_min, d_max, n)
 
 
 def size_scan_theta_deg() -> np.ndarray:
-    """configs[3] zenith grid: 0.05 deg steps over 0-10 deg (201 rows), then
+    """Size-scan zenith grid: 0.05 deg steps over 0-10 deg (201 rows), then
     0.5 deg steps over 10.5-180 deg (340 rows)."""
     return np.concatenate([np.arange(201) * 0.05, 10.5 + np.arange(340) * 0.5])
 

@@ -97,7 +97,7 @@ def test_multisize_rejects_missing_raw(absorbing):
 
 
 def test_size_scan_plates_nonuniform_grid():
-    """configs[3] shape at reduced orientation and azimuth counts: 16 plates
+    """The size scan at reduced orientation and azimuth counts: 16 plates
     (L = 0.2 D, D log-spaced 10-200 um) from one trace at D = 10 um, the
     non-uniform zenith grid (0.05 deg to 10 deg, 0.5 deg beyond), all sizes in
     one launch; sizes 0, 7 and 15 checked against the oracle."""

@@ -71,7 +71,8 @@ def test_producer_batch_is_lossless():
 
 
 def test_fixed_orientation_reference_paths_agree():
-    """the reference's fixed path HandleBeams and the prepared
+    """Fixed orientation (column 10x20 um at beta=30, gamma=15 deg): the
+    reference's fixed path HandleBeams and the prepared
     path HandleBeamsToLocal give the same Mueller grid (both cutoffs are 0)."""
     cfg = common.HEX_COLUMN_10x20
     grid = (0.0, 180.0, 36, 120)

@@ -128,7 +128,7 @@ def test_release_gate_particle():
 
 
 def test_fixed_orientation_config0():
-    """hexagonal column 10x20 um at beta=30, gamma=15 deg, grid
+    """Fixed orientation: hexagonal column 10x20 um at beta=30, gamma=15 deg, grid
     theta 0..180 in 0.25 deg x phi 0..360 in 2 deg, against the reference's
     fixed-orientation path HandleBeams."""
     cfg = common.HEX_COLUMN_10x20
