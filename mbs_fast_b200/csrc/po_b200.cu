@@ -46,8 +46,8 @@ struct GridDev {
 struct Variant {
     int tpb, dpt, minb;
 };
-constexpr Variant kVariantsF32[] = {{128, 2, 4}, {96, 2, 5}, {96, 1, 8}, {128, 2, 3},
-                                    {128, 1, 4}, {128, 4, 2}, {64, 4, 4}, {96, 4, 2}};
+constexpr Variant kVariantsF32[] = {{128, 2, 4}, {128, 2, 3}, {128, 1, 4}, {128, 1, 5},
+                                    {128, 1, 6}, {96, 2, 5}, {128, 4, 2}, {256, 1, 2}};
 constexpr Variant kVariantsF64[] = {{128, 1, 4}, {128, 2, 3}, {128, 1, 3}};
 constexpr int kNumVariantsF32 = sizeof(kVariantsF32) / sizeof(Variant);
 constexpr int kNumVariantsF64 = sizeof(kVariantsF64) / sizeof(Variant);
@@ -94,7 +94,7 @@ struct mbs_po_ctx {
     double *hres = nullptr;      // pinned [2][G*16]
     size_t hres_cap = 0;
     Arena raw;                   // raw upload area for staging
-    int *d_status = nullptr;
+    int *d_status = nullptr;      // [0] pack status, [1] work counter of the diffraction kernel
     mbs_po_staged host_staged;   // reused by mbs_po_diffract
     cudaEvent_t ev[8] = {};
     int variant[2] = {0, 0};     // chosen launch shape per precision
@@ -217,7 +217,7 @@ extern "C" int mbs_po_create(mbs_po_ctx **out, int device)
     for (int i = 0; i < 8 && e == cudaSuccess; ++i)
         e = cudaEventCreate(&ctx->ev[i]);
     if (e == cudaSuccess)
-        e = cudaMalloc((void **)&ctx->d_status, sizeof(int));
+        e = cudaMalloc((void **)&ctx->d_status, 64);
     if (e != cudaSuccess) {
         delete ctx;
         return MBS_PO_ECUDA;
@@ -503,9 +503,10 @@ struct LaunchPlan {
     int tiles_per_row, n_chunks, orient_per_chunk, chunks_per_set;
 };
 
-// Orientation chunks per output set: about six waves of CTAs over the
-// whole launch, at most 64 chunks per set (each chunk owns a partial plane).
-// n_orient is per set; n_chunks counts all sets.
+// Orientation chunks per output set: enough work items (chunk x azimuth x
+// zenith tile) for about 32 per resident CTA of the persistent kernel, so
+// the last items leave little tail; at most 64 chunks per set (each chunk
+// owns a partial plane).  n_orient is per set; n_chunks counts all sets.
 LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ctas_per_sm,
                        int n_sets = 1)
 {
@@ -520,7 +521,7 @@ LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ct
             sms = v;
     }
     n_sets = std::max(1, n_sets);
-    const long long target = (long long)sms * ctas_per_sm * 6;   // ~6 waves
+    const long long target = (long long)sms * ctas_per_sm * 32;
     long long chunks = (target + ctas_per_chunk * n_sets - 1) / (ctas_per_chunk * n_sets);
     chunks = std::max<long long>(1, std::min<long long>(chunks, std::max(1, n_orient)));
     chunks = std::min<long long>(chunks, 64);
@@ -531,42 +532,49 @@ LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ct
     return L;
 }
 
+// Persistent launch: as many CTAs as fit on the device at once (at most one
+// per work item); P.work must be zero on `st` when the kernel starts.
 template <typename T, int TPB, int DPT, bool NS, int MINB>
-cudaError_t launch_one(const KParams &P, dim3 grid, cudaStream_t st)
+cudaError_t launch_one(const KParams &P, cudaStream_t st)
 {
     auto kern = po_diffract_kernel<T, TPB, DPT, NS, MINB>;
     const size_t smem = diffract_smem_bytes<T, TPB, DPT, NS>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
         return e;
-    kern<<<grid, TPB, smem, st>>>(P);
+    int dev = 0, sms = 148, per_sm = 1;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess
+        || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess
+        || (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TPB, smem)) != cudaSuccess)
+        return e;
+    const int ctas = std::max(1, std::min(P.n_items, sms * std::max(per_sm, 1)));
+    kern<<<ctas, TPB, smem, st>>>(P);
     return cudaGetLastError();
 }
 
 // No-shadow sums use the default shape of each precision.
-cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &P, dim3 grid,
-                            cudaStream_t st)
+cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &P, cudaStream_t st)
 {
     if (precision == MBS_PO_FP64) {
         if (ns)
-            return launch_one<double, 128, 1, true, 4>(P, grid, st);
+            return launch_one<double, 128, 1, true, 4>(P, st);
         switch (variant) {
-        case 1: return launch_one<double, 128, 2, false, 3>(P, grid, st);
-        case 2: return launch_one<double, 128, 1, false, 3>(P, grid, st);
-        default: return launch_one<double, 128, 1, false, 4>(P, grid, st);
+        case 1: return launch_one<double, 128, 2, false, 3>(P, st);
+        case 2: return launch_one<double, 128, 1, false, 3>(P, st);
+        default: return launch_one<double, 128, 1, false, 4>(P, st);
         }
     }
     if (ns)
-        return launch_one<float, 128, 2, true, 4>(P, grid, st);
+        return launch_one<float, 128, 2, true, 4>(P, st);
     switch (variant) {
-    case 1: return launch_one<float, 96, 2, false, 5>(P, grid, st);
-    case 2: return launch_one<float, 96, 1, false, 8>(P, grid, st);
-    case 3: return launch_one<float, 128, 2, false, 3>(P, grid, st);
-    case 4: return launch_one<float, 128, 1, false, 4>(P, grid, st);
-    case 5: return launch_one<float, 128, 4, false, 2>(P, grid, st);
-    case 6: return launch_one<float, 64, 4, false, 4>(P, grid, st);
-    case 7: return launch_one<float, 96, 4, false, 2>(P, grid, st);
-    default: return launch_one<float, 128, 2, false, 4>(P, grid, st);
+    case 1: return launch_one<float, 128, 2, false, 3>(P, st);
+    case 2: return launch_one<float, 128, 1, false, 4>(P, st);
+    case 3: return launch_one<float, 128, 1, false, 5>(P, st);
+    case 4: return launch_one<float, 128, 1, false, 6>(P, st);
+    case 5: return launch_one<float, 96, 2, false, 5>(P, st);
+    case 6: return launch_one<float, 128, 4, false, 2>(P, st);
+    case 7: return launch_one<float, 256, 1, false, 2>(P, st);
+    default: return launch_one<float, 128, 2, false, 4>(P, st);
     }
 }
 
@@ -630,7 +638,8 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     P.wc = ctx->wc;
     P.partial = ctx->partial;
     P.partial_ns = ns ? ctx->partial + plane * L.n_chunks : nullptr;
-    dim3 grid((unsigned)(nAz * L.tiles_per_row), (unsigned)L.n_chunks);
+    P.work = ctx->d_status + 1;
+    P.n_items = L.n_chunks * nAz * L.tiles_per_row;
     int launches = 0;
     CK(cudaEventRecord(ctx->ev[0], st), "event");
     // polar rows on the side stream, concurrently with the main kernel
@@ -645,7 +654,8 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
         CK(cudaEventRecord(ctx->ev[6], ctx->side), "event");
         ++launches;
     }
-    const cudaError_t e = launch_diffract(precision, variant, ns, P, grid, st);
+    CK(cudaMemsetAsync(P.work, 0, sizeof(int), st), "memset work counter");
+    const cudaError_t e = launch_diffract(precision, variant, ns, P, st);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "diffraction kernel launch");
     ++launches;
@@ -1187,6 +1197,7 @@ namespace {
 
 constexpr size_t kNoAllocScratchBytes = MBS_PO_NOALLOC_SCRATCH_BYTES;
 constexpr size_t kNoAllocScratchDoubles = kNoAllocScratchBytes / sizeof(double);
+constexpr size_t kNoAllocHead = 32;   // work counter, 256 bytes
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
 
@@ -1240,8 +1251,11 @@ extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_stag
     const bool ns = Mns_dev != nullptr;
     const size_t plane = (size_t)16 * G;
     const size_t sets = ns ? 2 : 1;
+    // the first kNoAllocHead doubles hold the work counter of the kernel
+    int *work = reinterpret_cast<int *>(scratch);
+    scratch += kNoAllocHead;
     // one partial plane per orientation chunk (and per output set) must fit
-    if (plane * sets > kNoAllocScratchDoubles)
+    if (plane * sets > kNoAllocScratchDoubles - kNoAllocHead)
         return fail(ctx, MBS_PO_ERANGE,
                     "grid of " + std::to_string(G) + " directions needs "
                     + std::to_string(plane * sets * sizeof(double)) + " bytes of partials; the "
@@ -1252,7 +1266,7 @@ extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_stag
     const Variant V = pi == 0 ? kVariantsF64[variant] : kVariantsF32[variant];
     LaunchPlan L = plan_launch(nAz, nT, s->n_orient, V.tpb * V.dpt, V.minb);
     // fewer, larger orientation chunks when the fixed scratch is short
-    const int max_chunks = (int)std::min<size_t>(kNoAllocScratchDoubles / (plane * sets), 64);
+    const int max_chunks = (int)std::min<size_t>((kNoAllocScratchDoubles - kNoAllocHead) / (plane * sets), 64);
     if (L.n_chunks > max_chunks) {
         L.orient_per_chunk = (s->n_orient + max_chunks - 1) / max_chunks;
         L.n_chunks = (s->n_orient + L.orient_per_chunk - 1) / L.orient_per_chunk;
@@ -1286,8 +1300,9 @@ extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_stag
     P.wc = ctx->wc;
     P.partial = scratch;
     P.partial_ns = ns ? scratch + plane * L.n_chunks : nullptr;
+    P.work = work;
+    P.n_items = L.n_chunks * nAz * L.tiles_per_row;
     cudaStream_t st = (cudaStream_t)stream;
-    dim3 grid((unsigned)(nAz * L.tiles_per_row), (unsigned)L.n_chunks);
     if (ctx->grid.n_pole > 0) {
         CK(cudaEventRecord(ctx->ev[0], st), "event");
         CK(cudaStreamWaitEvent(ctx->side, ctx->ev[0], 0), "side wait");
@@ -1299,7 +1314,8 @@ extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_stag
         CK(cudaGetLastError(), "pole kernel launch");
         CK(cudaEventRecord(ctx->ev[6], ctx->side), "event");
     }
-    const cudaError_t e = launch_diffract(precision, variant, ns, P, grid, st);
+    CK(cudaMemsetAsync(work, 0, sizeof(int), st), "memset work counter");
+    const cudaError_t e = launch_diffract(precision, variant, ns, P, st);
     if (e != cudaSuccess)
         return cuda_fail(ctx, e, "diffraction kernel launch");
     if (ctx->grid.n_pole > 0)

@@ -80,6 +80,10 @@ struct KParams {
     // [s*chunks_per_set, (s+1)*chunks_per_set).  One set: the whole batch.
     int orient_per_set;
     int chunks_per_set;
+    // Work items (chunk, azimuth bin, zenith tile), chunk-major: the
+    // persistent CTAs of po_diffract_kernel take them in order from *work.
+    int *work;
+    int n_items;
     WaveConst wc;
     double *partial;           // [n_chunks][16][G]
     double *partial_ns;        // [n_chunks][16][G] or null
@@ -627,10 +631,14 @@ __device__ __forceinline__ void fill_beam(const BeamRec &r, double cp, double sp
                            __hiloint2double(vs, gbeam));
 }
 
+// FP32C: p0 carries the range-reduction constant 1.5*2^29 + 1/2, so the
+// phase sum st ps + ct pc + p0 lands directly in [2^29, 2^30), where the low
+// 23 mantissa bits hold frac(u + 1/2) (three roundings of at most 2^-24 turn).
 __device__ __forceinline__ void fill_vert(const VertRec &r, double cp, double sp, SVertRaw<float> &w)
 {
     w.q[0] = make_double2(-(cp * r.X + sp * r.Y), r.pc);
-    w.q[1] = make_double2(r.p0, __hiloint2double(__float_as_int((float)r.sxy), __float_as_int((float)r.syx)));
+    w.q[1] = make_double2(r.p0 + (kMagic29 + 0.5),
+                          __hiloint2double(__float_as_int((float)r.sxy), __float_as_int((float)r.syx)));
 }
 
 __device__ __forceinline__ void fill_vert(const VertRec &r, double cp, double sp, SVertRaw<double> &w)
@@ -721,20 +729,24 @@ __device__ __forceinline__ void load_vert(const SVertRaw<double> &w, VertRegs &v
     sxy = q2.x;
 }
 
-// Phasor (cos, sin) of 2 pi u.
-__device__ __forceinline__ void phasor(double u, double &s, double &c)
+// Vertex phasor (cos, sin) of 2 pi u, u = st ps + ct pc + p0 in turns.
+__device__ __forceinline__ void vertex_phasor(double st, double ct, const VertRegs &w, double &s,
+                                              double &c)
 {
-    sincos_turns(u, s, c);
+    sincos_turns(fma(st, w.ps, fma(ct, w.pc, w.p0)), s, c);
 }
 
-// FP32: fraction f of u in [-1/2, 1/2) to 2^-23 without an FP64->FP32
-// conversion (1.5*2^29 + 1/2 added in FP64 leaves frac(u + 1/2) in the low
-// 23 mantissa bits), then the hardware sine and cosine of 2 pi f.
-__device__ __forceinline__ void phasor(double u, float &s, float &c)
+// FP32C: the offset sum (p0 holds 1.5*2^29 + 1/2, see fill_vert) leaves
+// frac(u + 1/2) in the low 23 mantissa bits; as a float y = 1.f in [1, 2),
+// 2 pi (y - 3/2) = y 2 pi - 3 pi is the reduced angle in [-pi, pi) (one FFMA,
+// no FP64->FP32 conversion); then the hardware sine and cosine.
+__device__ __forceinline__ void vertex_phasor(double st, double ct, const VertRegs &w, float &s,
+                                              float &c)
 {
-    const double t = u + (kMagic29 + 0.5);
+    const double t = fma(st, w.ps, fma(ct, w.pc, w.p0));
     const unsigned lo = (unsigned)__double2loint(t);
-    const float x = (__int_as_float(0x3F800000u | (lo & 0x007FFFFFu)) - 1.5f) * 6.28318530717958647f;
+    const float x = fmaf(__int_as_float(0x3F800000u | (lo & 0x007FFFFFu)), 6.28318530717958647f,
+                         -9.42477796076937972f);
     asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(x));
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
 }
@@ -743,13 +755,14 @@ __device__ __forceinline__ double rcp_t(double x) { return rcp64(x); }
 __device__ __forceinline__ float rcp_t(float x) { return rcp32(x); }
 
 // Edge sums S_d = sum_e (P(e+1) - P(e)) / C_e of one beam for the DPT
-// directions of a thread; C_e = A + slope_yx B (x branch, |B| > |A|) or
-// A slope_xy + B.  All vertex phasors are independent, so the NV*DPT chains
-// interleave.  mn[d] receives the smallest |C_e| (nearly singular edges are
-// recomputed in FP64 by the caller).
+// directions of a thread.  The reference's two branches share one form,
+// C_e = X2 + slope_e X1 with (X1, X2, slope) = (B, A, slope_yx) when |B| > |A|
+// (x branch) and (A, B, slope_xy) otherwise (y branch).  All vertex phasors
+// are independent, so the NV*DPT chains interleave.  mn[d] receives the
+// smallest |C_e| (nearly singular edges go to the FP64 pass).
 template <typename T, int DPT, int NV>
 __device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const double *st, const double *ct,
-                                                const T *A, const T *B, const bool *useX,
+                                                const T *X1, const T *X2, const bool *useX,
                                                 T *sr, T *si, T *mn)
 {
     T c[DPT][NV], s[DPT][NV], syx[NV], sxy[NV];
@@ -759,7 +772,7 @@ __device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const doub
         load_vert(v[e], w, syx[e], sxy[e]);
 #pragma unroll
         for (int d = 0; d < DPT; ++d)
-            phasor(fma(st[d], w.ps, fma(ct[d], w.pc, w.p0)), s[d][e], c[d][e]);
+            vertex_phasor(st[d], ct[d], w, s[d][e], c[d][e]);
     }
 #pragma unroll
     for (int d = 0; d < DPT; ++d) {
@@ -772,7 +785,7 @@ __device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const doub
         const int en = (e + 1 < NV) ? e + 1 : 0;
 #pragma unroll
         for (int d = 0; d < DPT; ++d) {
-            const T coef = useX[d] ? fma(syx[e], B[d], A[d]) : fma(sxy[e], A[d], B[d]);
+            const T coef = fma(useX[d] ? syx[e] : sxy[e], X1[d], X2[d]);
             const T inv = rcp_t(coef);
             mn[d] = fmin(mn[d], fabs(coef));
             sr[d] = fma(c[d][en] - c[d][e], inv, sr[d]);
@@ -783,7 +796,7 @@ __device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const doub
 
 template <typename T, int DPT>
 __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, const double *st,
-                                               const double *ct, const T *A, const T *B,
+                                               const double *ct, const T *X1, const T *X2,
                                                const bool *useX, T *sr, T *si, T *mn)
 {
     T c0[DPT], s0[DPT], cp_[DPT], sp_[DPT];
@@ -792,7 +805,7 @@ __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, con
     load_vert(v[0], w, syx, sxy);
 #pragma unroll
     for (int d = 0; d < DPT; ++d) {
-        phasor(fma(st[d], w.ps, fma(ct[d], w.pc, w.p0)), s0[d], c0[d]);
+        vertex_phasor(st[d], ct[d], w, s0[d], c0[d]);
         cp_[d] = c0[d];
         sp_[d] = s0[d];
         mn[d] = T(1e30);
@@ -808,8 +821,8 @@ __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, con
         for (int d = 0; d < DPT; ++d) {
             T cn = c0[d], sn = s0[d];
             if (!last)
-                phasor(fma(st[d], w.ps, fma(ct[d], w.pc, w.p0)), sn, cn);
-            const T coef = useX[d] ? fma(syx_e, B[d], A[d]) : fma(sxy_e, A[d], B[d]);
+                vertex_phasor(st[d], ct[d], w, sn, cn);
+            const T coef = fma(useX[d] ? syx_e : sxy_e, X1[d], X2[d]);
             const T inv = rcp_t(coef);
             mn[d] = fmin(mn[d], fabs(coef));
             sr[d] = fma(cn - cp_[d], inv, sr[d]);
@@ -822,15 +835,15 @@ __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, con
 
 template <typename T, int DPT>
 __device__ __forceinline__ void edge_sums(const SVertRaw<T> *v, int nv, const double *st,
-                                          const double *ct, const T *A, const T *B,
+                                          const double *ct, const T *X1, const T *X2,
                                           const bool *useX, T *sr, T *si, T *mn)
 {
     switch (nv) {   // warp-uniform: every lane evaluates the same beam
-    case 3: edge_sums_fixed<T, DPT, 3>(v, st, ct, A, B, useX, sr, si, mn); break;
-    case 4: edge_sums_fixed<T, DPT, 4>(v, st, ct, A, B, useX, sr, si, mn); break;
-    case 5: edge_sums_fixed<T, DPT, 5>(v, st, ct, A, B, useX, sr, si, mn); break;
-    case 6: edge_sums_fixed<T, DPT, 6>(v, st, ct, A, B, useX, sr, si, mn); break;
-    default: edge_sums_loop<T, DPT>(v, nv, st, ct, A, B, useX, sr, si, mn); break;
+    case 3: edge_sums_fixed<T, DPT, 3>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+    case 4: edge_sums_fixed<T, DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+    case 5: edge_sums_fixed<T, DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+    case 6: edge_sums_fixed<T, DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+    default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn); break;
     }
 }
 
@@ -902,9 +915,10 @@ struct JonesAcc {
     }
 };
 
-// Fused diffraction kernel.  Grid: x = azimuth bin * zenith tiles, y =
-// orientation chunk.  Each thread owns DPT directions (zenith rows
-// t0 + d*TPB of the CTA's azimuth).  T = float selects FP32C.
+// Fused diffraction kernel, persistent: each CTA takes work items
+// (orientation chunk, azimuth bin, zenith tile) from a global counter.  Each
+// thread owns DPT directions of an item (zenith rows t0 + d*TPB of the
+// item's azimuth).  T = float selects FP32C.
 template <typename T, int TPB, int DPT, bool NS, int MINB>
 __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
 {
@@ -919,15 +933,32 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
     T *rsm = reinterpret_cast<T *>(smem_raw + Cfg::kBytes);
     // FP32C: Kahan running sums of the Jones matrices, [kSets][s, c][8][kDirs]
     float *Ksm = reinterpret_cast<float *>(rsm + 8 * TPB);
+    // per thread: bit masks of the stage's pairs for the FP64 pass, [DPT][words][TPB]
+    constexpr int kMaskWords = (Cfg::kBeams + 31) / 32;
+    uint32_t *rmask = reinterpret_cast<uint32_t *>(Ksm + (kF32 ? kSets * 16 * kDirs : 0));
 
-    const int p = blockIdx.x / P.tiles_per_row;
-    const int tile = blockIdx.x - p * P.tiles_per_row;
-    const int chunk = blockIdx.y;
+    const T eps = (T)(kF32 ? P.wc.eps1_f32 : P.wc.eps1);
+    T *rslot = rsm + threadIdx.x;
+    const int items_per_chunk = P.n_az * P.tiles_per_row;
+    __shared__ int s_item;
+
+    // Persistent: take work items until none are left, so CTAs of uneven
+    // cost (rare FP64 pairs, ragged beam counts) balance across the SMs.
+    for (;;) {
+    __syncthreads();   // the previous item is finished with s_item and the stage
+    if (threadIdx.x == 0)
+        s_item = atomicAdd(P.work, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= P.n_items)
+        break;
+    const int chunk = item / items_per_chunk;
+    const int pt = item - chunk * items_per_chunk;
+    const int p = pt / P.tiles_per_row;
+    const int tile = pt - p * P.tiles_per_row;
     int o0, o1;
     chunk_range(P, chunk, o0, o1);
     const double cp = P.cphi[p], sp = P.sphi[p];
-    const T eps = (T)(kF32 ? P.wc.eps1_f32 : P.wc.eps1);
-    T *rslot = rsm + threadIdx.x;
 
     int t[DPT];
     bool active[DPT], general[DPT];
@@ -981,34 +1012,45 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
             for (int i = threadIdx.x; i < nvs; i += TPB)
                 fill_vert(P.vrec[vb0 + i], cp, sp, sv[i]);
             __syncthreads();
+            // Hot loop: every (beam, direction) pair on the vectorised path;
+            // pairs that need FP64 (near-forward zone, small-phase candidates,
+            // nearly singular edges, irregular rows) contribute nothing here
+            // and are marked in the thread's bit mask for the pass below.
+            uint32_t bits[DPT];
+#pragma unroll
+            for (int d = 0; d < DPT; ++d)
+                bits[d] = 0u;
             for (int j = 0; j < nb; ++j) {
                 BeamRegs<T> b;
                 load_beam(sb[j], b);
-                T A[DPT], B[DPT], sr[DPT], si[DPT], mn[DPT];
-                bool useX[DPT], rare[DPT], near[DPT];
+                T X1[DPT], X2[DPT], sr[DPT], si[DPT], mn[DPT], mden[DPT];
+                bool useX[DPT], rare[DPT];
 #pragma unroll
                 for (int d = 0; d < DPT; ++d) {
-                    A[d] = fma(stT[d], b.a[0], fma(ctT[d], b.a[1], b.a[2]));
-                    B[d] = fma(stT[d], b.a[3], fma(ctT[d], b.a[4], b.a[5]));
-                    useX[d] = fabs(B[d]) > fabs(A[d]);
-                    near[d] = kF32 && (float)(A[d] * A[d] + B[d] * B[d]) <= b.nearr2;
-                    const bool cand = fabs(fma(A[d], b.slab[0], B[d] * b.slab[1])) <= T(1)
-                                   && fabs(fma(A[d], b.slab[2], B[d] * b.slab[3])) <= T(1);
-                    rare[d] = general[d] || near[d] || cand;
+                    const T A = fma(stT[d], b.a[0], fma(ctT[d], b.a[1], b.a[2]));
+                    const T B = fma(stT[d], b.a[3], fma(ctT[d], b.a[4], b.a[5]));
+                    useX[d] = fabs(B) > fabs(A);
+                    X1[d] = useX[d] ? B : A;
+                    X2[d] = useX[d] ? A : B;
+                    mden[d] = useX[d] ? B : -A;          // x branch: 1/B, y branch: -1/A
+                    const bool near = kF32 && (float)(A * A + B * B) <= b.nearr2;
+                    const bool cand = fabs(fma(A, b.slab[0], B * b.slab[1])) <= T(1)
+                                   && fabs(fma(A, b.slab[2], B * b.slab[3])) <= T(1);
+                    rare[d] = general[d] || near || cand;
                 }
-                edge_sums<T, DPT>(sv + b.vs, b.nv, st, ct, A, B, useX, sr, si, mn);
-                const bool internal = NS && !(P.beams[b.gbeam].flags & MBS_PO_BEAM_EXTERNAL);
+                edge_sums<T, DPT>(sv + b.vs, b.nv, st, ct, X1, X2, useX, sr, si, mn);
                 T s_r[DPT], s_i[DPT];
-                bool ok[DPT];
 #pragma unroll
                 for (int d = 0; d < DPT; ++d) {
-                    const T m = useX[d] ? rcp_t(B[d]) : -rcp_t(A[d]);
-                    s_r[d] = sr[d] * m;
-                    s_i[d] = si[d] * m;
-                    ok[d] = !(s_r[d] != s_r[d]);
+                    rare[d] = (rare[d] || mn[d] <= eps) && active[d];
+                    bits[d] |= (rare[d] ? 1u : 0u) << (j & 31);
+                    // select, not multiply: a marked pair may hold inf or NaN sums
+                    const T m = rcp_t(mden[d]);
+                    s_r[d] = rare[d] ? T(0) : sr[d] * m;
+                    s_i[d] = rare[d] ? T(0) : si[d] * m;
                 }
-                // d = s x (P0 + cos t Pc + sin t Ps), two complex entries at a time
-                T dj[DPT][8];
+                const T fi = (NS && !(P.beams[b.gbeam].flags & MBS_PO_BEAM_EXTERNAL)) ? T(1) : T(0);
+                // J += s x (P0 + cos t Pc + sin t Ps), two complex entries at a time
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     T p0[4], pc[4], ps[4];
@@ -1017,37 +1059,68 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                     for (int d = 0; d < DPT; ++d) {
 #pragma unroll
                         for (int e = 0; e < 2; ++e) {
+                            const int q = 4 * h + 2 * e;
                             const T rr = fma(stT[d], ps[2 * e], fma(ctT[d], pc[2 * e], p0[2 * e]));
                             const T ri = fma(stT[d], ps[2 * e + 1], fma(ctT[d], pc[2 * e + 1], p0[2 * e + 1]));
-                            dj[d][4 * h + 2 * e] = fma(s_r[d], rr, -s_i[d] * ri);
-                            dj[d][4 * h + 2 * e + 1] = fma(s_r[d], ri, s_i[d] * rr);
+                            J[d].b[q] = fma(s_r[d], rr, fma(-s_i[d], ri, J[d].b[q]));
+                            J[d].b[q + 1] = fma(s_r[d], ri, fma(s_i[d], rr, J[d].b[q + 1]));
+                            if (NS) {
+                                Jn[NS ? d : 0].b[q] = fma(fi * s_r[d], rr, fma(-fi * s_i[d], ri, Jn[NS ? d : 0].b[q]));
+                                Jn[NS ? d : 0].b[q + 1] = fma(fi * s_r[d], ri, fma(fi * s_i[d], rr, Jn[NS ? d : 0].b[q + 1]));
+                            }
                         }
                     }
                 }
+                if ((j & 31) == 31 || j + 1 == nb) {
 #pragma unroll
-                for (int d = 0; d < DPT; ++d) {
-                    if (!active[d])
-                        continue;
-                    if (rare[d] || mn[d] <= eps) {
-                        ok[d] = beam_rare<T>(P, b.gbeam, &sb[j], p, t[d], near[d] && !general[d], rslot, TPB);
-#pragma unroll
-                        for (int q = 0; q < 8; ++q)
-                            dj[d][q] = rslot[q * TPB];
-                    }
-                    if (ok[d]) {
-                        J[d].add(dj[d]);
-                        if (NS && internal)
-                            Jn[d].add(dj[d]);
+                    for (int d = 0; d < DPT; ++d) {
+                        rmask[(d * kMaskWords + (j >> 5)) * TPB + threadIdx.x] = bits[d];
+                        bits[d] = 0u;
                     }
                 }
-                if (kF32 && ((j & (kFlushEvery - 1)) == kFlushEvery - 1 || j + 1 == nb)) {
+                if (kF32 && (j & (kFlushEvery - 1)) == kFlushEvery - 1) {
 #pragma unroll
                     for (int d = 0; d < DPT; ++d) {
                         const int slot = d * TPB + threadIdx.x;
                         J[d].fold(Ksm + slot, Ksm + 8 * kDirs + slot, kDirs);
                         if (NS)
-                            Jn[d].fold(Ksm + 16 * kDirs + slot, Ksm + 24 * kDirs + slot, kDirs);
+                            Jn[NS ? d : 0].fold(Ksm + 16 * kDirs + slot, Ksm + 24 * kDirs + slot, kDirs);
                     }
+                }
+            }
+            // FP64 pass over this thread's marked pairs of the stage.
+            const int words = (nb + 31) >> 5;
+#pragma unroll
+            for (int d = 0; d < DPT; ++d) {
+                for (int w = 0; w < words; ++w) {
+                    uint32_t m = rmask[(d * kMaskWords + w) * TPB + threadIdx.x];
+                    while (m) {
+                        const int j = w * 32 + __ffs(m) - 1;
+                        m &= m - 1;
+                        BeamRegs<T> b;
+                        load_beam(sb[j], b);
+                        const T A = fma(stT[d], b.a[0], fma(ctT[d], b.a[1], b.a[2]));
+                        const T B = fma(stT[d], b.a[3], fma(ctT[d], b.a[4], b.a[5]));
+                        const bool near = kF32 && !general[d] && (float)(A * A + B * B) <= b.nearr2;
+                        if (beam_rare<T>(P, b.gbeam, &sb[j], p, t[d], near, rslot, TPB)) {
+                            T dj[8];
+#pragma unroll
+                            for (int q = 0; q < 8; ++q)
+                                dj[q] = rslot[q * TPB];
+                            J[d].add(dj);
+                            if (NS && !(P.beams[b.gbeam].flags & MBS_PO_BEAM_EXTERNAL))
+                                Jn[NS ? d : 0].add(dj);
+                        }
+                    }
+                }
+            }
+            if (kF32) {
+#pragma unroll
+                for (int d = 0; d < DPT; ++d) {
+                    const int slot = d * TPB + threadIdx.x;
+                    J[d].fold(Ksm + slot, Ksm + 8 * kDirs + slot, kDirs);
+                    if (NS)
+                        Jn[NS ? d : 0].fold(Ksm + 16 * kDirs + slot, Ksm + 24 * kDirs + slot, kDirs);
                 }
             }
             bs = be;
@@ -1092,13 +1165,15 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
             }
         }
     }
+    }   // work items
 }
 
 template <typename T, int TPB, int DPT, bool NS>
 constexpr size_t diffract_smem_bytes()
 {
     return StageCfg<T, TPB>::kBytes + 8 * TPB * sizeof(T)
-         + (sizeof(T) == 4 ? (NS ? 2 : 1) * 16 * TPB * DPT * sizeof(float) : 0);
+         + (sizeof(T) == 4 ? (NS ? 2 : 1) * 16 * TPB * DPT * sizeof(float) : 0)
+         + (size_t)DPT * ((StageCfg<T, TPB>::kBeams + 31) / 32) * TPB * sizeof(uint32_t);
 }
 
 // Polar zenith rows (row_kind 1): every azimuth bin has the same direction
