@@ -381,6 +381,11 @@ def main():
                                           pinned.beam_geom, pinned.beam_flags)))
     d2h_bytes = G * 16 * 8
 
+    # ---- the whole orientation average: host tracing overlapped with the device ----
+    from mbs_fast_b200.pipeline import orientation_average
+    beta_o, gamma_o, w_o = orients
+    _, _, tp = orientation_average(h, cfg, beta_o, gamma_o, w_o, precision=abi.FP32C, batch=2048)
+
     # ---- error vs FP64 on the same orientations ----
     if M64 is not None:
         from tests import common
@@ -410,6 +415,10 @@ def main():
         "fp64_orientations_per_s": (batch.n_orient / (fp64_ms * 1e-3)) if fp64_ms else None,
         "e2e": {"value": total_orient / e2e_s, "unit": "orientations/s",
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
+        "e2e_with_tracing": {"value": batch.n_orient / tp["wall_s"], "unit": "orientations/s",
+                             "wall_s": tp["wall_s"], "host_trace_s": tp["trace_s"],
+                             "what": "reference tracer on all host cores, batches of 2048, "
+                                     "overlapped with FP32C diffraction on the device"},
         "gpu_launches": launches,
         "autotune": tuned,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -1,0 +1,82 @@
+"""Host tracing overlapped with device diffraction.
+
+Once the diffraction runs on the B200, the orientation average is bound by
+the host's beam-splitting tracer (the reference runs it as phase 1,
+TracerPOTotal.cpp:5815-5898, before diffracting).  This pipeline traces
+batch k+1 on the host cores (the reference tracer behind include/mbs_host.h,
+OpenMP) while the device diffracts batch k into one device accumulator, so
+the wall time approaches max(trace, diffract) instead of their sum.  The
+accumulator receives the batches in order, so the result is the same as one
+call over all orientations split the same way.
+"""
+from __future__ import annotations
+
+import queue
+import threading
+import time
+
+import numpy as np
+
+from . import abi, beams as B
+
+
+def orientation_average(handler, cfg, beta, gamma, weight, precision: int = abi.FP32C,
+                        batch: int = 2048, depth: int = 2, noshadow: bool = False):
+    """Weighted Mueller sums [n_az, n_zen+1, 16] (and no-shadow sums) of the
+    orientations (beta, gamma, weight), traced in batches on the host while
+    the previous batch diffracts.  Returns (M, Mns or None, timings)."""
+    import torch
+    g = handler.grid
+    n = len(beta)
+    dev = torch.device(f"cuda:{torch.cuda.current_device()}")
+    acc = torch.zeros(g.n_az * (g.n_zen + 1) * 16, dtype=torch.float64, device=dev)
+    acc_ns = torch.zeros_like(acc) if noshadow else None
+    q: queue.Queue = queue.Queue(maxsize=max(1, depth))
+    err: list = []
+    t_trace = [0.0]
+
+    def producer():
+        try:
+            for s in range(0, n, batch):
+                e = min(n, s + batch)
+                t0 = time.perf_counter()
+                b = B.trace(cfg, beta[s:e], gamma[s:e], weight[s:e])
+                t_trace[0] += time.perf_counter() - t0
+                q.put(b)
+        except Exception as ex:      # surfaced to the caller after the join
+            err.append(ex)
+        finally:
+            q.put(None)
+
+    t0 = time.perf_counter()
+    th = threading.Thread(target=producer, daemon=True)
+    th.start()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    staged = []
+    n_beams = 0
+    while True:
+        b = q.get()
+        if b is None:
+            break
+        n_beams += b.n_beams
+        st = handler.stage(b)
+        handler.diffract_staged(st, acc.data_ptr(), acc_ns.data_ptr() if noshadow else None,
+                                precision=precision, stream=stream)
+        staged.append(st)
+        # keep at most `depth` staged batches alive (their records are in use
+        # until the stream passes them)
+        if len(staged) > depth:
+            torch.cuda.current_stream(dev).synchronize()
+            for s_ in staged[:-1]:
+                s_.free()
+            staged = staged[-1:]
+    th.join()
+    torch.cuda.current_stream(dev).synchronize()
+    for s_ in staged:
+        s_.free()
+    if err:
+        raise err[0]
+    wall = time.perf_counter() - t0
+    M = acc.cpu().numpy().reshape(g.n_az, g.n_zen + 1, 16)
+    Mns = acc_ns.cpu().numpy().reshape(g.n_az, g.n_zen + 1, 16) if noshadow else None
+    return M, Mns, {"wall_s": wall, "trace_s": t_trace[0], "beams": n_beams}

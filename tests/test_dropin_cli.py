@@ -1,0 +1,55 @@
+"""The drop-in binary (the reference CLI with its CUDA backend translation
+unit replaced by this library, mbs_fast_b200/host/Makefile `dropin`)
+against the reference CLI on its CPU backend (oracle/_ref/mbs_po_ref, built
+from the reference sources): same command line, same output files, results
+within the FP64 tolerance."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DROPIN = os.path.join(ROOT, "mbs_fast_b200", "_lib", "mbs_po_b200")
+REFCLI = os.path.join(ROOT, "oracle", "_ref", "mbs_po_ref")
+
+ARGS = ["--method", "po", "--particle", "1", "100", "40", "--refractive-index", "1.3116", "1e-9",
+        "--wavelength-um", "0.532", "--max-reflections", "4", "--sobol", "64",
+        "--scattering-grid", "0", "180", "48", "180", "--close"]
+
+
+def _run(binary, backend, out, env_extra=None):
+    env = dict(os.environ)
+    env.update(env_extra or {})
+    r = subprocess.run([binary] + ARGS + ["--backend", backend, "--output", out],
+                       capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
+    name = os.path.basename(out)
+    rows = np.loadtxt(os.path.join(out, name + ".dat"), skiprows=1)
+    with open(os.path.join(out, name + "_integrals.tsv")) as f:
+        lines = [ln.rstrip("\n").split("\t") for ln in f if ln.strip()]
+    integ = dict(zip(lines[0], lines[1]))
+    return rows, integ, r.stdout + r.stderr
+
+
+def _wl2(a, b):
+    w = b[:, 1:2]                      # 2 pi dcos column
+    return float(np.sqrt(np.sum(w * (a[:, 2:] - b[:, 2:]) ** 2) / np.sum(w * b[:, 2:] ** 2)))
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFCLI)),
+                    reason="drop-in or reference CLI not built")
+def test_dropin_matches_reference_cli(tmp_path):
+    ref, ref_i, _ = _run(REFCLI, "cpu", str(tmp_path / "ref"))
+    gpu, gpu_i, log = _run(DROPIN, "gpu", str(tmp_path / "gpu"), {"MBS_GPU_TIMING": "1"})
+    assert "path=b200-fp64" in log          # the B200 library served the diffraction
+    assert gpu.shape == ref.shape
+    np.testing.assert_array_equal(gpu[:, :2], ref[:, :2])
+    assert _wl2(gpu, ref) < 1e-7
+    for k in ("Cext", "Csca"):
+        assert abs(float(gpu_i[k]) / float(ref_i[k]) - 1) < 1e-7, k
+    f32, f32_i, log32 = _run(DROPIN, "gpu", str(tmp_path / "f32"),
+                             {"MBS_GPU_TIMING": "1", "MBS_B200_PRECISION": "fp32c"})
+    assert "path=b200-fp32c" in log32
+    assert _wl2(f32, ref) < 2e-4
