@@ -55,9 +55,11 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=48, help="orientations in the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error reference")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="column", choices=["column", "proposal"],
+    ap.add_argument("--workload", default="column", choices=["column", "proposal", "aggregate"],
                     help="column: the headline line (default); proposal: the learned "
-                         "orientation proposal against plain Sobol at equal error")
+                         "orientation proposal against plain Sobol at equal error; aggregate: "
+                         "the non-convex 8-column aggregate (thousands of beams per "
+                         "orientation), one graph-captured step per precision")
     return ap.parse_args()
 
 
@@ -282,6 +284,72 @@ def run_proposal(args):
     print(json.dumps(out), flush=True)
 
 
+def run_aggregate(args):
+    """Non-convex aggregate of 8 touching hexagonal columns (D=20 um, L=60 um,
+    seed-drawn orientations), 6 reflections, cutoff profile fast, Sobol
+    orientations on the headline grid: the diffraction step captured into a
+    CUDA graph and replayed, FP32C and FP64, device-resident inputs."""
+    import tempfile
+    import torch
+    from mbs_fast_b200 import abi, beams as B
+    from mbs_fast_b200.handler import GpuHandlerPO
+    from tests import common
+    torch.cuda.set_device(0)
+    n = args.orient if args.orient != 16384 else 32
+    path = os.path.join(tempfile.mkdtemp(), "agg8.particle")
+    cfg = common.aggregate_config(path)
+    bs, gs, _ = B.symmetry(cfg)
+    beta, gamma, w = B.sobol_orientations(n, bs, gs, 42)
+    t0 = time.perf_counter()
+    batch = B.trace(cfg, beta, gamma, w)
+    t_trace = time.perf_counter() - t0
+    grid = B.grid(0.0, 180.0, args.n_phi, args.n_theta)
+    G = grid.n_dirs
+    h = GpuHandlerPO(grid, B.wave(cfg))
+    st = h.stage(batch)
+    acc = torch.zeros(G * 16, dtype=torch.float64, device="cuda:0")
+    s = torch.cuda.Stream()
+    out = {}
+    for prec, name in ((abi.FP32C, "fp32c"), (abi.FP64, "fp64")):
+        best, ms = h.autotune(st, prec, max_orient=min(8, n))
+        with torch.cuda.stream(s):
+            h.diffract_staged(st, acc.data_ptr(), precision=prec, stream=s.cuda_stream, stats=False)
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            acc.zero_()
+            h.diffract_staged(st, acc.data_ptr(), precision=prec, stream=s.cuda_stream, stats=False)
+        for _ in range(args.warmup):
+            g.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ms_step = e0.elapsed_time(e1) / args.steps
+        out[name] = {"ms_per_step": ms_step, "orientations_per_s": n / (ms_step * 1e-3),
+                     "beam_dir_evals_per_s": batch.n_beams * G / (ms_step * 1e-3),
+                     "autotune": {"variant": best, "ms_per_variant": [round(m, 3) for m in ms]}}
+        del g
+    st.free()
+    h.close()
+    bpo = np.diff(batch.beam_offsets)
+    line = {"metric": METRIC, "value": out["fp32c"]["orientations_per_s"], "unit": "orientations/s",
+            "impl": "b200", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic (reference tracer)",
+            "config": {"workload": "non-convex aggregate of 8 hexagonal columns D=20um L=60um, "
+                                   "m=1.3116, 6 reflections, cutoff profile fast, %d Sobol "
+                                   "orientations, theta 0-180 step %.3g x %d phi; one "
+                                   "graph-captured step" % (n, 180.0 / args.n_theta, args.n_phi),
+                       "beams_per_orientation": [int(bpo.min()), int(bpo.max()), float(bpo.mean())],
+                       "trace_seconds": t_trace},
+            "fp32c": out["fp32c"], "fp64": out["fp64"],
+            "host_trace_orientations_per_s": n / t_trace}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -289,6 +357,9 @@ def main():
         return
     if args.workload == "proposal":
         run_proposal(args)
+        return
+    if args.workload == "aggregate":
+        run_aggregate(args)
         return
     rank, world, local = dist_env()
     import torch

@@ -34,7 +34,8 @@ typedef struct mbs_host_config {
     int32_t     absorption;      /* --absorption (also on when ri_im != 0)     */
     double      wavelength;      /* --wavelength-um                            */
     int32_t     max_reflections; /* --max-reflections                          */
-    int32_t     cutoff_off;      /* 1: --cutoff-profile off; 0: legacy default */
+    int32_t     cutoff_profile;  /* --cutoff-profile: 0 legacy-default, 1 off,
+                                    2 safe, 3 balanced, 4 fast (main.cpp:117-226) */
     int32_t     shadow_off;      /* --shadow_off                               */
     int32_t     legacy_sign;     /* --legacy_sign                              */
     int32_t     n_threads;       /* OpenMP threads for tracing (<=0: all)      */

@@ -81,7 +81,7 @@ class HostConfig(C.Structure):
         ("particle_file", C.c_char_p), ("resize", C.c_double),
         ("ri_re", C.c_double), ("ri_im", C.c_double), ("absorption", C.c_int32),
         ("wavelength", C.c_double), ("max_reflections", C.c_int32),
-        ("cutoff_off", C.c_int32), ("shadow_off", C.c_int32),
+        ("cutoff_profile", C.c_int32), ("shadow_off", C.c_int32),
         ("legacy_sign", C.c_int32), ("n_threads", C.c_int32),
     ]
 

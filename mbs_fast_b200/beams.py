@@ -156,9 +156,19 @@ class ParticleConfig:
     wavelength: float = 0.532
     max_reflections: int = 4
     cutoff_off: bool = False
+    # --cutoff-profile by name ("legacy-default", "off", "safe", "balanced",
+    # "fast"); None: "off" when cutoff_off is set, else "legacy-default"
+    cutoff_profile: str | None = None
     shadow_off: bool = False
     legacy_sign: bool = False
     n_threads: int = 0
+
+    PROFILES = ("legacy-default", "off", "safe", "balanced", "fast")
+
+    def _profile(self) -> int:
+        if self.cutoff_profile is None:
+            return 1 if self.cutoff_off else 0
+        return self.PROFILES.index(self.cutoff_profile)
 
     def as_c(self) -> abi.HostConfig:
         p = (C.c_double * 4)(*([float(x) for x in self.p] + [0.0] * (4 - len(self.p)))[:4])
@@ -167,7 +177,7 @@ class ParticleConfig:
             particle_file=(self.particle_file.encode() if self.particle_file else None),
             resize=self.resize, ri_re=self.ri_re, ri_im=self.ri_im,
             absorption=int(self.absorption), wavelength=self.wavelength,
-            max_reflections=self.max_reflections, cutoff_off=int(self.cutoff_off),
+            max_reflections=self.max_reflections, cutoff_profile=self._profile(),
             shadow_off=int(self.shadow_off), legacy_sign=int(self.legacy_sign),
             n_threads=self.n_threads)
 

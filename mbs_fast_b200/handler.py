@@ -275,10 +275,17 @@ class GpuHandlerPO:
 
     def diffract_staged(self, staged: Staged, m_dev_ptr: int, mns_dev_ptr: int | None = None,
                         precision: int = abi.FP64, stream: int = 0,
-                        stats: abi.Stats | None = None) -> None:
-        st = stats if stats is not None else self.last_stats
+                        stats: abi.Stats | None | bool = None) -> None:
+        """Accumulate the staged batch into device arrays on `stream`.  With
+        stats=False no statistics are taken, so the call neither waits for
+        the device nor does anything a CUDA graph capture forbids (after one
+        earlier call has sized the context's scratch)."""
+        if stats is False:
+            sp = None
+        else:
+            sp = C.byref(stats if stats is not None else self.last_stats)
         self._call(lib().mbs_po_diffract_staged(self.ctx, staged.handle, precision,
                                                 C.c_void_p(m_dev_ptr),
                                                 C.c_void_p(mns_dev_ptr) if mns_dev_ptr else None,
-                                                C.c_void_p(stream), C.byref(st)),
+                                                C.c_void_p(stream), sp),
                    "mbs_po_diffract_staged")

@@ -123,30 +123,47 @@ struct HostSetup
         tracer.reset(new TracerPOTotal(particle.get(), cfg.max_reflections, "mbs_b200_host"));
         tracer->m_scattering->m_wave = cfg.wavelength;
         Scattering *sc = tracer->m_scattering;
-        if (cfg.cutoff_off)
-        {   // --cutoff-profile off (main.cpp:205-211)
+        const int profile = cfg.cutoff_profile;
+        if (profile < 0 || profile > 4)
+            throw std::invalid_argument("unknown cutoff profile " + std::to_string(profile));
+        if (profile == 1)
+        {   // --cutoff-profile off (main.cpp:190-196)
             sc->restriction = std::numeric_limits<double>::infinity();
             sc->m_traceCutoffJRel = 0.0;
             sc->m_traceCutoffAreaRel = 0.0;
             sc->m_traceCutoffImportanceRel = 0.0;
         }
-        else
-        {   // legacy-default profile (main.cpp:212-221)
+        else if (profile == 0)
+        {   // legacy-default profile (main.cpp:197-206)
             sc->m_traceCutoffJRel = 1e-7;
             sc->m_traceCutoffAreaRel = 0.0;
             sc->m_traceCutoffImportanceRel = 0.0;
+        }
+        else
+        {   // safe / balanced / fast (main.cpp:207-215)
+            sc->m_traceCutoffJRel = 0.0;
+            sc->m_traceCutoffAreaRel = 0.0;
+            sc->m_traceCutoffImportanceRel = profile == 2 ? 1e-12 : (profile == 3 ? 1e-10 : 1e-8);
+            sc->restriction = profile == 2 ? 1e8 : (profile == 3 ? 1e5 : 1e3);
         }
         tracer->shadowOff = cfg.shadow_off != 0;
         handler.reset(new HostHandlerPO(particle.get(), &tracer->m_incidentLight,
                                         1, cfg.wavelength));
         handler->isCoh = true;
         handler->m_legacySign = cfg.legacy_sign != 0;
-        if (cfg.cutoff_off)
+        if (profile == 1)
         {   // main.cpp:131-137
             handler->m_targetEps = 0.0;
             handler->m_beamCutoffJRel = 0.0;
             handler->m_beamCutoffAreaRel = 0.0;
             handler->m_beamCutoffImportanceRel = 0.0;
+        }
+        else if (profile >= 2)
+        {   // main.cpp:138-145
+            handler->m_targetEps = 0.0;
+            handler->m_beamCutoffJRel = 0.0;
+            handler->m_beamCutoffAreaRel = 0.0;
+            handler->m_beamCutoffImportanceRel = profile == 2 ? 1e-10 : (profile == 3 ? 1e-8 : 1e-6);
         }
         // PrepareBeams does not read the scattering grid; a 1x1 placeholder
         // keeps the per-track matrices of SetTracks small.

@@ -51,7 +51,7 @@ typedef struct mbs_ref_config {
     int32_t     absorption;
     double      wavelength;
     int32_t     max_reflections;
-    int32_t     cutoff_off;
+    int32_t     cutoff_profile;   /* 0 legacy-default, 1 off, 2 safe, 3 balanced, 4 fast */
     int32_t     shadow_off;
     int32_t     legacy_sign;
     int32_t     n_threads;
@@ -106,29 +106,38 @@ struct RefSetup
         tracer.reset(new TracerPOTotal(particle.get(), cfg.max_reflections, "mbs_ref"));
         tracer->m_scattering->m_wave = cfg.wavelength;
         Scattering *sc = tracer->m_scattering;
-        if (cfg.cutoff_off)
+        const int profile = cfg.cutoff_profile;
+        if (profile == 1)
         {
             sc->restriction = std::numeric_limits<double>::infinity();
             sc->m_traceCutoffJRel = 0.0;
             sc->m_traceCutoffAreaRel = 0.0;
             sc->m_traceCutoffImportanceRel = 0.0;
         }
-        else
+        else if (profile == 0)
         {
             sc->m_traceCutoffJRel = 1e-7;
             sc->m_traceCutoffAreaRel = 0.0;
             sc->m_traceCutoffImportanceRel = 0.0;
         }
+        else
+        {
+            sc->m_traceCutoffJRel = 0.0;
+            sc->m_traceCutoffAreaRel = 0.0;
+            sc->m_traceCutoffImportanceRel = profile == 2 ? 1e-12 : (profile == 3 ? 1e-10 : 1e-8);
+            sc->restriction = profile == 2 ? 1e8 : (profile == 3 ? 1e5 : 1e3);
+        }
         tracer->shadowOff = cfg.shadow_off != 0;
         handler.reset(new HandlerPOTotal(particle.get(), &tracer->m_incidentLight, 1, cfg.wavelength));
         handler->isCoh = true;
         handler->m_legacySign = cfg.legacy_sign != 0;
-        if (cfg.cutoff_off)
+        if (profile >= 1)
         {
             handler->m_targetEps = 0.0;
             handler->m_beamCutoffJRel = 0.0;
             handler->m_beamCutoffAreaRel = 0.0;
-            handler->m_beamCutoffImportanceRel = 0.0;
+            handler->m_beamCutoffImportanceRel = profile == 1 ? 0.0
+                : (profile == 2 ? 1e-10 : (profile == 3 ? 1e-8 : 1e-6));
         }
         ScatteringRange range(DegToRad(gs.zen_start_deg), DegToRad(gs.zen_end_deg), gs.n_az, gs.n_zen);
         if (gs.theta_deg)

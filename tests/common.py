@@ -97,3 +97,14 @@ def element_errors(M: np.ndarray, Mref: np.ndarray, grid: B.GridTables) -> dict:
     for name, idx in (("M12", 1), ("M22", 5), ("M33", 10), ("M34", 11), ("M44", 15)):
         out[name + "/M11_max_abs"] = float(np.max(np.abs(r[:, idx] / r[:, 0] - q[:, idx] / q[:, 0])))
     return out
+
+
+def aggregate_config(path: str, max_reflections: int = 6, profile: str = "fast"):
+    """Non-convex aggregate of 8 hexagonal columns (D=20 um, L=60 um,
+    seed-drawn orientations, touching, written as a reference particle file
+    at `path`), m=1.3116, 6 reflections, cutoff profile `profile`."""
+    from mbs_fast_b200 import particles as PT
+    PT.write_particle_file(path, PT.column_aggregate())
+    return B.ParticleConfig(particle_type=0, particle_file=path, ri_re=1.3116, ri_im=0.0,
+                            wavelength=0.532, max_reflections=max_reflections,
+                            cutoff_profile=profile)
