@@ -55,11 +55,12 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=48, help="orientations in the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error reference")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="column", choices=["column", "proposal", "aggregate"],
+    ap.add_argument("--workload", default="column", choices=["column", "proposal", "aggregate", "refgpu"],
                     help="column: the headline line (default); proposal: the learned "
                          "orientation proposal against plain Sobol at equal error; aggregate: "
                          "the non-convex 8-column aggregate (thousands of beams per "
-                         "orientation), one graph-captured step per precision")
+                         "orientation), one graph-captured step per precision; refgpu: the "
+                         "reference's own CUDA build against the drop-in binary, same CLI run")
     return ap.parse_args()
 
 
@@ -350,6 +351,61 @@ def run_aggregate(args):
     print(json.dumps(line), flush=True)
 
 
+def run_refgpu(args):
+    """Same-box GPU comparison at the CLI: the reference's own CUDA build
+    (oracle/_ref/mbs_po_gpu_ref_{fp64,fp32}, its GpuDiffraction.cu for sm_100)
+    against the drop-in binary (the same CLI with this library underneath,
+    FP64 and FP32C), on the D=40 um, L=100 um column with N Sobol orientations
+    and the headline grid.  Diffraction time is the sum of the "GPU timing
+    diffract" lines (MBS_GPU_TIMING=1) of each run: kernels and the whole
+    call (packing, copies, kernels, accumulation)."""
+    import re
+    import subprocess
+    import tempfile
+    n = args.orient if args.orient != 16384 else 2048
+    cli = ["--method", "po", "--particle", "1", "100", "40", "--refractive-index", "1.3116", "1e-9",
+           "--wavelength-um", "0.532", "--max-reflections", "4", "--sobol", str(n),
+           "--scattering-grid", "0", "180", str(args.n_phi), str(args.n_theta), "--close",
+           "--backend", "gpu"]
+    runs = {"reference_fp64": (os.path.join(ROOT, "oracle", "_ref", "mbs_po_gpu_ref_fp64"), {}),
+            "reference_fp32": (os.path.join(ROOT, "oracle", "_ref", "mbs_po_gpu_ref_fp32"), {}),
+            "b200_fp64": (os.path.join(ROOT, "mbs_fast_b200", "_lib", "mbs_po_b200"),
+                          {"MBS_B200_PRECISION": "fp64"}),
+            "b200_fp32c": (os.path.join(ROOT, "mbs_fast_b200", "_lib", "mbs_po_b200"),
+                           {"MBS_B200_PRECISION": "fp32c"})}
+    out = {}
+    for name, (binary, env_extra) in runs.items():
+        if not os.path.exists(binary):
+            out[name] = {"unavailable": "not built"}
+            continue
+        env = dict(os.environ, MBS_GPU_TIMING="1", **env_extra)
+        d = tempfile.mkdtemp()
+        t0 = time.perf_counter()
+        r = subprocess.run([binary] + cli + ["--output", os.path.join(d, "o")], capture_output=True,
+                           text=True, env=env, timeout=1800)
+        wall = time.perf_counter() - t0
+        text = r.stdout + r.stderr
+        lines = [ln for ln in text.splitlines() if "GPU timing diffract" in ln]
+        kern = sum(float(m) for ln in lines for m in re.findall(r"kernels=([0-9.]+)ms", ln))
+        tot = sum(float(m) for ln in lines for m in re.findall(r"total=([0-9.]+)ms", ln))
+        out[name] = {"rc": r.returncode, "calls": len(lines), "kernel_ms": kern, "call_ms": tot,
+                     "orientations_per_s_kernel": n / (kern * 1e-3) if kern else None,
+                     "orientations_per_s_call": n / (tot * 1e-3) if tot else None,
+                     "process_wall_s": wall}
+    line = {"metric": METRIC, "unit": "orientations/s", "impl": "b200-vs-reference-gpu",
+            "config": {"workload": WORKLOAD.replace("16384", str(n)), "orientations": n},
+            "runs": out}
+    ref, mine = out.get("reference_fp64", {}), out.get("b200_fp64", {})
+    if ref.get("kernel_ms") and mine.get("kernel_ms"):
+        line["fp64_kernel_speedup_vs_reference"] = ref["kernel_ms"] / mine["kernel_ms"]
+        line["fp64_call_speedup_vs_reference"] = ref["call_ms"] / mine["call_ms"]
+    r32, m32 = out.get("reference_fp32", {}), out.get("b200_fp32c", {})
+    if r32.get("kernel_ms") and m32.get("kernel_ms"):
+        line["fp32_kernel_speedup_vs_reference"] = r32["kernel_ms"] / m32["kernel_ms"]
+        line["fp32_call_speedup_vs_reference"] = r32["call_ms"] / m32["call_ms"]
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -360,6 +416,9 @@ def main():
         return
     if args.workload == "aggregate":
         run_aggregate(args)
+        return
+    if args.workload == "refgpu":
+        run_refgpu(args)
         return
     rank, world, local = dist_env()
     import torch
