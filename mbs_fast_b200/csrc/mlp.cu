@@ -1,10 +1,13 @@
 // mlp.cu — the learned orientation proposal network (include/mbs_mlp.h).
 //
 // 4 -> 128 -> 128 -> 128 -> 1 with erf GELU.  Every layer product runs on
-// the tensor cores as BF16 x BF16 -> FP32 (mma.sync m16n8k16, one 64 x 64
-// output tile per CTA, operands staged through shared memory with arbitrary
-// strides so transposed operands of the backward pass need no copies).  The
-// 128 -> 1 head is a per-sample dot product in FP32.  Master parameters,
+// the 5th-generation tensor cores as BF16 x BF16 -> FP32: tcgen05.mma
+// (M = 128, N <= 128, K = 16 per instruction) issued by one thread per CTA,
+// both operands in shared memory in the K-major no-swizzle layout (8 x 16-byte
+// core matrices), the accumulator in tensor memory, read back with
+// tcgen05.ld for the epilogue.  Operands are staged from global memory with
+// arbitrary strides, so the transposed operands of the backward pass need no
+// copies.  The 128 -> 1 head is a per-sample dot product in FP32.  Master parameters,
 // gradients and Adam moments are FP32; the BF16 weight copies are refreshed
 // after every update.  All reductions (bias gradients, loss) run in a fixed
 // order, so training is bitwise repeatable for a given seed.
@@ -26,7 +29,9 @@ namespace mlp {
 constexpr int kH = MBS_MLP_HIDDEN;   // 128
 constexpr int kIn = MBS_MLP_IN;      // 4
 constexpr int kInPad = 16;           // K of the first layer, padded for the MMA
-constexpr int kTile = 64;
+constexpr int kTile = 128;           // M of one tcgen05.mma tile (batch rows padded to it)
+constexpr int kTileK = 128;          // K staged per round
+constexpr int kGemmSmem = 2 * kTile * kTileK * 2 + 1024;   // A, B tiles (BF16) + barrier
 
 // Flat parameter offsets (include/mbs_mlp.h)
 constexpr int oW1 = 0, ob1 = oW1 + kH * kIn, oW2 = ob1 + kH, ob2 = oW2 + kH * kH;
@@ -64,85 +69,158 @@ struct GemmOut {
     int ldo;
 };
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
-                                         uint32_t a3, uint32_t b0, uint32_t b1)
+// ---- tcgen05 helpers --------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+    return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// C[M][N] = A[M][K] B[K][N] with the epilogue of MODE.  Grid: x over N
-// tiles, y over M tiles; 128 threads = 2 x 2 warps of 32 x 32 outputs.
-template <int MODE>
-__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, Mat A, Mat B, GemmOut o)
+// Shared-memory matrix descriptor, K-major without swizzle: start address,
+// leading byte offset (between the two 8-element core matrices along K),
+// stride byte offset (between 8-row groups), version 1, swizzle none.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
-    // [row][k] with a pad of 8 so the 32-bit fragment loads spread over banks
-    __shared__ __align__(16) bf16 sA[kTile][kInPad + 8];
-    __shared__ __align__(16) bf16 sB[kTile][kInPad + 8];
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16)
+         | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N and M of the tile.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Byte offset of element (row, k) in a K-major no-swizzle tile whose rows hold
+// kt elements: core matrix (row / 8, k / 8), 16 bytes per row inside it.
+__device__ __forceinline__ uint32_t kmajor_off(int row, int k, int kt)
+{
+    return (uint32_t)((row >> 3) * (kt * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// Bounded wait on an mbarrier phase; false when it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase)
+{
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred P1;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P1;\n\t}"
+                     : "=r"(done) : "r"(bar), "r"(phase) : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+
+// C[M][N] = A[M][K] B[K][N] with the epilogue of MODE.  M a multiple of 128,
+// N a multiple of 16 (at most 128 per CTA), K a multiple of 16.  Grid: x over
+// N tiles, y over M tiles; 128 threads, thread i owns accumulator row i
+// (tensor-memory lane i).  On a barrier timeout *err is set and the CTA
+// frees its tensor memory and returns without storing.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, Mat A, Mat B, GemmOut o, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char gsm[];
+    bf16 *sA = reinterpret_cast<bf16 *>(gsm);
+    bf16 *sB = reinterpret_cast<bf16 *>(gsm + kTile * kTileK * 2);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(gsm + 2 * kTile * kTileK * 2);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
     const int m0 = blockIdx.y * kTile, n0 = blockIdx.x * kTile;
+    const int nt = min(kTile, N - n0);                   // multiple of 16
+    const int ncols = nt <= 32 ? 32 : (nt <= 64 ? 64 : 128);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int gid = lane >> 2, tig = lane & 3;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                acc[i][j][q] = 0.f;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tslot)), "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(1));
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tslot;
+    const uint32_t idesc = umma_idesc(kTile, nt);
     const bf16 zero = __float2bfloat16(0.f);
-    for (int k0 = 0; k0 < K; k0 += kInPad) {
-        for (int i = threadIdx.x; i < kTile * kInPad; i += blockDim.x) {
-            const int r = i >> 4, c = i & 15;
-            const int gk = k0 + c;
-            const int gm = m0 + r, gn = n0 + r;
-            sA[r][c] = (gm < M && gk < K) ? A.p[gm * A.sr + gk * A.sc] : zero;
-            sB[r][c] = (gn < N && gk < K) ? B.p[gk * B.sr + gn * B.sc] : zero;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int k0 = 0; k0 < K && ok; k0 += kTileK) {
+        const int kt = min(kTileK, K - k0);              // multiple of 16
+        // stage A (kTile x kt) and B (nt x kt) in the K-major layout
+        for (int i = threadIdx.x; i < kTile * kt; i += blockDim.x) {
+            const int r = i / kt, k = i - r * kt;
+            const int gm = m0 + r, gk = k0 + k;
+            *reinterpret_cast<bf16 *>(reinterpret_cast<unsigned char *>(sA) + kmajor_off(r, k, kt)) =
+                gm < M ? A.p[gm * A.sr + gk * A.sc] : zero;
         }
+        for (int i = threadIdx.x; i < nt * kt; i += blockDim.x) {
+            const int r = i / kt, k = i - r * kt;
+            *reinterpret_cast<bf16 *>(reinterpret_cast<unsigned char *>(sB) + kmajor_off(r, k, kt)) =
+                B.p[(k0 + k) * B.sr + (n0 + r) * B.sc];
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-#pragma unroll
-        for (int mi = 0; mi < 2; ++mi) {
-            const int rb = wm + mi * 16;
-            const uint32_t a0 = *reinterpret_cast<const uint32_t *>(&sA[rb + gid][tig * 2]);
-            const uint32_t a1 = *reinterpret_cast<const uint32_t *>(&sA[rb + gid + 8][tig * 2]);
-            const uint32_t a2 = *reinterpret_cast<const uint32_t *>(&sA[rb + gid][tig * 2 + 8]);
-            const uint32_t a3 = *reinterpret_cast<const uint32_t *>(&sA[rb + gid + 8][tig * 2 + 8]);
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni) {
-                const int cb = wn + ni * 8;
-                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&sB[cb + gid][tig * 2]);
-                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&sB[cb + gid][tig * 2 + 8]);
-                mma_bf16(acc[mi][ni], a0, a1, a2, a3, b0, b1);
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB), sbo = (uint32_t)kt * 16;
+            for (int s = 0; s < kt / 16; ++s) {
+                const uint64_t da = umma_desc(a0 + 256 * s, 128, sbo);
+                const uint64_t db = umma_desc(b0 + 256 * s, 128, sbo);
+                const uint32_t acc = (k0 > 0 || s > 0) ? 1u : 0u;
+                asm volatile("{\n\t.reg .pred p;\n\t"
+                             "setp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                             :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc));
             }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(smem_u32(bar)) : "memory");
         }
+        // the tiles may be overwritten once the MMAs that read them are done
+        ok = mbar_wait(smem_u32(bar), phase);
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
         __syncthreads();
     }
+    if (!ok) {
+        if (threadIdx.x == 0)
+            atomicExch(err, 1);
+        mbar_wait(smem_u32(bar), phase ^ 1u);   // let any MMA in flight finish, bounded
+    } else {
+        const int r = m0 + warp * 32 + lane;
+        for (int c0 = 0; c0 < nt; c0 += 16) {
+            uint32_t v[16];
+            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                         "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                           "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                           "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                         : "r"(ta));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (r < M) {
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int r = m0 + wm + mi * 16 + gid + (q >= 2 ? 8 : 0);
-                const int c = n0 + wn + ni * 8 + tig * 2 + (q & 1);
-                if (r >= M || c >= N)
-                    continue;
-                const long idx = (long)r * o.ldo + c;
-                const float v = acc[mi][ni][q];
-                if (MODE == kModeFwd) {
-                    const float z = v + o.bias[c];
-                    o.z[idx] = z;
-                    o.h[idx] = __float2bfloat16(gelu(z));
-                } else if (MODE == kModeBwd) {
-                    o.h[idx] = __float2bfloat16(v * gelu_grad(o.zin[idx]));
-                } else {
-                    o.f[idx] = v;
+                for (int i = 0; i < 16; ++i) {
+                    const int c = n0 + c0 + i;
+                    const long idx = (long)r * o.ldo + c;
+                    const float val = __uint_as_float(v[i]);
+                    if (MODE == kModeFwd) {
+                        const float z = val + o.bias[c];
+                        o.z[idx] = z;
+                        o.h[idx] = __float2bfloat16(gelu(z));
+                    } else if (MODE == kModeBwd) {
+                        o.h[idx] = __float2bfloat16(val * gelu_grad(o.zin[idx]));
+                    } else {
+                        o.f[idx] = val;
+                    }
                 }
             }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(ncols));
 }
 
 // X0[b][0..15] (BF16): the quaternion in columns 0..3, zeros elsewhere and
@@ -282,7 +360,7 @@ __global__ void k_gather(const float *q, const float *t, const int *idx, int n, 
     tb[i] = t[s];
 }
 
-inline int pad64(int n) { return (n + kTile - 1) / kTile * kTile; }
+inline int pad_rows(int n) { return (n + kTile - 1) / kTile * kTile; }
 
 }  // namespace mlp
 
@@ -333,7 +411,7 @@ void free_acts(mbs_mlp *net)
 
 int ensure_acts(mbs_mlp *net, int rows)
 {
-    const int need = pad64(std::max(rows, 1));
+    const int need = pad_rows(std::max(rows, 1));
     if (need <= net->cap)
         return 0;
     free_acts(net);
@@ -358,24 +436,51 @@ int ensure_acts(mbs_mlp *net, int rows)
 
 dim3 tiles(int M, int N) { return dim3((N + kTile - 1) / kTile, (M + kTile - 1) / kTile); }
 
+// Device flag set by a GEMM whose tensor-core barrier wait ran out (the
+// third int of the network's scalar scratch).
+int *mlp_err(mbs_mlp *net) { return reinterpret_cast<int *>(net->scalar) + 2; }
+
+// Reset before a call's kernels, checked after its final synchronisation.
+int check_err(mbs_mlp *net)
+{
+    int e = 0;
+    MK(cudaMemcpy(&e, mlp_err(net), sizeof(int), cudaMemcpyDeviceToHost), "D2H error flag");
+    if (e) {
+        cudaMemset(mlp_err(net), 0, sizeof(int));
+        return mfail(net, -6, "tensor-core barrier wait timed out");
+    }
+    return 0;
+}
+
+template <int MODE>
+void gemm(cudaStream_t s, int M, int N, int K, Mat A, Mat B, GemmOut o, int *err)
+{
+    static bool attr = false;   // the dynamic shared-memory limit, once per instantiation
+    if (!attr) {
+        cudaFuncSetAttribute(k_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+        attr = true;
+    }
+    k_gemm<MODE><<<tiles(M, N), 128, kGemmSmem, s>>>(M, N, K, A, B, o, err);
+}
+
 // Forward pass of n samples already in net->q (device); train keeps the
 // pre-activations for the backward pass.
 int forward_dev(mbs_mlp *net, int n)
 {
-    const int bp = pad64(n);
+    const int bp = pad_rows(n);
     cudaStream_t s = net->stream;
     k_input<<<(bp * kInPad + 255) / 256, 256, 0, s>>>(net->q, n, bp, net->x0);
     GemmOut o{};
     o.ldo = kH;
     o.bias = net->params + ob1; o.z = net->z1; o.h = net->h1;
-    k_gemm<kModeFwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kInPad, Mat{net->x0, kInPad, 1},
-                                                   Mat{net->w1p, 1, kInPad}, o);
+    gemm<kModeFwd>(s, bp, kH, kInPad, Mat{net->x0, kInPad, 1},
+                   Mat{net->w1p, 1, kInPad}, o, mlp_err(net));
     o.bias = net->params + ob2; o.z = net->z2; o.h = net->h2;
-    k_gemm<kModeFwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kH, Mat{net->h1, kH, 1},
-                                                   Mat{net->w2, 1, kH}, o);
+    gemm<kModeFwd>(s, bp, kH, kH, Mat{net->h1, kH, 1},
+                   Mat{net->w2, 1, kH}, o, mlp_err(net));
     o.bias = net->params + ob3; o.z = net->z3; o.h = net->h3;
-    k_gemm<kModeFwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kH, Mat{net->h2, kH, 1},
-                                                   Mat{net->w3, 1, kH}, o);
+    gemm<kModeFwd>(s, bp, kH, kH, Mat{net->h2, kH, 1},
+                   Mat{net->w3, 1, kH}, o, mlp_err(net));
     k_head_fwd<<<(n + 7) / 8, 256, 0, s>>>(net->h3, net->params, n, net->y);
     MK(cudaGetLastError(), "mlp forward launch");
     return 0;
@@ -384,7 +489,7 @@ int forward_dev(mbs_mlp *net, int n)
 // Backward pass after forward_dev (targets in net->t): net->grad (flat).
 int backward_dev(mbs_mlp *net, int n)
 {
-    const int bp = pad64(n);
+    const int bp = pad_rows(n);
     cudaStream_t s = net->stream;
     k_head_bwd<<<(bp * kH + 255) / 256, 256, 0, s>>>(net->y, net->t, n, bp, net->params, net->z3,
                                                      net->dy, net->dz3);
@@ -392,24 +497,24 @@ int backward_dev(mbs_mlp *net, int n)
     GemmOut o{};
     // layer 3: dW3 = dZ3^T H2, db3 = colsum dZ3, dZ2 = (dZ3 W3) * gelu'(Z2)
     o.ldo = kH; o.f = net->grad + oW3;
-    k_gemm<kModeF32><<<tiles(kH, kH), 128, 0, s>>>(kH, kH, bp, Mat{net->dz3, 1, kH},
-                                                   Mat{net->h2, kH, 1}, o);
+    gemm<kModeF32>(s, kH, kH, bp, Mat{net->dz3, 1, kH},
+                   Mat{net->h2, kH, 1}, o, mlp_err(net));
     k_colsum_bf16<<<1, kH, 0, s>>>(net->dz3, bp, kH, net->grad + ob3);
     o = GemmOut{}; o.ldo = kH; o.zin = net->z2; o.h = net->dz2;
-    k_gemm<kModeBwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kH, Mat{net->dz3, kH, 1},
-                                                   Mat{net->w3, kH, 1}, o);
+    gemm<kModeBwd>(s, bp, kH, kH, Mat{net->dz3, kH, 1},
+                   Mat{net->w3, kH, 1}, o, mlp_err(net));
     // layer 2
     o = GemmOut{}; o.ldo = kH; o.f = net->grad + oW2;
-    k_gemm<kModeF32><<<tiles(kH, kH), 128, 0, s>>>(kH, kH, bp, Mat{net->dz2, 1, kH},
-                                                   Mat{net->h1, kH, 1}, o);
+    gemm<kModeF32>(s, kH, kH, bp, Mat{net->dz2, 1, kH},
+                   Mat{net->h1, kH, 1}, o, mlp_err(net));
     k_colsum_bf16<<<1, kH, 0, s>>>(net->dz2, bp, kH, net->grad + ob2);
     o = GemmOut{}; o.ldo = kH; o.zin = net->z1; o.h = net->dz1;
-    k_gemm<kModeBwd><<<tiles(bp, kH), 128, 0, s>>>(bp, kH, kH, Mat{net->dz2, kH, 1},
-                                                   Mat{net->w2, kH, 1}, o);
+    gemm<kModeBwd>(s, bp, kH, kH, Mat{net->dz2, kH, 1},
+                   Mat{net->w2, kH, 1}, o, mlp_err(net));
     // layer 1
     o = GemmOut{}; o.ldo = kInPad; o.f = net->gw1p;
-    k_gemm<kModeF32><<<tiles(kH, kInPad), 128, 0, s>>>(kH, kInPad, bp, Mat{net->dz1, 1, kH},
-                                                       Mat{net->x0, kInPad, 1}, o);
+    gemm<kModeF32>(s, kH, kInPad, bp, Mat{net->dz1, 1, kH},
+                   Mat{net->x0, kInPad, 1}, o, mlp_err(net));
     k_pack_w1_grad<<<(kH * kIn + 127) / 128, 128, 0, s>>>(net->gw1p, net->grad);
     k_colsum_bf16<<<1, kH, 0, s>>>(net->dz1, bp, kH, net->grad + ob1);
     MK(cudaGetLastError(), "mlp backward launch");
@@ -441,7 +546,8 @@ extern "C" int mbs_mlp_create(mbs_mlp **out, int device, uint64_t seed)
         || cudaMalloc((void **)&net->w1p, kH * kInPad * sizeof(bf16))
         || cudaMalloc((void **)&net->w2, kH * kH * sizeof(bf16))
         || cudaMalloc((void **)&net->w3, kH * kH * sizeof(bf16))
-        || cudaMalloc((void **)&net->gw1p, kH * kInPad * 4) || cudaMalloc((void **)&net->scalar, 16))
+        || cudaMalloc((void **)&net->gw1p, kH * kInPad * 4) || cudaMalloc((void **)&net->scalar, 16)
+        || cudaMemset(net->scalar, 0, 16))
         return bail(-4);
     // uniform +-sqrt(6 / fan_in) weights, zero biases
     std::vector<float> p(np, 0.f);
@@ -524,7 +630,7 @@ extern "C" int mbs_mlp_forward(mbs_mlp *net, const float *q, int n, float *y)
         return rc;
     MK(cudaMemcpyAsync(y, net->y, (size_t)n * 4, cudaMemcpyDeviceToHost, net->stream), "D2H y");
     MK(cudaStreamSynchronize(net->stream), "sync");
-    return 0;
+    return check_err(net);
 }
 
 extern "C" int mbs_mlp_loss_grad(mbs_mlp *net, const float *q, const float *t, int n, float *loss,
@@ -549,7 +655,7 @@ extern "C" int mbs_mlp_loss_grad(mbs_mlp *net, const float *q, const float *t, i
     MK(cudaStreamSynchronize(net->stream), "sync");
     if (loss)
         *loss = l;
-    return 0;
+    return check_err(net);
 }
 
 extern "C" int mbs_mlp_train(mbs_mlp *net, const float *q, const float *t, int n, int epochs,
@@ -621,5 +727,5 @@ extern "C" int mbs_mlp_train(mbs_mlp *net, const float *q, const float *t, int n
         return rc;
     if (e != cudaSuccess)
         return mfail(net, -3, std::string("training: ") + cudaGetErrorString(e));
-    return 0;
+    return check_err(net);
 }
