@@ -55,12 +55,13 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=48, help="orientations in the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error reference")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="column", choices=["column", "proposal", "aggregate", "refgpu"],
+    ap.add_argument("--workload", default="column", choices=["column", "proposal", "aggregate", "refgpu", "mlp"],
                     help="column: the headline line (default); proposal: the learned "
                          "orientation proposal against plain Sobol at equal error; aggregate: "
                          "the non-convex 8-column aggregate (thousands of beams per "
                          "orientation), one graph-captured step per precision; refgpu: the "
-                         "reference's own CUDA build against the drop-in binary, same CLI run")
+                         "reference's own CUDA build against the drop-in binary, same CLI run; mlp: "
+                         "training and inference of the proposal network alone")
     return ap.parse_args()
 
 
@@ -406,6 +407,25 @@ def run_refgpu(args):
     print(json.dumps(line), flush=True)
 
 
+def run_mlp(args):
+    """The proposal network's kernels alone: Adam training on 8192 seeded unit
+    quaternions (2 epochs, batches of 2048) and one forward pass over them."""
+    from mbs_fast_b200.mlp import ProposalNet
+    rng = np.random.default_rng(0)
+    q = rng.normal(size=(8192, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    t = np.sin(3 * q[:, 0]) + q[:, 1] * q[:, 2]
+    net = ProposalNet(seed=1)
+    t0 = time.perf_counter()
+    loss = net.train(q, t, epochs=2, batch=2048, lr=2e-3)
+    t1 = time.perf_counter()
+    net.forward(q)
+    t2 = time.perf_counter()
+    net.close()
+    print(json.dumps({"workload": "proposal network 4-128-128-128-1, BF16 tcgen05", "train_s": t1 - t0,
+                      "forward_s": t2 - t1, "loss": loss}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -419,6 +439,9 @@ def main():
         return
     if args.workload == "refgpu":
         run_refgpu(args)
+        return
+    if args.workload == "mlp":
+        run_mlp(args)
         return
     rank, world, local = dist_env()
     import torch
