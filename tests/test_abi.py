@@ -19,6 +19,7 @@ def declared_functions(header: str) -> list[str]:
 
 
 @pytest.mark.parametrize("header,lib", [("mbs_po_b200.h", "libmbs_po_b200.so"),
+                                        ("mbs_mlp.h", "libmbs_po_b200.so"),
                                         ("mbs_host.h", "libmbs_host.so")])
 def test_exports(header, lib):
     names = declared_functions(header)
