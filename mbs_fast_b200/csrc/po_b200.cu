@@ -46,9 +46,12 @@ struct GridDev {
 struct Variant {
     int tpb, dpt, minb;
 };
-constexpr Variant kVariantsF32[] = {{128, 2, 4}, {128, 2, 3}, {128, 1, 4}, {128, 1, 5},
-                                    {128, 1, 6}, {96, 2, 5}, {128, 4, 2}, {256, 1, 2}};
-constexpr Variant kVariantsF64[] = {{128, 1, 4}, {128, 2, 3}, {128, 1, 3}};
+constexpr Variant kVariantsF32[] = {{64, 3, 6}, {64, 3, 5}, {128, 3, 3},
+                                    {96, 2, 5}, {128, 2, 4}, {64, 3, 4}};
+constexpr Variant kVariantsF64[] = {{64, 2, 6}, {128, 1, 3}, {96, 2, 4}, {128, 1, 4}, {64, 3, 4}};
+// Shapes of the kernels that also accumulate the no-shadow sums.
+constexpr Variant kNoShadowF32 = {128, 2, 4};
+constexpr Variant kNoShadowF64 = {128, 1, 4};
 constexpr int kNumVariantsF32 = sizeof(kVariantsF32) / sizeof(Variant);
 constexpr int kNumVariantsF64 = sizeof(kVariantsF64) / sizeof(Variant);
 
@@ -552,30 +555,38 @@ cudaError_t launch_one(const KParams &P, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// No-shadow sums use the default shape of each precision.
+// The cases follow kVariantsF64 / kVariantsF32 entry by entry; no-shadow
+// sums use kNoShadowF64 / kNoShadowF32.
 cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &P, cudaStream_t st)
 {
     if (precision == MBS_PO_FP64) {
         if (ns)
             return launch_one<double, 128, 1, true, 4>(P, st);
         switch (variant) {
-        case 1: return launch_one<double, 128, 2, false, 3>(P, st);
-        case 2: return launch_one<double, 128, 1, false, 3>(P, st);
-        default: return launch_one<double, 128, 1, false, 4>(P, st);
+        case 1: return launch_one<double, 128, 1, false, 3>(P, st);
+        case 2: return launch_one<double, 96, 2, false, 4>(P, st);
+        case 3: return launch_one<double, 128, 1, false, 4>(P, st);
+        case 4: return launch_one<double, 64, 3, false, 4>(P, st);
+        default: return launch_one<double, 64, 2, false, 6>(P, st);
         }
     }
     if (ns)
         return launch_one<float, 128, 2, true, 4>(P, st);
     switch (variant) {
-    case 1: return launch_one<float, 128, 2, false, 3>(P, st);
-    case 2: return launch_one<float, 128, 1, false, 4>(P, st);
-    case 3: return launch_one<float, 128, 1, false, 5>(P, st);
-    case 4: return launch_one<float, 128, 1, false, 6>(P, st);
-    case 5: return launch_one<float, 96, 2, false, 5>(P, st);
-    case 6: return launch_one<float, 128, 4, false, 2>(P, st);
-    case 7: return launch_one<float, 256, 1, false, 2>(P, st);
-    default: return launch_one<float, 128, 2, false, 4>(P, st);
+    case 1: return launch_one<float, 64, 3, false, 5>(P, st);
+    case 2: return launch_one<float, 128, 3, false, 3>(P, st);
+    case 3: return launch_one<float, 96, 2, false, 5>(P, st);
+    case 4: return launch_one<float, 128, 2, false, 4>(P, st);
+    case 5: return launch_one<float, 64, 3, false, 4>(P, st);
+    default: return launch_one<float, 64, 3, false, 6>(P, st);
     }
+}
+
+Variant shape_of(int pi, int variant, bool ns)
+{
+    if (ns)
+        return pi == 0 ? kNoShadowF64 : kNoShadowF32;
+    return pi == 0 ? kVariantsF64[variant] : kVariantsF32[variant];
 }
 
 int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double *M_dev,
@@ -601,9 +612,7 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     const int pi = precision == MBS_PO_FP64 ? 0 : 1;
     if (variant < 0)
         variant = ctx->variant[pi];
-    if (ns)
-        variant = 0;
-    const Variant V = pi == 0 ? kVariantsF64[variant] : kVariantsF32[variant];
+    const Variant V = shape_of(pi, variant, ns);
     // the autotuner's slice: the first orient_limit orientations of set 0
     const int n_sets = orient_limit > 0 ? 1 : s->n_sets;
     const int per_set = orient_limit > 0 ? std::min(orient_limit, s->orient_per_set) : s->orient_per_set;
@@ -1262,8 +1271,8 @@ extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_stag
                     "no-allocation scratch holds " + std::to_string(kNoAllocScratchBytes)
                     + " bytes (use mbs_po_diffract_staged)");
     const int pi = precision == MBS_PO_FP64 ? 0 : 1;
-    const int variant = ns ? 0 : ctx->variant[pi];
-    const Variant V = pi == 0 ? kVariantsF64[variant] : kVariantsF32[variant];
+    const int variant = ctx->variant[pi];
+    const Variant V = shape_of(pi, variant, ns);
     LaunchPlan L = plan_launch(nAz, nT, s->n_orient, V.tpb * V.dpt, V.minb);
     // fewer, larger orientation chunks when the fixed scratch is short
     const int max_chunks = (int)std::min<size_t>((kNoAllocScratchDoubles - kNoAllocHead) / (plane * sets), 64);
