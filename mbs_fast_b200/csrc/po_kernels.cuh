@@ -885,6 +885,74 @@ __device__ __noinline__ bool beam_rare(const KParams &P, int gbeam, const SBeamR
     return ok;
 }
 
+// A pair marked only for a nearly singular edge (|C_e| <= eps): the fast
+// path's arithmetic from the shared-memory records, with every edge whose
+// |C_e| <= eps taken in the stable form of the same quotient,
+//   (e^{i phi_{e+1}} - e^{i phi_e}) / C_e = e^{i phi_e} (e^{iz} - 1) / C_e,
+//   z = k C_e delta_e (delta_e: the edge's x or y extent on the branch),
+// in FP64 (stable_edge, the reference's singular correction,
+// GpuDiffraction.cu:951-970).  The result equals the general evaluation
+// (beam_general) without its global-memory walk over the beam; the edge
+// extents come from the two vertices' general records.  Writes the Jones
+// contribution to out[0..7] (stride `stride`); returns false when the sum
+// is not finite, where the general evaluation drops the beam.
+template <typename T>
+__device__ __noinline__ bool beam_sing(const KParams &P, const SBeamRaw<T> *sbr, const SVertRaw<T> *sv,
+                                       int vglob, double st, double ct, T *out, int stride)
+{
+    constexpr bool kF32 = sizeof(T) == 4;
+    BeamRegs<T> b;
+    load_beam(*sbr, b);
+    const T stT = (T)st, ctT = (T)ct;
+    const T A = fma(stT, b.a[0], fma(ctT, b.a[1], b.a[2]));
+    const T B = fma(stT, b.a[3], fma(ctT, b.a[4], b.a[5]));
+    const bool useX = fabs(B) > fabs(A);
+    const T X1 = useX ? B : A, X2 = useX ? A : B;
+    const T eps = (T)(kF32 ? P.wc.eps1_f32 : P.wc.eps1);
+    const SVertRaw<T> *v = sv + b.vs;
+    const DevVert *gv = P.verts + vglob + b.vs;
+    VertRegs w;
+    T syx, sxy, c0, s0;
+    load_vert(v[0], w, syx, sxy);
+    vertex_phasor(st, ct, w, s0, c0);
+    T cprev = c0, sprev = s0, sr = T(0), si = T(0);
+    double dr = 0.0, di = 0.0;
+    for (int e = 0; e < b.nv; ++e) {
+        const int en = (e + 1 < b.nv) ? e + 1 : 0;
+        const T syx_e = syx, sxy_e = sxy;
+        T cn = c0, sn = s0;
+        if (en != 0) {
+            load_vert(v[en], w, syx, sxy);
+            vertex_phasor(st, ct, w, sn, cn);
+        }
+        const T coef = fma(useX ? syx_e : sxy_e, X1, X2);
+        if (fabs(coef) > eps) {
+            const T inv = rcp_t(coef);
+            sr = fma(cn - cprev, inv, sr);
+            si = fma(sn - sprev, inv, si);
+        } else if (fabs(coef) <= eps) {           // NaN: invalid edge, dropped
+            const double delta = useX ? gv[en].x - gv[e].x : gv[en].y - gv[e].y;
+            stable_edge((double)cprev, (double)sprev, delta, (double)coef, P.wc.k, dr, di);
+        }
+        cprev = cn;
+        sprev = sn;
+    }
+    const T m = rcp_t(useX ? B : -A);
+    const T s_r = (sr + (T)dr) * m, s_i = (si + (T)di) * m;
+    if (!isfinite(s_r) || !isfinite(s_i))
+        return false;
+    T Pm[24];
+    load_P(*sbr, Pm);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const T rr = fma(stT, Pm[16 + 2 * e], fma(ctT, Pm[8 + 2 * e], Pm[2 * e]));
+        const T ri = fma(stT, Pm[17 + 2 * e], fma(ctT, Pm[9 + 2 * e], Pm[2 * e + 1]));
+        out[(2 * e) * stride] = fma(s_r, rr, -s_i * ri);
+        out[(2 * e + 1) * stride] = fma(s_r, ri, s_i * rr);
+    }
+    return true;
+}
+
 // Accumulator of the coherent Jones sum of one orientation for one
 // direction.  FP32: plain sums over blocks of kFlushEvery beams in
 // registers, folded into a Kahan-compensated running sum kept in shared
@@ -1102,7 +1170,12 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                         const T A = fma(stT[d], b.a[0], fma(ctT[d], b.a[1], b.a[2]));
                         const T B = fma(stT[d], b.a[3], fma(ctT[d], b.a[4], b.a[5]));
                         const bool near = kF32 && !general[d] && (float)(A * A + B * B) <= b.nearr2;
-                        if (beam_rare<T>(P, b.gbeam, &sb[j], p, t[d], near, rslot, TPB)) {
+                        const bool cand = fabs(fma(A, b.slab[0], B * b.slab[1])) <= T(1)
+                                       && fabs(fma(A, b.slab[2], B * b.slab[3])) <= T(1);
+                        const bool ok = (general[d] || near || cand)
+                                      ? beam_rare<T>(P, b.gbeam, &sb[j], p, t[d], near, rslot, TPB)
+                                      : beam_sing<T>(P, &sb[j], sv, vb0, st[d], ct[d], rslot, TPB);
+                        if (ok) {
                             T dj[8];
 #pragma unroll
                             for (int q = 0; q < 8; ++q)
@@ -1128,6 +1201,9 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
         // Mueller of this orientation, weighted, added to the chunk's
         // partial plane in global memory (coalesced: consecutive threads
         // own consecutive directions; the first orientation initialises).
+        // The adds are reductions performed in L2 (no load on the thread's
+        // path); each partial element has a single owner thread, whose adds
+        // reach it in program order, so the sums are deterministic.
         const double wgt = P.weight[o] * 0.25;
 #pragma unroll
         for (int d = 0; d < DPT; ++d) {
@@ -1160,7 +1236,7 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                 } else {
 #pragma unroll
                     for (int i = 0; i < 16; ++i)
-                        out[i * G] += m[i];
+                        atomicAdd(out + i * G, m[i]);
                 }
             }
         }
