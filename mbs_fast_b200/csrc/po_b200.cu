@@ -67,8 +67,8 @@ struct mbs_po_staged {
     Arena arena;
     DevBeam *beams = nullptr;
     DevVert *verts = nullptr;
-    BeamRec *brec = nullptr;
-    VertRec *vrec = nullptr;
+    double *brec = nullptr;        // [kBrecWords][n_beams]
+    double *vrec = nullptr;        // [kVrecWords][n_verts]
     double *moments = nullptr;
     int32_t *vbeg = nullptr;
     int32_t *beam_off = nullptr;
@@ -411,8 +411,8 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     const size_t o_beams = 0;
     const size_t o_verts = o_beams + align256(iB * sizeof(DevBeam));
     const size_t o_brec = o_verts + align256(iV * sizeof(DevVert));
-    const size_t o_vrec = o_brec + align256(iB * sizeof(BeamRec));
-    const size_t o_mom = o_vrec + align256(iV * sizeof(VertRec));
+    const size_t o_vrec = o_brec + align256(iB * kBrecWords * sizeof(double));
+    const size_t o_mom = o_vrec + align256(iV * kVrecWords * sizeof(double));
     const size_t o_vbeg = o_mom + align256(iB * kNumMoments * sizeof(double));
     const size_t o_boff = o_vbeg + align256((iB + 1) * sizeof(int32_t));
     const size_t o_w = o_boff + align256((iO + 1) * sizeof(int32_t));
@@ -422,8 +422,8 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     unsigned char *base = (unsigned char *)s->arena.base;
     s->beams = (DevBeam *)(base + o_beams);
     s->verts = (DevVert *)(base + o_verts);
-    s->brec = (BeamRec *)(base + o_brec);
-    s->vrec = (VertRec *)(base + o_vrec);
+    s->brec = (double *)(base + o_brec);
+    s->vrec = (double *)(base + o_vrec);
     s->moments = (double *)(base + o_mom);
     s->vbeg = (int32_t *)(base + o_vbeg);
     s->beam_off = (int32_t *)(base + o_boff);
@@ -477,6 +477,8 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
         P.verts = s->verts;
         P.brec = s->brec;
         P.vrec = s->vrec;
+        P.brec_stride = iB;
+        P.vrec_stride = iV;
         P.moments = s->moments;
         P.vbeg = s->vbeg;
         P.status = ctx->d_status;
@@ -627,6 +629,8 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     P.verts = s->verts;
     P.brec = s->brec;
     P.vrec = s->vrec;
+    P.brec_stride = s->n_beams;
+    P.vrec_stride = s->n_verts;
     P.moments = s->moments;
     P.vbeg = s->vbeg;
     P.beam_off = s->beam_off;
@@ -1144,9 +1148,9 @@ extern "C" int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams, i
     double budget = freeB * mem_fraction - fixed;
     int count = 0;
     const int end = std::min(beams->n_orient, start + std::max(0, max_count));
-    const double per_beam = sizeof(DevBeam) + sizeof(BeamRec) + kNumMoments * 8 + 4
+    const double per_beam = sizeof(DevBeam) + kBrecWords * 8 + kNumMoments * 8 + 4
                           + MBS_PO_GEOM_STRIDE * 8 + 8 + 1;
-    const double per_vert = sizeof(DevVert) + sizeof(VertRec) + 4 * 8 + 1;
+    const double per_vert = sizeof(DevVert) + kVrecWords * 8 + 4 * 8 + 1;
     for (int o = start; o < end; ++o) {
         const int64_t b0 = beams->beam_offsets[o], b1 = beams->beam_offsets[o + 1];
         const int64_t nv = b1 > b0 ? beams->vert_offsets[b1] - beams->vert_offsets[b0] : 0;
@@ -1289,6 +1293,8 @@ extern "C" int mbs_po_diffract_staged_noalloc(mbs_po_ctx *ctx, const mbs_po_stag
     P.verts = s->verts;
     P.brec = s->brec;
     P.vrec = s->vrec;
+    P.brec_stride = s->n_beams;
+    P.vrec_stride = s->n_verts;
     P.moments = s->moments;
     P.vbeg = s->vbeg;
     P.beam_off = s->beam_off;

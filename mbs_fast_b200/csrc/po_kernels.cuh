@@ -51,6 +51,58 @@ struct __align__(16) VertRec {
     double syx, sxy;
 };
 
+// Both record arrays are stored as structures of arrays: word w of record i
+// at base[w * stride + i], so the lanes of a warp that fill consecutive
+// records read consecutive words (full 32-byte sectors) instead of one
+// scattered sector per lane.
+constexpr int kBrecWords = 54;   // ab[8] Q[40] slab[4] (nearr2 | vbeg) (nv | 0)
+constexpr int kVrecWords = 6;    // X Y pc p0 syx sxy
+
+struct BrecRef {
+    const double *p;   // word 0 of the record
+    int64_t s;         // stride between words
+    __device__ __forceinline__ double ab(int i) const { return p[i * s]; }
+    __device__ __forceinline__ double Q(int i) const { return p[(8 + i) * s]; }
+    __device__ __forceinline__ double slab(int i) const { return p[(48 + i) * s]; }
+    __device__ __forceinline__ float nearr2() const { return __int_as_float(__double2loint(p[52 * s])); }
+    __device__ __forceinline__ int nv() const { return __double2loint(p[53 * s]); }
+};
+
+struct VrecRef {
+    const double *p;
+    int64_t s;
+    __device__ __forceinline__ double X() const { return p[0]; }
+    __device__ __forceinline__ double Y() const { return p[s]; }
+    __device__ __forceinline__ double pc() const { return p[2 * s]; }
+    __device__ __forceinline__ double p0() const { return p[3 * s]; }
+    __device__ __forceinline__ double syx() const { return p[4 * s]; }
+    __device__ __forceinline__ double sxy() const { return p[5 * s]; }
+};
+
+__device__ __forceinline__ void store_brec(double *base, int64_t s, int64_t i, const BeamRec &r)
+{
+    double *p = base + i;
+    for (int w = 0; w < 8; ++w)
+        p[w * s] = r.ab[w];
+    for (int w = 0; w < 40; ++w)
+        p[(8 + w) * s] = r.Q[w];
+    for (int w = 0; w < 4; ++w)
+        p[(48 + w) * s] = r.slab[w];
+    p[52 * s] = __hiloint2double(r.vbeg, __float_as_int(r.nearr2));
+    p[53 * s] = __hiloint2double(0, r.nv);
+}
+
+__device__ __forceinline__ void store_vrec(double *base, int64_t s, int64_t i, const VertRec &r)
+{
+    double *p = base + i;
+    p[0] = r.X;
+    p[s] = r.Y;
+    p[2 * s] = r.pc;
+    p[3 * s] = r.p0;
+    p[4 * s] = r.syx;
+    p[5 * s] = r.sxy;
+}
+
 constexpr double kInvalidSlope = 1.0e30;
 constexpr int kMomentOrder = 6;      // near-forward expansion order
 constexpr int kNumMoments = 28;      // (6+1)(6+2)/2
@@ -63,8 +115,9 @@ constexpr double kNearPhase = 0.25;
 struct KParams {
     const DevBeam *beams;
     const DevVert *verts;
-    const BeamRec *brec;
-    const VertRec *vrec;
+    const double *brec;        // [kBrecWords][brec_stride]
+    const double *vrec;        // [kVrecWords][vrec_stride]
+    int64_t brec_stride, vrec_stride;
     const double *moments;     // [n_beams][kNumMoments] c_pq = <x^p y^q>/(p! q!)
     const int32_t *vbeg;       // [n_beams+1]
     const int32_t *beam_off;   // [n_orient+1]
@@ -130,8 +183,9 @@ struct PackParams {
     WaveConst wc;
     DevBeam *beams;
     DevVert *verts;
-    BeamRec *brec;
-    VertRec *vrec;
+    double *brec;               // [kBrecWords][brec_stride]
+    double *vrec;               // [kVrecWords][vrec_stride]
+    int64_t brec_stride, vrec_stride;
     double *moments;
     int32_t *vbeg;
     int *status;   // set to 1 on a malformed beam
@@ -251,7 +305,7 @@ __global__ void po_pack_kernel(PackParams P)
         vr.p0 = kt * (d.a0 * x + d.b0 * y);
         vr.syx = (f & MBS_PO_EDGE_VALID_X) ? P.syx[v0l + e] : kInvalidSlope;
         vr.sxy = (f & MBS_PO_EDGE_VALID_Y) ? P.sxy[v0l + e] : kInvalidSlope;
-        P.vrec[v0 + e] = vr;
+        store_vrec(P.vrec, P.vrec_stride, v0 + e, vr);
     }
     // Small-phase candidates.  The reference's moment branch needs every
     // vertex phase |k(A x_v + B y_v)| <= 1e-3 (HandlerPO_fast.h:161-173); in
@@ -310,7 +364,7 @@ __global__ void po_pack_kernel(PackParams P)
     r.vbeg = (int32_t)v0;
     r.nv = nv;
     r.pad = 0;
-    P.brec[b] = r;
+    store_brec(P.brec, P.brec_stride, b, r);
 
     // Polygon moments I(p,q) = integral of x^p y^q over the aperture, by
     // Green's theorem over the edges (exact for polygons), normalised by
@@ -591,61 +645,61 @@ struct StageCfg {
     static constexpr size_t kBytes = kBeams * sizeof(SBeamRaw<T>) + kVerts * sizeof(SVertRaw<T>);
 };
 
-__device__ __forceinline__ void fill_beam(const BeamRec &r, double cp, double sp, int vs, int gbeam,
+__device__ __forceinline__ void fill_beam(const BrecRef &r, double cp, double sp, int vs, int gbeam,
                                           SBeamRaw<float> &s)
 {
     float a[6], P[24];
-    a[0] = (float)(-(cp * r.ab[0] + sp * r.ab[1])); a[1] = (float)r.ab[2]; a[2] = (float)r.ab[3];
-    a[3] = (float)(-(cp * r.ab[4] + sp * r.ab[5])); a[4] = (float)r.ab[6]; a[5] = (float)r.ab[7];
+    a[0] = (float)(-(cp * r.ab(0) + sp * r.ab(1))); a[1] = (float)r.ab(2); a[2] = (float)r.ab(3);
+    a[3] = (float)(-(cp * r.ab(4) + sp * r.ab(5))); a[4] = (float)r.ab(6); a[5] = (float)r.ab(7);
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
-        P[e] = (float)(sp * r.Q[e] + cp * r.Q[8 + e]);
-        P[8 + e] = (float)(-(cp * r.Q[16 + e] + sp * r.Q[24 + e]));
-        P[16 + e] = (float)r.Q[32 + e];
+        P[e] = (float)(sp * r.Q(e) + cp * r.Q(8 + e));
+        P[8 + e] = (float)(-(cp * r.Q(16 + e) + sp * r.Q(24 + e)));
+        P[16 + e] = (float)r.Q(32 + e);
     }
     s.q[0] = make_float4(a[0], a[1], a[2], a[3]);
-    s.q[1] = make_float4(a[4], a[5], (float)r.slab[0], (float)r.slab[1]);
-    s.q[2] = make_float4((float)r.slab[2], (float)r.slab[3], r.nearr2, __int_as_float(r.nv));
+    s.q[1] = make_float4(a[4], a[5], (float)r.slab(0), (float)r.slab(1));
+    s.q[2] = make_float4((float)r.slab(2), (float)r.slab(3), r.nearr2(), __int_as_float(r.nv()));
 #pragma unroll
     for (int i = 0; i < 6; ++i)
         s.q[3 + i] = make_float4(P[4 * i], P[4 * i + 1], P[4 * i + 2], P[4 * i + 3]);
     s.q[9] = make_float4(__int_as_float(gbeam), __int_as_float(vs), 0.f, 0.f);
 }
 
-__device__ __forceinline__ void fill_beam(const BeamRec &r, double cp, double sp, int vs, int gbeam,
+__device__ __forceinline__ void fill_beam(const BrecRef &r, double cp, double sp, int vs, int gbeam,
                                           SBeamRaw<double> &s)
 {
-    s.q[0] = make_double2(-(cp * r.ab[0] + sp * r.ab[1]), r.ab[2]);
-    s.q[1] = make_double2(r.ab[3], -(cp * r.ab[4] + sp * r.ab[5]));
-    s.q[2] = make_double2(r.ab[6], r.ab[7]);
-    s.q[3] = make_double2(r.slab[0], r.slab[1]);
-    s.q[4] = make_double2(r.slab[2], r.slab[3]);
+    s.q[0] = make_double2(-(cp * r.ab(0) + sp * r.ab(1)), r.ab(2));
+    s.q[1] = make_double2(r.ab(3), -(cp * r.ab(4) + sp * r.ab(5)));
+    s.q[2] = make_double2(r.ab(6), r.ab(7));
+    s.q[3] = make_double2(r.slab(0), r.slab(1));
+    s.q[4] = make_double2(r.slab(2), r.slab(3));
 #pragma unroll
     for (int e = 0; e < 8; e += 2) {
-        s.q[5 + e / 2] = make_double2(sp * r.Q[e] + cp * r.Q[8 + e], sp * r.Q[e + 1] + cp * r.Q[9 + e]);
-        s.q[9 + e / 2] = make_double2(-(cp * r.Q[16 + e] + sp * r.Q[24 + e]),
-                                      -(cp * r.Q[17 + e] + sp * r.Q[25 + e]));
-        s.q[13 + e / 2] = make_double2(r.Q[32 + e], r.Q[33 + e]);
+        s.q[5 + e / 2] = make_double2(sp * r.Q(e) + cp * r.Q(8 + e), sp * r.Q(e + 1) + cp * r.Q(9 + e));
+        s.q[9 + e / 2] = make_double2(-(cp * r.Q(16 + e) + sp * r.Q(24 + e)),
+                                      -(cp * r.Q(17 + e) + sp * r.Q(25 + e)));
+        s.q[13 + e / 2] = make_double2(r.Q(32 + e), r.Q(33 + e));
     }
-    s.q[17] = make_double2(__hiloint2double(r.nv, __float_as_int(r.nearr2)),
+    s.q[17] = make_double2(__hiloint2double(r.nv(), __float_as_int(r.nearr2())),
                            __hiloint2double(vs, gbeam));
 }
 
 // FP32C: p0 carries the range-reduction constant 1.5*2^29 + 1/2, so the
 // phase sum st ps + ct pc + p0 lands directly in [2^29, 2^30), where the low
 // 23 mantissa bits hold frac(u + 1/2) (three roundings of at most 2^-24 turn).
-__device__ __forceinline__ void fill_vert(const VertRec &r, double cp, double sp, SVertRaw<float> &w)
+__device__ __forceinline__ void fill_vert(const VrecRef &r, double cp, double sp, SVertRaw<float> &w)
 {
-    w.q[0] = make_double2(-(cp * r.X + sp * r.Y), r.pc);
-    w.q[1] = make_double2(r.p0 + (kMagic29 + 0.5),
-                          __hiloint2double(__float_as_int((float)r.sxy), __float_as_int((float)r.syx)));
+    w.q[0] = make_double2(-(cp * r.X() + sp * r.Y()), r.pc());
+    w.q[1] = make_double2(r.p0() + (kMagic29 + 0.5),
+                          __hiloint2double(__float_as_int((float)r.sxy()), __float_as_int((float)r.syx())));
 }
 
-__device__ __forceinline__ void fill_vert(const VertRec &r, double cp, double sp, SVertRaw<double> &w)
+__device__ __forceinline__ void fill_vert(const VrecRef &r, double cp, double sp, SVertRaw<double> &w)
 {
-    w.q[0] = make_double2(-(cp * r.X + sp * r.Y), r.pc);
-    w.q[1] = make_double2(r.p0, r.syx);
-    w.q[2] = make_double2(r.sxy, 0.0);
+    w.q[0] = make_double2(-(cp * r.X() + sp * r.Y()), r.pc());
+    w.q[1] = make_double2(r.p0(), r.syx());
+    w.q[2] = make_double2(r.sxy(), 0.0);
 }
 
 __device__ __forceinline__ void load_beam(const SBeamRaw<float> &s, BeamRegs<float> &b)
@@ -1073,12 +1127,10 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
             const int nb = be - bs;
             const int nvs = P.vbeg[be] - vb0;
             __syncthreads();   // previous stage fully consumed
-            for (int i = threadIdx.x; i < nb; i += TPB) {
-                const BeamRec &r = P.brec[bs + i];
-                fill_beam(r, cp, sp, r.vbeg - vb0, bs + i, sb[i]);
-            }
+            for (int i = threadIdx.x; i < nb; i += TPB)
+                fill_beam(BrecRef{P.brec + bs + i, P.brec_stride}, cp, sp, P.vbeg[bs + i] - vb0, bs + i, sb[i]);
             for (int i = threadIdx.x; i < nvs; i += TPB)
-                fill_vert(P.vrec[vb0 + i], cp, sp, sv[i]);
+                fill_vert(VrecRef{P.vrec + vb0 + i, P.vrec_stride}, cp, sp, sv[i]);
             __syncthreads();
             // Hot loop: every (beam, direction) pair on the vectorised path;
             // pairs that need FP64 (near-forward zone, small-phase candidates,
