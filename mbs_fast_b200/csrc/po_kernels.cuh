@@ -1140,7 +1140,12 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
 #pragma unroll
             for (int d = 0; d < DPT; ++d)
                 bits[d] = 0u;
-            for (int j = 0; j < nb; ++j) {
+            // blocks of kFlushEvery beams: the mask store and the Kahan fold
+            // run between blocks, not as tests inside the beam loop
+            static_assert(32 % kFlushEvery == 0, "mask words hold whole blocks");
+            for (int j0 = 0; j0 < nb; j0 += kFlushEvery) {
+            const int j1 = min(nb, j0 + kFlushEvery);
+            for (int j = j0; j < j1; ++j) {
                 BeamRegs<T> b;
                 load_beam(sb[j], b);
                 T X1[DPT], X2[DPT], sr[DPT], si[DPT], mn[DPT], mden[DPT];
@@ -1191,22 +1196,23 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                         }
                     }
                 }
-                if ((j & 31) == 31 || j + 1 == nb) {
+            }
+            if ((j1 & 31) == 0 || j1 == nb) {
 #pragma unroll
-                    for (int d = 0; d < DPT; ++d) {
-                        rmask[(d * kMaskWords + (j >> 5)) * TPB + threadIdx.x] = bits[d];
-                        bits[d] = 0u;
-                    }
+                for (int d = 0; d < DPT; ++d) {
+                    rmask[(d * kMaskWords + ((j1 - 1) >> 5)) * TPB + threadIdx.x] = bits[d];
+                    bits[d] = 0u;
                 }
-                if (kF32 && (j & (kFlushEvery - 1)) == kFlushEvery - 1) {
+            }
+            if (kF32 && j1 - j0 == kFlushEvery) {
 #pragma unroll
-                    for (int d = 0; d < DPT; ++d) {
-                        const int slot = d * TPB + threadIdx.x;
-                        J[d].fold(Ksm + slot, Ksm + 8 * kDirs + slot, kDirs);
-                        if (NS)
-                            Jn[NS ? d : 0].fold(Ksm + 16 * kDirs + slot, Ksm + 24 * kDirs + slot, kDirs);
-                    }
+                for (int d = 0; d < DPT; ++d) {
+                    const int slot = d * TPB + threadIdx.x;
+                    J[d].fold(Ksm + slot, Ksm + 8 * kDirs + slot, kDirs);
+                    if (NS)
+                        Jn[NS ? d : 0].fold(Ksm + 16 * kDirs + slot, Ksm + 24 * kDirs + slot, kDirs);
                 }
+            }
             }
             // FP64 pass over this thread's marked pairs of the stage.
             const int words = (nb + 31) >> 5;
