@@ -617,7 +617,8 @@ struct SBeamRaw;
 
 template <>
 struct __align__(16) SBeamRaw<float> {
-    float4 q[10];   // a0-3 | a4 a5 slab0 slab1 | slab2 slab3 nearr2 nv | P[24] | gbeam vs
+    float4 q[10];   // a0 a3 a1 a4 | a2 a5 slab0 slab1 | slab2 slab3 nearr2 nv | P[24] | gbeam vs
+                    // ((a0, a3), (a1, a4), (a2, a5): operand pairs of the packed A, B)
 };
 
 template <>
@@ -657,8 +658,8 @@ __device__ __forceinline__ void fill_beam(const BrecRef &r, double cp, double sp
         P[8 + e] = (float)(-(cp * r.Q(16 + e) + sp * r.Q(24 + e)));
         P[16 + e] = (float)r.Q(32 + e);
     }
-    s.q[0] = make_float4(a[0], a[1], a[2], a[3]);
-    s.q[1] = make_float4(a[4], a[5], (float)r.slab(0), (float)r.slab(1));
+    s.q[0] = make_float4(a[0], a[3], a[1], a[4]);
+    s.q[1] = make_float4(a[2], a[5], (float)r.slab(0), (float)r.slab(1));
     s.q[2] = make_float4((float)r.slab(2), (float)r.slab(3), r.nearr2(), __int_as_float(r.nv()));
 #pragma unroll
     for (int i = 0; i < 6; ++i)
@@ -705,7 +706,7 @@ __device__ __forceinline__ void fill_vert(const VrecRef &r, double cp, double sp
 __device__ __forceinline__ void load_beam(const SBeamRaw<float> &s, BeamRegs<float> &b)
 {
     const float4 q0 = s.q[0], q1 = s.q[1], q2 = s.q[2], q9 = s.q[9];
-    b.a[0] = q0.x; b.a[1] = q0.y; b.a[2] = q0.z; b.a[3] = q0.w; b.a[4] = q1.x; b.a[5] = q1.y;
+    b.a[0] = q0.x; b.a[3] = q0.y; b.a[1] = q0.z; b.a[4] = q0.w; b.a[2] = q1.x; b.a[5] = q1.y;
     b.slab[0] = q1.z; b.slab[1] = q1.w; b.slab[2] = q2.x; b.slab[3] = q2.y;
     b.nearr2 = q2.z;
     b.nv = __float_as_int(q2.w);
@@ -848,6 +849,47 @@ __device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const doub
     }
 }
 
+// FP32C form of edge_sums_fixed: the phasors of a vertex as (cos, sin)
+// pairs, the edge differences as one packed FP32x2 operation (the same
+// rounding as two subtractions: (-1) c_e + c_{e+1} is exact before its
+// single rounding).
+template <int DPT, int NV>
+__device__ __forceinline__ void edge_sums_fixed_f32(const SVertRaw<float> *v, const double *st,
+                                                    const double *ct, const float *X1, const float *X2,
+                                                    const bool *useX, float *sr, float *si, float *mn)
+{
+    float2 cs[DPT][NV];
+    float syx[NV], sxy[NV];
+#pragma unroll
+    for (int e = 0; e < NV; ++e) {
+        VertRegs w;
+        load_vert(v[e], w, syx[e], sxy[e]);
+#pragma unroll
+        for (int d = 0; d < DPT; ++d)
+            vertex_phasor(st[d], ct[d], w, cs[d][e].y, cs[d][e].x);
+    }
+    const float2 m1 = make_float2(-1.f, -1.f);
+#pragma unroll
+    for (int d = 0; d < DPT; ++d) {
+        mn[d] = 1e30f;
+        sr[d] = 0.f;
+        si[d] = 0.f;
+    }
+#pragma unroll
+    for (int e = 0; e < NV; ++e) {
+        const int en = (e + 1 < NV) ? e + 1 : 0;
+#pragma unroll
+        for (int d = 0; d < DPT; ++d) {
+            const float coef = fmaf(useX[d] ? syx[e] : sxy[e], X1[d], X2[d]);
+            const float inv = rcp32(coef);
+            mn[d] = fminf(mn[d], fabsf(coef));
+            const float2 df = __ffma2_rn(cs[d][e], m1, cs[d][en]);
+            sr[d] = fmaf(df.x, inv, sr[d]);
+            si[d] = fmaf(df.y, inv, si[d]);
+        }
+    }
+}
+
 template <typename T, int DPT>
 __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, const double *st,
                                                const double *ct, const T *X1, const T *X2,
@@ -892,12 +934,22 @@ __device__ __forceinline__ void edge_sums(const SVertRaw<T> *v, int nv, const do
                                           const double *ct, const T *X1, const T *X2,
                                           const bool *useX, T *sr, T *si, T *mn)
 {
-    switch (nv) {   // warp-uniform: every lane evaluates the same beam
-    case 3: edge_sums_fixed<T, DPT, 3>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-    case 4: edge_sums_fixed<T, DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-    case 5: edge_sums_fixed<T, DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-    case 6: edge_sums_fixed<T, DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-    default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn); break;
+    if constexpr (sizeof(T) == 4) {
+        switch (nv) {   // warp-uniform: every lane evaluates the same beam
+        case 3: edge_sums_fixed_f32<DPT, 3>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+        case 4: edge_sums_fixed_f32<DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+        case 5: edge_sums_fixed_f32<DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+        case 6: edge_sums_fixed_f32<DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+        default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn); break;
+        }
+    } else {
+        switch (nv) {
+        case 3: edge_sums_fixed<T, DPT, 3>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+        case 4: edge_sums_fixed<T, DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+        case 5: edge_sums_fixed<T, DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+        case 6: edge_sums_fixed<T, DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn); break;
+        default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn); break;
+        }
     }
 }
 
@@ -1098,6 +1150,12 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
         stT[d] = (T)st[d];
         ctT[d] = (T)ct[d];
     }
+    float2 st2[DPT], ct2[DPT];   // FP32C: (sin t, sin t), (cos t, cos t) operand pairs
+#pragma unroll
+    for (int d = 0; d < DPT; ++d) {
+        st2[d] = make_float2((float)stT[d], (float)stT[d]);
+        ct2[d] = make_float2((float)ctT[d], (float)ctT[d]);
+    }
     const size_t G = (size_t)P.n_az * P.n_t;
 
     for (int o = o0; o < o1; ++o) {
@@ -1152,8 +1210,17 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                 bool useX[DPT], rare[DPT];
 #pragma unroll
                 for (int d = 0; d < DPT; ++d) {
-                    const T A = fma(stT[d], b.a[0], fma(ctT[d], b.a[1], b.a[2]));
-                    const T B = fma(stT[d], b.a[3], fma(ctT[d], b.a[4], b.a[5]));
+                    T A, B;
+                    if constexpr (kF32) {
+                        const float2 ab = __ffma2_rn(st2[d], make_float2(b.a[0], b.a[3]),
+                                                     __ffma2_rn(ct2[d], make_float2(b.a[1], b.a[4]),
+                                                                make_float2(b.a[2], b.a[5])));
+                        A = ab.x;
+                        B = ab.y;
+                    } else {
+                        A = fma(stT[d], b.a[0], fma(ctT[d], b.a[1], b.a[2]));
+                        B = fma(stT[d], b.a[3], fma(ctT[d], b.a[4], b.a[5]));
+                    }
                     useX[d] = fabs(B) > fabs(A);
                     X1[d] = useX[d] ? B : A;
                     X2[d] = useX[d] ? A : B;
@@ -1180,6 +1247,29 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                 for (int h = 0; h < 2; ++h) {
                     T p0[4], pc[4], ps[4];
                     load_P_pair(sb[j], h, p0, pc, ps);
+                    if constexpr (kF32 && !NS) {
+                        // packed (re, im) pairs: R = P0 + cos t Pc + sin t Ps, then
+                        // J += s R as (-s_i, s_i) (R_i, R_r) + (s_r, s_r) (R_r, R_i),
+                        // the scalar form's operations lane by lane
+#pragma unroll
+                        for (int d = 0; d < DPT; ++d) {
+                            const float2 srr = make_float2(s_r[d], s_r[d]);
+                            const float2 nsi = make_float2(-s_i[d], s_i[d]);
+#pragma unroll
+                            for (int e = 0; e < 2; ++e) {
+                                const int q = 4 * h + 2 * e;
+                                const float2 R = __ffma2_rn(st2[d], make_float2(ps[2 * e], ps[2 * e + 1]),
+                                                            __ffma2_rn(ct2[d], make_float2(pc[2 * e], pc[2 * e + 1]),
+                                                                       make_float2(p0[2 * e], p0[2 * e + 1])));
+                                float2 jv = make_float2(J[d].b[q], J[d].b[q + 1]);
+                                jv = __ffma2_rn(nsi, make_float2(R.y, R.x), jv);
+                                jv = __ffma2_rn(srr, R, jv);
+                                J[d].b[q] = jv.x;
+                                J[d].b[q + 1] = jv.y;
+                            }
+                        }
+                        continue;
+                    }
 #pragma unroll
                     for (int d = 0; d < DPT; ++d) {
 #pragma unroll
