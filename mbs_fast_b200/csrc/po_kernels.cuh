@@ -890,6 +890,113 @@ __device__ __forceinline__ void edge_sums_fixed_f32(const SVertRaw<float> *v, co
     }
 }
 
+// FP32C edge sums in two parts.  The head (vertices 0-2, edges 0 and 1:
+// every aperture has at least three vertices) sits in the beam loop's
+// straight-line code with the beam's A, B and zone tests, so their chains
+// interleave; the tail (the remaining vertices and edges, the closing edge
+// back to vertex 0) follows the warp-uniform switch on the vertex count.
+// Operations and their order are those of edge_sums_fixed_f32.
+__device__ __forceinline__ void edge_step_f32(float2 a, float2 b, float slope, float X1, float X2,
+                                              float &sr, float &si, float &mn)
+{
+    const float coef = fmaf(slope, X1, X2);
+    const float inv = rcp32(coef);
+    mn = fminf(mn, fabsf(coef));
+    const float2 df = __ffma2_rn(a, make_float2(-1.f, -1.f), b);
+    sr = fmaf(df.x, inv, sr);
+    si = fmaf(df.y, inv, si);
+}
+
+template <int DPT>
+struct EdgeHead {
+    float2 c0[DPT], c2[DPT];   // phasors of vertices 0 and 2
+    float syx2, sxy2;          // slopes of vertex 2's edge
+};
+
+template <int DPT>
+__device__ __forceinline__ void edge_head_f32(const SVertRaw<float> *v, const double *st, const double *ct,
+                                              const float *X1, const float *X2, const bool *useX,
+                                              EdgeHead<DPT> &h, float *sr, float *si, float *mn)
+{
+    float2 c1[DPT];
+    float syx0, sxy0, syx1, sxy1;
+    VertRegs w0, w1, w2;
+    load_vert(v[0], w0, syx0, sxy0);
+    load_vert(v[1], w1, syx1, sxy1);
+    load_vert(v[2], w2, h.syx2, h.sxy2);
+#pragma unroll
+    for (int d = 0; d < DPT; ++d) {
+        vertex_phasor(st[d], ct[d], w0, h.c0[d].y, h.c0[d].x);
+        vertex_phasor(st[d], ct[d], w1, c1[d].y, c1[d].x);
+        vertex_phasor(st[d], ct[d], w2, h.c2[d].y, h.c2[d].x);
+    }
+#pragma unroll
+    for (int d = 0; d < DPT; ++d) {
+        mn[d] = 1e30f;
+        sr[d] = 0.f;
+        si[d] = 0.f;
+        edge_step_f32(h.c0[d], c1[d], useX[d] ? syx0 : sxy0, X1[d], X2[d], sr[d], si[d], mn[d]);
+        edge_step_f32(c1[d], h.c2[d], useX[d] ? syx1 : sxy1, X1[d], X2[d], sr[d], si[d], mn[d]);
+    }
+}
+
+template <int DPT, int NV>
+__device__ __forceinline__ void edge_tail_fixed_f32(const SVertRaw<float> *v, const double *st, const double *ct,
+                                                    const float *X1, const float *X2, const bool *useX,
+                                                    const EdgeHead<DPT> &h, float *sr, float *si, float *mn)
+{
+    constexpr int kM = NV > 3 ? NV - 3 : 1;
+    float2 cs[DPT][kM];
+    float syx[kM], sxy[kM];
+#pragma unroll
+    for (int e = 3; e < NV; ++e) {
+        VertRegs w;
+        load_vert(v[e], w, syx[e - 3], sxy[e - 3]);
+#pragma unroll
+        for (int d = 0; d < DPT; ++d)
+            vertex_phasor(st[d], ct[d], w, cs[d][e - 3].y, cs[d][e - 3].x);
+    }
+#pragma unroll
+    for (int e = 2; e < NV; ++e) {
+#pragma unroll
+        for (int d = 0; d < DPT; ++d) {
+            const float2 a = e == 2 ? h.c2[d] : cs[d][e - 3];
+            const float2 b = e + 1 < NV ? cs[d][e - 2] : h.c0[d];
+            const float slope = e == 2 ? (useX[d] ? h.syx2 : h.sxy2)
+                                       : (useX[d] ? syx[e - 3] : sxy[e - 3]);
+            edge_step_f32(a, b, slope, X1[d], X2[d], sr[d], si[d], mn[d]);
+        }
+    }
+}
+
+template <int DPT>
+__device__ __forceinline__ void edge_tail_loop_f32(const SVertRaw<float> *v, int nv, const double *st,
+                                                   const double *ct, const float *X1, const float *X2,
+                                                   const bool *useX, const EdgeHead<DPT> &h, float *sr,
+                                                   float *si, float *mn)
+{
+    float2 prev[DPT];
+#pragma unroll
+    for (int d = 0; d < DPT; ++d)
+        prev[d] = h.c2[d];
+    float syx = h.syx2, sxy = h.sxy2;
+    for (int e = 2; e < nv; ++e) {
+        const bool last = e + 1 == nv;
+        const float syx_e = syx, sxy_e = sxy;
+        VertRegs w;
+        if (!last)
+            load_vert(v[e + 1], w, syx, sxy);
+#pragma unroll
+        for (int d = 0; d < DPT; ++d) {
+            float2 nx = h.c0[d];
+            if (!last)
+                vertex_phasor(st[d], ct[d], w, nx.y, nx.x);
+            edge_step_f32(prev[d], nx, useX[d] ? syx_e : sxy_e, X1[d], X2[d], sr[d], si[d], mn[d]);
+            prev[d] = nx;
+        }
+    }
+}
+
 template <typename T, int DPT>
 __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, const double *st,
                                                const double *ct, const T *X1, const T *X2,
@@ -1230,7 +1337,20 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                                    && fabs(fma(A, b.slab[2], B * b.slab[3])) <= T(1);
                     rare[d] = general[d] || near || cand;
                 }
-                edge_sums<T, DPT>(sv + b.vs, b.nv, st, ct, X1, X2, useX, sr, si, mn);
+                if constexpr (kF32) {
+                    EdgeHead<DPT> eh;
+                    const SVertRaw<float> *vb = sv + b.vs;
+                    edge_head_f32<DPT>(vb, st, ct, X1, X2, useX, eh, sr, si, mn);
+                    switch (b.nv) {   // warp-uniform: every lane evaluates the same beam
+                    case 3: edge_tail_fixed_f32<DPT, 3>(vb, st, ct, X1, X2, useX, eh, sr, si, mn); break;
+                    case 4: edge_tail_fixed_f32<DPT, 4>(vb, st, ct, X1, X2, useX, eh, sr, si, mn); break;
+                    case 5: edge_tail_fixed_f32<DPT, 5>(vb, st, ct, X1, X2, useX, eh, sr, si, mn); break;
+                    case 6: edge_tail_fixed_f32<DPT, 6>(vb, st, ct, X1, X2, useX, eh, sr, si, mn); break;
+                    default: edge_tail_loop_f32<DPT>(vb, b.nv, st, ct, X1, X2, useX, eh, sr, si, mn); break;
+                    }
+                } else {
+                    edge_sums<T, DPT>(sv + b.vs, b.nv, st, ct, X1, X2, useX, sr, si, mn);
+                }
                 T s_r[DPT], s_i[DPT];
 #pragma unroll
                 for (int d = 0; d < DPT; ++d) {
