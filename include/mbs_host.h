@@ -55,6 +55,11 @@ const mbs_po_beams *mbs_host_batch_view(const mbs_host_batch *batch);
 double mbs_host_batch_extinction(const mbs_host_batch *batch, int o);
 /* Seconds spent tracing + preparing (wall clock). */
 double mbs_host_batch_trace_seconds(const mbs_host_batch *batch);
+/* Time split of the batch's production: out3[0] = seconds in the tracer
+ * (rotation, shadow beam, ScatterLight) and out3[1] = seconds in
+ * PrepareBeams, both summed over the worker threads; out3[2] = wall seconds
+ * of packing the prepared orientations into the flat batch. */
+int    mbs_host_batch_phase_seconds(const mbs_host_batch *batch, double *out3);
 void   mbs_host_batch_free(mbs_host_batch *batch);
 
 /* Particle symmetry (Particle::GetSymmetry): beta and gamma domains. */

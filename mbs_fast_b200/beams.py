@@ -33,6 +33,8 @@ class BeamBatch:
     abs_paths: np.ndarray | None = None
     extinction_ot: np.ndarray | None = None   # host CPU PreparedOrientation::extinctionOt
     trace_seconds: float = 0.0
+    # thread-summed tracer and PrepareBeams seconds, wall seconds of packing
+    phase_seconds: tuple = (0.0, 0.0, 0.0)
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -194,6 +196,8 @@ def _host():
         lib.mbs_host_batch_extinction.argtypes = [C.c_void_p, C.c_int]
         lib.mbs_host_batch_trace_seconds.restype = C.c_double
         lib.mbs_host_batch_trace_seconds.argtypes = [C.c_void_p]
+        lib.mbs_host_batch_phase_seconds.restype = C.c_int
+        lib.mbs_host_batch_phase_seconds.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         lib.mbs_host_batch_free.argtypes = [C.c_void_p]
         lib.mbs_host_symmetry.argtypes = [C.POINTER(abi.HostConfig), abi._dp, abi._dp, abi._dp]
         lib.mbs_host_sobol_orientations.argtypes = [C.c_int, C.c_uint, C.c_double, C.c_double,
@@ -245,6 +249,9 @@ def trace(cfg: ParticleConfig, beta, gamma, weight, alpha=None) -> BeamBatch:
         out.abs_paths = _copy(v.abs_paths, int(out.abs_offsets[-1]), np.float64)
         out.extinction_ot = np.array([lib.mbs_host_batch_extinction(handle, o) for o in range(n)])
         out.trace_seconds = lib.mbs_host_batch_trace_seconds(handle)
+        ph = (C.c_double * 3)()
+        if lib.mbs_host_batch_phase_seconds(handle, ph) == 0:
+            out.phase_seconds = (ph[0], ph[1], ph[2])
     finally:
         lib.mbs_host_batch_free(handle)
     return out

@@ -38,6 +38,9 @@ struct mbs_host_batch
     MbsPackedBeams packed;
     mbs_po_beams view;
     double trace_seconds = 0.0;
+    // thread-summed seconds in ScatterLight (with the shadow beam) and in
+    // PrepareBeams, and wall seconds of the packing into the flat batch
+    double phase_seconds[3] = {0.0, 0.0, 0.0};
 };
 
 namespace
@@ -196,6 +199,7 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
         master->PrepareForParallelTrace();
         bool failed = false;
         std::string failMsg;
+        double scatterSeconds = 0.0, prepareSeconds = 0.0;
         const int nThreads = cfg->n_threads > 0 ? cfg->n_threads : 0;
 #pragma omp parallel num_threads(nThreads > 0 ? nThreads : omp_get_max_threads())
         {
@@ -205,20 +209,25 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
                                    setup.handler->nTheta, master->m_wave);
             localHandler.ConfigureForThreadLocalPrepare(*setup.handler, localScatter);
             std::vector<Beam> localBeams;
+            double tScatter = 0.0, tPrepare = 0.0;
 #pragma omp for schedule(dynamic, 4)
             for (int i = 0; i < n_orient; ++i)
             {
                 try
                 {
+                    const auto a = std::chrono::steady_clock::now();
                     localParticle.Rotate(beta[i], gamma[i], alpha ? alpha[i] : 0.0);
                     if (!setup.tracer->shadowOff)
                         localScatter->FormShadowBeam(localBeams);
                     const bool ok = localScatter->ScatterLight(0, 0, localBeams);
+                    const auto b = std::chrono::steady_clock::now();
                     if (ok)
                         localHandler.PrepareBeams(localBeams, weight[i], prepared[i]);
                     else
                         prepared[i].sinZenith = weight[i];
                     localBeams.clear();
+                    tScatter += std::chrono::duration<double>(b - a).count();
+                    tPrepare += std::chrono::duration<double>(std::chrono::steady_clock::now() - b).count();
                 }
                 catch (const std::exception &e)
                 {
@@ -230,6 +239,11 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
                 }
             }
             delete localScatter;
+#pragma omp critical(mbs_host_trace_time)
+            {
+                scatterSeconds += tScatter;
+                prepareSeconds += tPrepare;
+            }
         }
         if (failed)
         {
@@ -238,7 +252,11 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
         }
         std::unique_ptr<mbs_host_batch> batch(new mbs_host_batch());
         std::string perr;
+        const auto tp = std::chrono::steady_clock::now();
         const int rc = mbs_pack_prepared(prepared, 0, n_orient, true, batch->packed, &perr);
+        batch->phase_seconds[0] = scatterSeconds;
+        batch->phase_seconds[1] = prepareSeconds;
+        batch->phase_seconds[2] = std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count();
         if (rc != MBS_PO_OK)
         {
             set_err(err, errlen, perr);
@@ -267,6 +285,15 @@ extern "C" double mbs_host_batch_extinction(const mbs_host_batch *batch, int o)
     if (!batch || o < 0 || o >= (int)batch->packed.extinction_ot.size())
         return 0.0;
     return batch->packed.extinction_ot[o];
+}
+
+extern "C" int mbs_host_batch_phase_seconds(const mbs_host_batch *batch, double *out3)
+{
+    if (!batch || !out3)
+        return MBS_PO_EINVAL;
+    for (int i = 0; i < 3; ++i)
+        out3[i] = batch->phase_seconds[i];
+    return MBS_PO_OK;
 }
 
 extern "C" double mbs_host_batch_trace_seconds(const mbs_host_batch *batch)
