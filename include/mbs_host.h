@@ -39,6 +39,10 @@ typedef struct mbs_host_config {
     int32_t     shadow_off;      /* --shadow_off                               */
     int32_t     legacy_sign;     /* --legacy_sign                              */
     int32_t     n_threads;       /* OpenMP threads for tracing (<=0: all)      */
+    int32_t     reference_prepare; /* 1: the reference's HandlerPO::PrepareBeams;
+                                    0: the producer's restatement of it (same
+                                    result bit for bit, edge tolerance and
+                                    facet tracks computed once)               */
 } mbs_host_config;
 
 typedef struct mbs_host_batch mbs_host_batch;

@@ -83,6 +83,7 @@ class HostConfig(C.Structure):
         ("wavelength", C.c_double), ("max_reflections", C.c_int32),
         ("cutoff_profile", C.c_int32), ("shadow_off", C.c_int32),
         ("legacy_sign", C.c_int32), ("n_threads", C.c_int32),
+        ("reference_prepare", C.c_int32),
     ]
 
 

@@ -164,6 +164,9 @@ class ParticleConfig:
     shadow_off: bool = False
     legacy_sign: bool = False
     n_threads: int = 0
+    # True: the reference's PrepareBeams; False: the producer's bit-identical
+    # restatement of it (host/prepare.cpp), several times faster
+    reference_prepare: bool = False
 
     PROFILES = ("legacy-default", "off", "safe", "balanced", "fast")
 
@@ -181,7 +184,7 @@ class ParticleConfig:
             absorption=int(self.absorption), wavelength=self.wavelength,
             max_reflections=self.max_reflections, cutoff_profile=self._profile(),
             shadow_off=int(self.shadow_off), legacy_sign=int(self.legacy_sign),
-            n_threads=self.n_threads)
+            n_threads=self.n_threads, reference_prepare=int(self.reference_prepare))
 
 
 def _host():

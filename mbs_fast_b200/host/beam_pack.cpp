@@ -41,10 +41,12 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
     const int nOrient = std::min(count, (int)prepared.size() - start);
 
     // Pass 1: sizes and validity (GpuDiffraction.cu:4290-4318 does the same
-    // scan and rejects beams without valid edge data).
-    int64_t nBeams = 0, nVerts = 0;
+    // scan and rejects beams without valid edge data), and each orientation's
+    // first beam, vertex and absorption-path slot.
+    std::vector<int64_t> ob(nOrient + 1, 0), ov(nOrient + 1, 0), oa(nOrient + 1, 0);
     for (int oi = 0; oi < nOrient; ++oi)
     {
+        int64_t nb = 0, nvt = 0, na = 0;
         for (const PreparedBeam &pb : prepared[start + oi].beams)
         {
             const int nv = pb.edgeData.nVertices;
@@ -53,10 +55,15 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
                 if (err) *err = "beam without valid edge data (nv=" + std::to_string(nv) + ")";
                 return MBS_PO_EBEAM;
             }
-            ++nBeams;
-            nVerts += nv;
+            ++nb;
+            nvt += nv;
+            na += (int64_t)pb.absorptionPaths.size();
         }
+        ob[oi + 1] = ob[oi] + nb;
+        ov[oi + 1] = ov[oi] + nvt;
+        oa[oi + 1] = oa[oi] + na;
     }
+    const int64_t nBeams = ob[nOrient], nVerts = ov[nOrient];
 
     out.beam_offsets.assign(nOrient + 1, 0);
     out.orient_weight.assign(nOrient, 0.0);
@@ -69,12 +76,11 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
     out.edge_flags.resize(nVerts);
     out.beam_geom.resize((size_t)nBeams * MBS_PO_GEOM_STRIDE);
     out.beam_flags.resize(nBeams);
-    out.max_vertices = 0;
     if (with_raw)
     {
         out.beam_raw.resize((size_t)nBeams * MBS_PO_RAW_STRIDE);
         out.abs_offsets.assign(nBeams + 1, 0);
-        out.abs_paths.clear();
+        out.abs_paths.resize(oa[nOrient]);
     }
     else
     {
@@ -83,10 +89,13 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
         out.abs_paths.clear();
     }
 
-    int64_t b = 0, v = 0;
+    // Pass 2: the orientations fill disjoint slices, in parallel.
+    int maxNv = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(max : maxNv)
     for (int oi = 0; oi < nOrient; ++oi)
     {
         const PreparedOrientation &po = prepared[start + oi];
+        int64_t b = ob[oi], v = ov[oi], a = oa[oi];
         out.beam_offsets[oi] = b;
         out.orient_weight[oi] = po.sinZenith;
         out.extinction_ot[oi] = po.extinctionOt;
@@ -95,8 +104,8 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
             const BeamEdgeData &ed = pb.edgeData;
             const int nv = ed.nVertices;
             out.vert_offsets[b] = v;
-            if (nv > out.max_vertices)
-                out.max_vertices = nv;
+            if (nv > maxNv)
+                maxNv = nv;
             for (int e = 0; e < nv; ++e)
             {
                 out.vx[v + e] = ed.x[e];
@@ -143,15 +152,16 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
                 if (!pb.isExternal && (pb.origBeam.nActs & 1))
                     sign = -sign;
                 r[MBS_PO_R_SIGN] = sign;
-                out.abs_offsets[b] = (int64_t)out.abs_paths.size();
-                out.abs_paths.insert(out.abs_paths.end(),
-                                     pb.absorptionPaths.begin(),
-                                     pb.absorptionPaths.end());
+                out.abs_offsets[b] = a;
+                for (double path : pb.absorptionPaths)
+                    out.abs_paths[a++] = path;
             }
             v += nv;
             ++b;
         }
     }
+    out.max_vertices = maxNv;
+    const int64_t b = nBeams, v = nVerts;
     out.beam_offsets[nOrient] = b;
     out.vert_offsets[nBeams] = v;
     if (with_raw)

@@ -10,6 +10,7 @@
 // prepared orientations are flattened with mbs_pack_prepared.
 #include "mbs_host.h"
 #include "beam_pack.h"
+#include "prepare.h"
 
 #include "HandlerPOTotal.h"
 #include "Hexagonal.h"
@@ -205,12 +206,13 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
         {
             Particle localParticle = *setup.particle;
             Scattering *localScatter = master->CloneFor(&localParticle, &setup.tracer->m_incidentLight);
-            HandlerPO localHandler(&localParticle, &setup.tracer->m_incidentLight,
-                                   setup.handler->nTheta, master->m_wave);
+            PrepareHandler localHandler(&localParticle, &setup.tracer->m_incidentLight,
+                                        setup.handler->nTheta, master->m_wave);
+            const bool referencePrepare = cfg->reference_prepare != 0;
             localHandler.ConfigureForThreadLocalPrepare(*setup.handler, localScatter);
             std::vector<Beam> localBeams;
             double tScatter = 0.0, tPrepare = 0.0;
-#pragma omp for schedule(dynamic, 4)
+#pragma omp for schedule(dynamic, 1)
             for (int i = 0; i < n_orient; ++i)
             {
                 try
@@ -221,8 +223,10 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
                         localScatter->FormShadowBeam(localBeams);
                     const bool ok = localScatter->ScatterLight(0, 0, localBeams);
                     const auto b = std::chrono::steady_clock::now();
-                    if (ok)
+                    if (ok && referencePrepare)
                         localHandler.PrepareBeams(localBeams, weight[i], prepared[i]);
+                    else if (ok)
+                        localHandler.Prepare(localBeams, weight[i], prepared[i]);
                     else
                         prepared[i].sinZenith = weight[i];
                     localBeams.clear();
