@@ -570,8 +570,9 @@ def main():
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
         "e2e_with_tracing": {"value": batch.n_orient / tp["wall_s"], "unit": "orientations/s",
                              "wall_s": tp["wall_s"], "host_trace_s": tp["trace_s"],
-                             "what": "reference tracer on all host cores, batches of 2048, "
-                                     "overlapped with FP32C diffraction on the device"},
+                             "what": "reference tracer and restated PrepareBeams on all host "
+                                     "cores, batches of 2048, overlapped with FP32C diffraction "
+                                     "on the device"},
         "gpu_launches": launches,
         "autotune": tuned,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
