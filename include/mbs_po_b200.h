@@ -243,10 +243,9 @@ int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams,
 
 /* Allocation-free variant of mbs_po_diffract_staged (no counterpart in the
  * reference).  For callers that cannot allocate device memory when they
- * diffract: work recorded into a CUDA graph while a stream is captured,
- * callers whose device memory belongs to an external pool or a fixed budget,
- * and real-time loops that must not stall on cudaMalloc/cudaFree (both
- * synchronise the device).  The orientation-chunk partials that
+ * diffract: callers whose device memory belongs to an external pool or a
+ * fixed budget that the library must not draw from, and real-time loops that
+ * must not stall on cudaMalloc/cudaFree (both can synchronise the device).  The orientation-chunk partials that
  * mbs_po_diffract_staged keeps in context memory it allocates on demand live
  * here in one fixed device array of MBS_PO_NOALLOC_SCRATCH_BYTES, which
  * every GPU that loads the library holds until the process exits.

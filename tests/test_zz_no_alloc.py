@@ -1,8 +1,9 @@
 """The allocation-free entry point mbs_po_diffract_staged_noalloc.
 
-It serves callers that cannot allocate device memory when they diffract
-(stream capture into a CUDA graph, externally owned memory pools, real-time
-loops that must not stall on cudaMalloc/cudaFree).  Its chunk partials live
+It serves callers that cannot allocate device memory when they diffract:
+callers whose device memory belongs to an external pool or a fixed budget,
+and real-time loops that must not stall on cudaMalloc/cudaFree, which can
+synchronise the device.  Its chunk partials live
 in the library's fixed device array instead of context memory, so it must
 give the same Mueller sums as mbs_po_diffract_staged, call after call, with
 the array reused.  This file is collected last (after every other test).
