@@ -1388,20 +1388,20 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                                 J[d].b[q + 1] = jv.y;
                             }
                         }
-                        continue;
-                    }
+                    } else {
 #pragma unroll
-                    for (int d = 0; d < DPT; ++d) {
+                        for (int d = 0; d < DPT; ++d) {
 #pragma unroll
-                        for (int e = 0; e < 2; ++e) {
-                            const int q = 4 * h + 2 * e;
-                            const T rr = fma(stT[d], ps[2 * e], fma(ctT[d], pc[2 * e], p0[2 * e]));
-                            const T ri = fma(stT[d], ps[2 * e + 1], fma(ctT[d], pc[2 * e + 1], p0[2 * e + 1]));
-                            J[d].b[q] = fma(s_r[d], rr, fma(-s_i[d], ri, J[d].b[q]));
-                            J[d].b[q + 1] = fma(s_r[d], ri, fma(s_i[d], rr, J[d].b[q + 1]));
-                            if (NS) {
-                                Jn[NS ? d : 0].b[q] = fma(fi * s_r[d], rr, fma(-fi * s_i[d], ri, Jn[NS ? d : 0].b[q]));
-                                Jn[NS ? d : 0].b[q + 1] = fma(fi * s_r[d], ri, fma(fi * s_i[d], rr, Jn[NS ? d : 0].b[q + 1]));
+                            for (int e = 0; e < 2; ++e) {
+                                const int q = 4 * h + 2 * e;
+                                const T rr = fma(stT[d], ps[2 * e], fma(ctT[d], pc[2 * e], p0[2 * e]));
+                                const T ri = fma(stT[d], ps[2 * e + 1], fma(ctT[d], pc[2 * e + 1], p0[2 * e + 1]));
+                                J[d].b[q] = fma(s_r[d], rr, fma(-s_i[d], ri, J[d].b[q]));
+                                J[d].b[q + 1] = fma(s_r[d], ri, fma(s_i[d], rr, J[d].b[q + 1]));
+                                if (NS) {
+                                    Jn[NS ? d : 0].b[q] = fma(fi * s_r[d], rr, fma(-fi * s_i[d], ri, Jn[NS ? d : 0].b[q]));
+                                    Jn[NS ? d : 0].b[q + 1] = fma(fi * s_r[d], ri, fma(fi * s_i[d], rr, Jn[NS ? d : 0].b[q + 1]));
+                                }
                             }
                         }
                     }
