@@ -1197,10 +1197,9 @@ extern "C" int mbs_po_probe_fp32_peak(mbs_po_ctx *ctx, double *tflops)
 
 // ------------------------------------------------- allocation-free variant --
 // For callers that cannot allocate device memory at the time they diffract:
-// code running while a stream is being captured into a CUDA graph, callers
-// whose device memory is owned by an external pool or a fixed budget, and
-// real-time loops that must not block on cudaMalloc/cudaFree (both
-// synchronise the device).  mbs_po_diffract_staged keeps its chunk partials
+// callers whose device memory is owned by an external pool or a fixed budget
+// that the library must not draw from, and real-time loops that must not
+// block on cudaMalloc/cudaFree (both can synchronise the device).  mbs_po_diffract_staged keeps its chunk partials
 // in context memory that it allocates and grows on demand; this variant
 // keeps them in the fixed device array below instead.  The array is a
 // file-scope __device__ variable, so every GPU that loads this library holds
