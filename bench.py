@@ -55,13 +55,14 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=48, help="orientations in the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error reference")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="column", choices=["column", "proposal", "aggregate", "refgpu", "mlp"],
+    ap.add_argument("--workload", default="column", choices=["column", "proposal", "aggregate", "refgpu", "mlp", "fftphi"],
                     help="column: the headline line (default); proposal: the learned "
                          "orientation proposal against plain Sobol at equal error; aggregate: "
                          "the non-convex 8-column aggregate (thousands of beams per "
                          "orientation), one graph-captured step per precision; refgpu: the "
                          "reference's own CUDA build against the drop-in binary, same CLI run; mlp: "
-                         "training and inference of the proposal network alone")
+                         "training and inference of the proposal network alone; fftphi: the FFT-phi "
+                         "azimuth interpolation path against the direct evaluation")
     return ap.parse_args()
 
 
@@ -352,6 +353,81 @@ def run_aggregate(args):
     print(json.dumps(line), flush=True)
 
 
+def run_fftphi(args):
+    """FFT-phi path on the headline column and grid: the direct evaluation on
+    n_phi / factor azimuth bins plus the device interpolation to n_phi bins,
+    against the direct evaluation on n_phi bins, both FP32C with
+    device-resident inputs (2048 Sobol orientations unless --orient is
+    given).  Reports the time per step of each and the interpolation error
+    of the azimuth-averaged rows and of the grid against the direct result."""
+    import torch
+    from mbs_fast_b200 import abi, beams as B
+    from mbs_fast_b200.handler import GpuHandlerPO
+    from tests import common
+    torch.cuda.set_device(0)
+    n = args.orient if args.orient != 16384 else 2048
+    cfg = B.ParticleConfig(particle_type=1, p=(100.0, 40.0), ri_re=1.3116, ri_im=1e-9,
+                           wavelength=0.532, max_reflections=4)
+    bs, gs, _ = B.symmetry(cfg)
+    beta, gamma, w = B.sobol_orientations(n, bs, gs, 42)
+    batch = B.trace(cfg, beta, gamma, w)
+    full = B.grid(0.0, 180.0, args.n_phi, args.n_theta)
+    factor = GpuHandlerPO.fft_phi_factor(full.n_az)
+    n_low = max(full.n_az // factor, min(full.n_az, 16))
+    low = full.with_azimuths(n_low)
+    rows = full.n_zen + 1
+    hf, hl = GpuHandlerPO(full, B.wave(cfg)), GpuHandlerPO(low, B.wave(cfg))
+    sf, sl = hf.stage(batch), hl.stage(batch)
+    acc_f = torch.zeros(full.n_dirs * 16, dtype=torch.float64, device="cuda:0")
+    acc_l = torch.zeros(low.n_dirs * 16, dtype=torch.float64, device="cuda:0")
+    acc_i = torch.zeros_like(acc_f)
+    hf.autotune(sf, abi.FP32C)
+    hl.autotune(sl, abi.FP32C)
+
+    def direct():
+        acc_f.zero_()
+        hf.diffract_staged(sf, acc_f.data_ptr(), precision=abi.FP32C, stats=False)
+
+    def fft():
+        acc_l.zero_()
+        acc_i.zero_()
+        hl.diffract_staged(sl, acc_l.data_ptr(), precision=abi.FP32C, stats=False)
+        hl.phi_interpolate(acc_l.data_ptr(), n_low, rows, acc_i.data_ptr(), full.n_az)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    ms_direct, ms_fft = timed(direct), timed(fft)
+    Md = acc_f.cpu().numpy().reshape(full.n_az, rows, 16)
+    Mi = acc_i.cpu().numpy().reshape(full.n_az, rows, 16)
+    errs = common.element_errors(Mi, Md, full)
+    errs["weighted_L2_rows"] = common.weighted_l2(Mi, Md, full)
+    errs["L2_grid"] = common.grid_l2(Mi, Md)
+    for s_ in (sf, sl):
+        s_.free()
+    hf.close()
+    hl.close()
+    line = {"metric": METRIC, "value": n / (ms_fft * 1e-3), "unit": "orientations/s",
+            "impl": "b200", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic (reference tracer)",
+            "config": {"workload": WORKLOAD.replace("16384", str(n)) + "; FFT-phi: direct on %d "
+                                   "azimuth bins, interpolated to %d" % (n_low, full.n_az),
+                       "factor": factor},
+            "fft_phi_ms_per_step": ms_fft, "direct_ms_per_step": ms_direct,
+            "speedup_vs_direct": ms_direct / ms_fft,
+            "interpolation_error_vs_direct": errs}
+    print(json.dumps(line), flush=True)
+
+
 def run_refgpu(args):
     """Same-box GPU comparison at the CLI: the reference's own CUDA build
     (oracle/_ref/mbs_po_gpu_ref_{fp64,fp32}, its GpuDiffraction.cu for sm_100)
@@ -436,6 +512,9 @@ def main():
         return
     if args.workload == "aggregate":
         run_aggregate(args)
+        return
+    if args.workload == "fftphi":
+        run_fftphi(args)
         return
     if args.workload == "refgpu":
         run_refgpu(args)

@@ -204,6 +204,28 @@ int mbs_po_staged_sets(const mbs_po_staged *staged);
 int mbs_po_diffract_thetas(mbs_po_ctx *ctx, const mbs_po_beams *beams,
                            const double *theta_rad, int n, double *m11_out);
 
+/* FFT-phi azimuth interpolation (replaces the upsampling of
+ * HandlerPO::HandleOrientationsToLocalGpuFftPhi, reference
+ * GpuDiffraction.cu:3206-3320 fft_upsample_phi_arr2d and :3504-3760): a
+ * Mueller grid low_dev [n_low][n_rows][16] on n_low equally spaced azimuth
+ * bins (device) is interpolated to n_full >= n_low bins and added into
+ * full_dev [n_full][n_rows][16] (device, +=): the real part of the
+ * zero-padded DFT upsampling, frequencies -(n_low-1)/2 .. n_low/2 (the
+ * Nyquist bin of an even n_low kept at +n_low/2), applied as one linear map
+ * in FP64.  n_low <= 4096, n_full <= 65535 (MBS_PO_ERANGE beyond). */
+int mbs_po_phi_interpolate(mbs_po_ctx *ctx, const double *low_dev, int n_low, int n_rows,
+                           double *full_dev, int n_full, void *stream);
+
+/* mbs_po_diffract on the context's grid (n_az azimuth bins), followed on the
+ * device by mbs_po_phi_interpolate to n_full bins: M_accum (and Mns_accum)
+ * are [n_full][n_zen+1][16] host arrays, accumulated +=.  The low-resolution
+ * direct evaluation plus interpolation of the reference's FFT-phi path; the
+ * result is an approximation of the direct evaluation on n_full bins whose
+ * error depends on how band-limited the pattern is in azimuth. */
+int mbs_po_diffract_fft_phi(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
+                            int n_full, double *M_accum, double *Mns_accum,
+                            mbs_po_stats *stats);
+
 /* Post-step on the device: the azimuth-averaged rows of a Mueller grid held
  * in device memory (M_dev, [n_az*(n_zen+1)*16], e.g. the accumulator of
  * mbs_po_diffract_staged), as HandlerPOTotal::WriteMatricesToFile writes them

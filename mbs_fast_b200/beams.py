@@ -312,6 +312,18 @@ class GridTables:
     theta: np.ndarray      # [n_zen+1]
     vf: np.ndarray         # [n_az, n_zen+1, 3]
     dcos2pi: np.ndarray    # [n_zen+1] Compute2PiDcos
+    # how the zenith rows were made: (zen_start_deg, zen_end_deg, n_zen,
+    # theta_deg or None), so that the same rows can be paired with another
+    # azimuth count (with_azimuths)
+    zenith: tuple | None = None
+
+    def with_azimuths(self, n_az: int) -> "GridTables":
+        """The same zenith rows on n_az equally spaced azimuth bins (the
+        reference's ScatteringRange with nAzimuth and azinuthStep changed)."""
+        if self.zenith is None:
+            raise ValueError("grid without its zenith construction")
+        z0, z1, n_zen, theta_deg = self.zenith
+        return grid(z0, z1, n_az, n_zen, theta_deg)
 
     def as_c(self) -> abi.Grid:
         return abi.Grid(n_az=self.n_az, n_zen=self.n_zen, az_step=self.az_step,
@@ -338,4 +350,5 @@ def grid(zen_start_deg: float, zen_end_deg: float, n_az: int, n_zen: int,
                                 abi.ptr(theta_deg, C.c_double), abi.ptr(theta, C.c_double),
                                 abi.ptr(vf, C.c_double), abi.ptr(dc, C.c_double),
                                 C.byref(step)), "mbs_host_grid")
-    return GridTables(n_az, n_zen, step.value, theta, vf, dc)
+    return GridTables(n_az, n_zen, step.value, theta, vf, dc,
+                      zenith=(zen_start_deg, zen_end_deg, n_zen, theta_deg))

@@ -96,6 +96,11 @@ struct mbs_po_ctx {
     size_t macc_cap = 0;
     double *hres = nullptr;      // pinned [2][G*16]
     size_t hres_cap = 0;
+    double *mfull = nullptr;     // [2][n_full*(n_zen+1)*16] interpolated planes (FFT-phi calls)
+    size_t mfull_cap = 0;
+    double *phiW = nullptr;      // azimuth interpolation weights [n_full][n_low]
+    size_t phiW_cap = 0;
+    int phiW_low = 0, phiW_full = 0;
     Arena raw;                   // raw upload area for staging
     int *d_status = nullptr;      // [0] pack status, [1] work counter of the diffraction kernel
     mbs_po_staged host_staged;   // reused by mbs_po_diffract
@@ -241,6 +246,8 @@ extern "C" int mbs_po_destroy(mbs_po_ctx *ctx)
     grid_release(ctx->grid);
     cudaFree(ctx->partial);
     cudaFree(ctx->macc);
+    cudaFree(ctx->mfull);
+    cudaFree(ctx->phiW);
     cudaFreeHost(ctx->hres);
     cudaFree(ctx->raw.base);
     cudaFree(ctx->d_status);
@@ -797,11 +804,89 @@ extern "C" int mbs_po_diffract_staged(mbs_po_ctx *ctx, const mbs_po_staged *s, i
 namespace {
 
 // Host-buffer path shared by mbs_po_diffract and mbs_po_diffract_multisize:
+// ------------------------------------------------ azimuth interpolation --
+// The FFT-phi path of the reference (GpuDiffraction.cu:3206-3320,
+// fft_upsample_phi_arr2d_impl and fft_phi_pad_kernel) computes a Mueller grid
+// on n_low azimuth bins, takes the DFT of every (zenith row, element) series
+// over azimuth, keeps the frequencies f = k for k <= n_low/2 and f = k - n_low
+// above (the Nyquist bin of an even n_low at +n_low/2 only), scales by
+// 1/n_low, zero-pads to n_full bins, transforms back and keeps the real part.
+// For real input that is one linear map of the n_low samples,
+//   out(p) = sum_m W[p][m] low(m),
+//   W[p][m] = (1/n_low) sum_{f in F} cos(2 pi f (p/n_full - m/n_low)),
+// which the device applies as a small matrix product.  With x = 2 pi r / D,
+// r = (p n_low - m n_full) mod D, D = n_full n_low, the frequency sum has the
+// closed forms  sin(n_low x/2) / sin(x/2)  (odd n_low) and
+// sin(n_low x/2) cos(x/2) / sin(x/2)  (even n_low, the Nyquist term at +n_low/2),
+// n_low at r = 0; every angle is reduced exactly in integers first.
+
+constexpr int kMaxPhiLow = 4096;      // W row of one output azimuth in shared memory
+constexpr int kMaxPhiFull = 65535;    // output azimuths run on grid.y
+
+void phi_weights(int n_low, int n_full, std::vector<double> &W)
+{
+    W.assign((size_t)n_full * n_low, 0.0);
+    const int64_t D = (int64_t)n_full * n_low;
+    const bool even = (n_low % 2) == 0;
+    for (int p = 0; p < n_full; ++p)
+        for (int m = 0; m < n_low; ++m) {
+            int64_t r = ((int64_t)p * n_low - (int64_t)m * n_full) % D;
+            if (r < 0)
+                r += D;
+            double S;
+            if (r == 0) {
+                S = n_low;
+            } else {
+                // n_low x / 2 = pi r / n_full, reduced modulo 2 pi
+                const double sn = std::sin(M_PI * (double)(r % (2 * (int64_t)n_full)) / n_full);
+                // x / 2 = pi r / D in (0, pi): sin from the nearer end
+                const int64_t rr = r <= D / 2 ? r : D - r;
+                const double sh = std::sin(M_PI * (double)rr / (double)D);
+                double ch = std::cos(M_PI * (double)rr / (double)D);
+                if (r > D / 2)
+                    ch = -ch;
+                S = even ? sn * ch / sh : sn / sh;
+            }
+            W[(size_t)p * n_low + m] = S / n_low;
+        }
+}
+
+int run_phi_interp(mbs_po_ctx *ctx, const double *low, int n_low, int n_rows, double *full,
+                   int n_full, cudaStream_t st)
+{
+    if (n_low < 1 || n_rows < 1 || n_full < n_low)
+        return fail(ctx, MBS_PO_EINVAL, "azimuth interpolation needs 1 <= n_low <= n_full and rows");
+    if (n_low > kMaxPhiLow || n_full > kMaxPhiFull)
+        return fail(ctx, MBS_PO_ERANGE, "azimuth interpolation supports n_low <= "
+                    + std::to_string(kMaxPhiLow) + " and n_full <= " + std::to_string(kMaxPhiFull));
+    int rc;
+    if (ctx->phiW_low != n_low || ctx->phiW_full != n_full) {
+        std::vector<double> W;
+        phi_weights(n_low, n_full, W);
+        if ((rc = ensure(ctx, ctx->phiW, ctx->phiW_cap, W.size(), "azimuth weights")))
+            return rc;
+        // the stream may still be reading an earlier table
+        CK(cudaStreamSynchronize(st), "sync");
+        CK(cudaMemcpy(ctx->phiW, W.data(), W.size() * sizeof(double), cudaMemcpyHostToDevice), "H2D weights");
+        ctx->phiW_low = n_low;
+        ctx->phiW_full = n_full;
+    }
+    const int64_t plane = (int64_t)n_rows * 16;
+    const int tb = 256;
+    const dim3 g((unsigned)((plane + tb - 1) / tb), (unsigned)n_full);
+    po_phi_interp_kernel<<<g, tb, n_low * sizeof(double), st>>>(low, ctx->phiW, n_low, plane, full);
+    CK(cudaGetLastError(), "azimuth interpolation launch");
+    return MBS_PO_OK;
+}
+
 // stage (one size instance per scale, or the batch as is), diffract into
-// device accumulators, copy back, add into the caller's planes.
+// device accumulators, copy back, add into the caller's planes.  n_full > 0
+// (one size instance only): the planes are interpolated from the grid's
+// n_az azimuth bins to n_full bins on the device first, and the caller's
+// planes are [n_full][n_zen+1][16].
 int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scales, int n_scales,
                   double k_rephase, int precision, double *M_accum, double *Mns_accum,
-                  mbs_po_stats *stats)
+                  mbs_po_stats *stats, int n_full = 0)
 {
     if (!ctx || !beams || !M_accum)
         return fail(ctx, MBS_PO_EINVAL, "null argument");
@@ -817,15 +902,20 @@ int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scal
     const bool ns = Mns_accum != nullptr;
     const size_t sets = scales ? (size_t)n_scales : 1;
     const size_t n = (size_t)G * 16 * sets;
+    const int n_rows = ctx->grid.n_zen + 1;
+    // planes handed back: the grid's, or the interpolated ones
+    const size_t n_out = n_full > 0 ? (size_t)n_full * n_rows * 16 : n;
     int rc;
     if ((rc = ensure(ctx, ctx->macc, ctx->macc_cap, n * 2, "accumulators")))
         return rc;
-    if (ctx->hres_cap < n * 2 || !ctx->hres) {
+    if (n_full > 0 && (rc = ensure(ctx, ctx->mfull, ctx->mfull_cap, n_out * 2, "interpolated planes")))
+        return rc;
+    if (ctx->hres_cap < n_out * 2 || !ctx->hres) {
         cudaFreeHost(ctx->hres);
         ctx->hres = nullptr;
         ctx->hres_cap = 0;
-        CK(cudaMallocHost((void **)&ctx->hres, n * 2 * sizeof(double)), "cudaMallocHost");
-        ctx->hres_cap = n * 2;
+        CK(cudaMallocHost((void **)&ctx->hres, n_out * 2 * sizeof(double)), "cudaMallocHost");
+        ctx->hres_cap = n_out * 2;
     }
     CK(cudaEventRecord(ctx->ev[3], st), "event");
     if ((rc = stage_into(ctx, beams, &ctx->host_staged, st, scales, n_scales, k_rephase)))
@@ -835,18 +925,28 @@ int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scal
     rc = run_diffract(ctx, &ctx->host_staged, precision, ctx->macc, ns ? ctx->macc + n : nullptr, st, stats);
     if (rc)
         return rc;
+    const double *dev_out = ctx->macc;
+    if (n_full > 0) {
+        CK(cudaMemsetAsync(ctx->mfull, 0, n_out * (ns ? 2 : 1) * sizeof(double), st), "memset planes");
+        if ((rc = run_phi_interp(ctx, ctx->macc, ctx->grid.n_az, n_rows, ctx->mfull, n_full, st)))
+            return rc;
+        if (ns && (rc = run_phi_interp(ctx, ctx->macc + n, ctx->grid.n_az, n_rows, ctx->mfull + n_out,
+                                       n_full, st)))
+            return rc;
+        dev_out = ctx->mfull;
+    }
     CK(cudaEventRecord(ctx->ev[5], st), "event");
-    CK(cudaMemcpyAsync(ctx->hres, ctx->macc, n * (ns ? 2 : 1) * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+    CK(cudaMemcpyAsync(ctx->hres, dev_out, n_out * (ns ? 2 : 1) * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
     CK(cudaEventRecord(ctx->ev[7], st), "event");
     CK(cudaStreamSynchronize(st), "sync");
     float h2d = 0.f, d2h = 0.f;
     cudaEventElapsedTime(&h2d, ctx->ev[3], ctx->ev[4]);
     cudaEventElapsedTime(&d2h, ctx->ev[5], ctx->ev[7]);
-    for (size_t i = 0; i < n; ++i)
+    for (size_t i = 0; i < n_out; ++i)
         M_accum[i] += ctx->hres[i];
     if (ns)
-        for (size_t i = 0; i < n; ++i)
-            Mns_accum[i] += ctx->hres[n + i];
+        for (size_t i = 0; i < n_out; ++i)
+            Mns_accum[i] += ctx->hres[n_out + i];
     if (stats) {
         stats->h2d_ms = h2d;
         stats->d2h_ms = d2h;
@@ -861,6 +961,26 @@ extern "C" int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int p
                                double *M_accum, double *Mns_accum, mbs_po_stats *stats)
 {
     return diffract_host(ctx, beams, nullptr, 0, 0.0, precision, M_accum, Mns_accum, stats);
+}
+
+extern "C" int mbs_po_diffract_fft_phi(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
+                                       int n_full, double *M_accum, double *Mns_accum,
+                                       mbs_po_stats *stats)
+{
+    if (!ctx)
+        return MBS_PO_EINVAL;
+    if (ctx->has_grid && n_full < ctx->grid.n_az)
+        return fail(ctx, MBS_PO_EINVAL, "n_full must be at least the grid's azimuth bins");
+    return diffract_host(ctx, beams, nullptr, 0, 0.0, precision, M_accum, Mns_accum, stats, n_full);
+}
+
+extern "C" int mbs_po_phi_interpolate(mbs_po_ctx *ctx, const double *low_dev, int n_low, int n_rows,
+                                      double *full_dev, int n_full, void *stream)
+{
+    if (!ctx || !low_dev || !full_dev)
+        return fail(ctx, MBS_PO_EINVAL, "null argument");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    return run_phi_interp(ctx, low_dev, n_low, n_rows, full_dev, n_full, (cudaStream_t)stream);
 }
 
 extern "C" int mbs_po_diffract_multisize(mbs_po_ctx *ctx, const mbs_po_beams *beams,

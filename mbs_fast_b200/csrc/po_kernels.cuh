@@ -1594,6 +1594,30 @@ __global__ void po_reduce_kernel(const double *__restrict__ partial, int chunks_
     out[g * 16 + k] += s;
 }
 
+// Azimuth interpolation of a Mueller grid (the FFT-phi path): for every output
+// azimuth p, out[p][r] += sum_m W[p][m] low[m][r], r running over the
+// (zenith row, element) entries of one azimuth plane (plane = rows * 16
+// doubles, coalesced across the block).  W [n_full][n_low] is the linear map
+// of the zero-padded DFT upsampling (see phi_weights on the host); the
+// block keeps its output azimuth's row of W in shared memory.
+__global__ void __launch_bounds__(256) po_phi_interp_kernel(const double *__restrict__ low,
+                                                            const double *__restrict__ W, int n_low,
+                                                            int64_t plane, double *__restrict__ out)
+{
+    extern __shared__ double w_row[];
+    const int p = blockIdx.y;
+    for (int m = threadIdx.x; m < n_low; m += blockDim.x)
+        w_row[m] = W[(size_t)p * n_low + m];
+    __syncthreads();
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= plane)
+        return;
+    double acc = 0.0;
+    for (int m = 0; m < n_low; ++m)
+        acc = fma(w_row[m], low[(size_t)m * plane + r], acc);
+    out[(size_t)p * plane + r] += acc;
+}
+
 // ------------------------------------------------------- azimuth average
 // Per zenith row t the azimuth average of M(p, t) L(2 az_p), az_p = -p 2 pi / n_az
 // (L the Stokes rotation [1 0 0 0; 0 c s 0; 0 -s c 0; 0 0 0 1]), the polar

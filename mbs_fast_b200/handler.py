@@ -17,6 +17,7 @@ direction order (row p, column t, 16 row-major elements).
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -62,6 +63,10 @@ def lib() -> C.CDLL:
         L.mbs_po_phi_average.argtypes = [vp, C.c_void_p, abi._dp, abi._dp, abi._dp, abi._dp,
                                          C.c_void_p]
         L.mbs_po_orientation_rows.argtypes = [vp, C.POINTER(abi.Beams), C.c_int, abi._dp]
+        L.mbs_po_phi_interpolate.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                             C.c_void_p]
+        L.mbs_po_diffract_fft_phi.argtypes = [vp, C.POINTER(abi.Beams), C.c_int, C.c_int, abi._dp,
+                                              abi._dp, C.POINTER(abi.Stats)]
         _lib = L
     return _lib
 
@@ -139,6 +144,70 @@ class GpuHandlerPO:
             return False
         self._call(rc, "mbs_po_diffract")
         return True
+
+    # -- HandlerPO::HandleOrientationsToLocalGpuFftPhi ----------------------
+    @staticmethod
+    def fft_phi_factor(n_full: int, configured: int = 0) -> int:
+        """Azimuth factor of the FFT-phi path (reference
+        GpuDiffraction.cu:712-726): the configured one, else
+        MBS_FFT_PHI_FACTOR (1-64), else 8 / 6 / 3 / 2 for at least 2400 /
+        600 / 240 / fewer output azimuths."""
+        if configured > 0:
+            return configured
+        v = os.environ.get("MBS_FFT_PHI_FACTOR", "")
+        if v.isdigit() and 1 <= int(v) <= 64:
+            return int(v)
+        return 8 if n_full >= 2400 else 6 if n_full >= 600 else 3 if n_full >= 240 else 2
+
+    def diffract_fft_phi(self, batch: BeamBatch, low: GridTables, n_full: int,
+                         precision: int = abi.FP64, noshadow: bool = False):
+        """Direct evaluation on `low` (same zenith rows, fewer azimuth bins),
+        interpolated on the device to n_full bins (mbs_po_diffract_fft_phi).
+        Returns (M, Mns or None), each [n_full, n_zen+1, 16]."""
+        shape = (n_full, low.n_zen + 1, 16)
+        M = np.zeros(shape)
+        Mns = np.zeros(shape) if noshadow else None
+        b = batch.as_c(with_raw=False)
+        self._call(lib().mbs_po_set_grid(self.ctx, C.byref(low.as_c())), "mbs_po_set_grid")
+        try:
+            rc = lib().mbs_po_diffract_fft_phi(self.ctx, C.byref(b), precision, n_full,
+                                               abi.ptr(M, C.c_double), abi.ptr(Mns, C.c_double),
+                                               C.byref(self.last_stats))
+            self._call(rc, "mbs_po_diffract_fft_phi")
+        finally:
+            self._call(lib().mbs_po_set_grid(self.ctx, C.byref(self.grid.as_c())), "mbs_po_set_grid")
+        return M, Mns
+
+    def handle_orientations_to_local_gpu_fft_phi(self, prepared: BeamBatch, local_m: np.ndarray,
+                                                 local_m_noshadow: np.ndarray | None = None,
+                                                 factor: int = 0,
+                                                 precision: int = abi.FP64) -> bool:
+        """The FFT-phi path on this handler's grid (reference
+        GpuDiffraction.cu:3504-3760): direct evaluation on n_az / factor
+        azimuth bins (at least 16), interpolated to n_az; the plain direct
+        evaluation when the factor is 1, the grid has fewer than 32 azimuth
+        bins or the reduced count would not be smaller."""
+        n_full = self.grid.n_az
+        f = self.fft_phi_factor(n_full, factor)
+        n_low = n_full // f if f > 1 else n_full
+        if n_low < 16:
+            n_low = min(n_full, 16)
+        if f <= 1 or n_full < 32 or n_low >= n_full:
+            return self.handle_orientations_to_local_gpu(prepared, local_m, local_m_noshadow,
+                                                         precision=precision)
+        M, Mns = self.diffract_fft_phi(prepared, self.grid.with_azimuths(n_low), n_full,
+                                       precision, noshadow=local_m_noshadow is not None)
+        local_m += M
+        if local_m_noshadow is not None:
+            local_m_noshadow += Mns
+        return True
+
+    def phi_interpolate(self, low_dev_ptr: int, n_low: int, n_rows: int, full_dev_ptr: int,
+                        n_full: int, stream: int = 0) -> None:
+        """mbs_po_phi_interpolate on device arrays (+= into the full grid)."""
+        self._call(lib().mbs_po_phi_interpolate(self.ctx, C.c_void_p(low_dev_ptr), n_low, n_rows,
+                                                C.c_void_p(full_dev_ptr), n_full, C.c_void_p(stream)),
+                   "mbs_po_phi_interpolate")
 
     # -- HandlerPO::HandleOrientationsToLocalGpuMultiK ----------------------
     def handle_orientations_to_local_gpu_multik(self, prepared: BeamBatch, start: int, count: int,

@@ -17,6 +17,7 @@
 // reference's double build), MBS_GPU_TIMING=1 prints per-call timings,
 // MBS_GPU_MEM_FRACTION bounds batch sizes like the reference.
 #include "HandlerPO.h"
+#include "FftStatistics.h"
 #include "beam_pack.h"
 #include "mbs_po_b200.h"
 
@@ -371,15 +372,200 @@ bool HandlerPO::HandleBeamsToLocalGpu(const PreparedOrientation &prepared, Arr2D
     return HandleOrientationsToLocalGpu(one, 0, 1, localM, localM_noshadow, 1.0, 0.0);
 }
 
+namespace
+{
+
+// MBS_FFT_PHI_FACTOR: 1..64, or "auto"/unset (0), as the reference reads it
+// (GpuDiffraction.cu:514-530).
+int fft_phi_factor_env()
+{
+    const char *v = std::getenv("MBS_FFT_PHI_FACTOR");
+    if (!v || !*v)
+        return 0;
+    char *end = nullptr;
+    const long f = std::strtol(v, &end, 10);
+    if (!end || *end != '\0' || f < 1 || f > 64)
+        return 0;
+    return (int)f;
+}
+
+// Azimuth factor of the FFT-phi path (choose_fft_phi_factor,
+// GpuDiffraction.cu:712-726): the handler's configured factor, else the
+// environment's, else by the output azimuth count.
+int fft_phi_factor(int nFull, int configured)
+{
+    if (configured > 0)
+        return configured;
+    const int env = fft_phi_factor_env();
+    if (env > 0)
+        return env;
+    if (nFull >= 2400)
+        return 8;
+    if (nFull >= 600)
+        return 6;
+    if (nFull >= 240)
+        return 3;
+    return 2;
+}
+
+// The interpolated grid against the one from twice the direct azimuths
+// (report_fft_check, GpuDiffraction.cu:3142-3204): the larger of the maximum
+// relative M11 error over directions with M11 >= 1e-3 of the grid's maximum,
+// and of the maximum error of any element relative to max(|M11|, that floor).
+double fft_check_estimate(const std::vector<double> &fft, const std::vector<double> &ref,
+                          int nAz, int nRows, const char *name)
+{
+    double refMax = 0.0;
+    for (int i = 0; i < nAz * nRows; ++i)
+        refMax = std::max(refMax, std::fabs(ref[(size_t)i * 16]));
+    const double significant = 1e-3 * refMax;
+    double sigRel = 0.0, normRel = 0.0, maxRel = 0.0;
+    for (int i = 0; i < nAz * nRows; ++i) {
+        const double a = ref[(size_t)i * 16], b = fft[(size_t)i * 16];
+        const double rel = std::fabs(b - a) / std::max(std::fabs(a), 1e-12);
+        maxRel = std::max(maxRel, rel);
+        if (std::fabs(a) >= significant)
+            sigRel = std::max(sigRel, rel);
+        const double scale = std::max(std::fabs(a), significant);
+        for (int e = 0; e < 16; ++e)
+            normRel = std::max(normRel, std::fabs(fft[(size_t)i * 16 + e] - ref[(size_t)i * 16 + e]) / scale);
+    }
+    std::fprintf(stderr, "GPU FFT check %s: M11 max_rel=%.6g significant_max_rel=%.6g "
+                 "Mueller/M11 max_rel=%.6g\n", name, maxRel, sigRel, normRel);
+    return std::max(sigRel, normRel);
+}
+
+}  // namespace
+
+// Direct evaluation of prepared[start, start+count) on `low` (n_az azimuth
+// bins), interpolated on the device to nFull bins: adds into M (and Mns),
+// flat [nFull][nZen+1][16].
+static bool diffract_fft_phi(HandlerPO &h, const ScatteringRange &low,
+                             const std::vector<PreparedOrientation> &prepared, int start, int count,
+                             int nFull, std::vector<double> &M, std::vector<double> *Mns, int device)
+{
+    const bool timing = env_is("MBS_GPU_TIMING", "1");
+    const auto t0 = std::chrono::steady_clock::now();
+    MbsPackedBeams packed;
+    std::string err;
+    const int prc = mbs_pack_prepared(prepared, start, count, false, packed, &err);
+    if (prc != MBS_PO_OK)
+        return false;
+    const mbs_po_beams view = packed.view(false);
+    if (view.n_beams == 0)
+        return true;
+    if (!HandlerPOBoundary::Prepare(h, low, HandlerPOWaveAccess::Get(h, 0.0), device))
+        return false;
+    mbs_po_stats st;
+    std::memset(&st, 0, sizeof(st));
+    const int rc = mbs_po_diffract_fft_phi(g_ctx.ctx, &view, precision_from_env(), nFull, M.data(),
+                                           Mns ? Mns->data() : nullptr, &st);
+    if (rc == MBS_PO_EBEAM)
+        return false;
+    if (!report(rc, "FFT-phi diffraction"))
+        return false;
+    if (timing)
+        std::fprintf(stderr,
+                     "GPU timing fft_phi path=b200-%s orient=%d beams=%lld nPhiDirect=%d nPhiOut=%d "
+                     "kernels=%.3fms total=%.3fms\n",
+                     precision_from_env() == MBS_PO_FP32C ? "fp32c" : "fp64", view.n_orient,
+                     (long long)view.n_beams, low.nAzimuth, nFull, st.kernel_ms,
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    return true;
+}
+
 bool HandlerPO::HandleOrientationsToLocalGpuFftPhi(const std::vector<PreparedOrientation> &prepared,
                                                    int start, int count, Arr2D &localM,
                                                    Arr2D &localM_noshadow, double scale,
                                                    double waveIndex)
 {
-    // The FFT azimuth interpolation is an approximation of the direct
-    // evaluation; the direct path is exact on the requested grid.
-    return HandleOrientationsToLocalGpu(prepared, start, count, localM, localM_noshadow,
-                                        scale, waveIndex);
+    // Direct evaluation on nFull / factor azimuth bins, then the azimuth
+    // interpolation of the reference's FFT-phi path on the device
+    // (GpuDiffraction.cu:3504-3760): an approximation of the direct result on
+    // the requested grid.  Not carried over: the environment-driven zenith
+    // factor (MBS_FFT_THETA_FACTOR) and adaptive spike rows
+    // (MBS_FFT_ADAPTIVE_PHI), both off by default there; size-scaled calls
+    // take the direct path.
+    if (!isCoh)
+        return false;
+    if (start < 0 || count < 0 || start > (int)prepared.size())
+        return false;
+    const int nFull = m_sphere.nAzimuth;
+    const int nZen = m_sphere.nZenith;
+    const int nRows = nZen + 1;
+    const bool ns = ComputeNoShadow();
+    const int factor = fft_phi_factor(nFull, m_fftPhiFactor);
+    int nLow = factor > 1 ? nFull / factor : nFull;
+    if (nLow < 16)
+        nLow = std::min(nFull, 16);
+    if (factor <= 1 || nFull < 32 || nLow >= nFull || std::fabs(scale - 1.0) > 1e-15)
+    {
+        if (m_fftStatistics)
+            m_fftStatistics->RecordCall(nFull, nFull, 1);
+        return HandleOrientationsToLocalGpu(prepared, start, count, localM, localM_noshadow,
+                                            scale, waveIndex);
+    }
+    if (m_fftStatistics)
+        m_fftStatistics->RecordCall(nFull, nLow, factor);
+    static bool announced = false;
+    if (!announced)
+    {
+        std::fprintf(stderr, "GPU FFT azimuth interpolation: direct Nphi=%d, output Nphi=%d "
+                     "(factor=%d), on the B200 library\n", nLow, nFull, factor);
+        announced = true;
+    }
+    auto sphere_with = [&](int nAz) {
+        ScatteringRange s = m_sphere;
+        s.nAzimuth = nAz;
+        s.azinuthStep = M_2PI / nAz;
+        s.ComputeSphereDirections(*m_incidentLight);
+        return s;
+    };
+    const size_t n = (size_t)nFull * nRows * 16;
+    std::vector<double> fftM(n, 0.0), fftMns(ns ? n : 0, 0.0);
+    const int device = current_device();
+    if (!diffract_fft_phi(*this, sphere_with(nLow), prepared, start, count, nFull, fftM,
+                          ns ? &fftMns : nullptr, device))
+        return false;
+    const char *chk = std::getenv("MBS_FFT_CHECK");
+    const bool doCheck = (chk && std::strcmp(chk, "1") == 0) || m_fftTolerance > 0.0;
+    if (doCheck)
+    {
+        const int nCheck = std::min(nFull, 2 * nLow);
+        std::vector<double> checkM(n, 0.0), checkMns(ns ? n : 0, 0.0);
+        if (!diffract_fft_phi(*this, sphere_with(nCheck), prepared, start, count, nFull, checkM,
+                              ns ? &checkMns : nullptr, device))
+            return false;
+        double est = fft_check_estimate(fftM, checkM, nFull, nRows, "full");
+        if (ns)
+            est = std::max(est, fft_check_estimate(fftMns, checkMns, nFull, nRows, "no-shadow"));
+        const bool refine = m_fftTolerance > 0.0 && est > m_fftTolerance;
+        if (m_fftStatistics)
+            m_fftStatistics->RecordValidation(est, refine);
+        if (refine)
+        {
+            fftM.swap(checkM);
+            fftMns.swap(checkMns);
+            std::fprintf(stderr, "GPU FFT validation exceeded tolerance: estimate=%.6g, "
+                         "tolerance=%.6g; using the doubled direct Nphi=%d result\n",
+                         est, m_fftTolerance, nCheck);
+        }
+    }
+    for (int p = 0; p < nFull; ++p)
+        for (int t = 0; t < nRows; ++t)
+        {
+            const size_t off = ((size_t)p * nRows + t) * 16;
+            double *cell = localM.RawCell(p, t);
+            for (int q = 0; q < 16; ++q)
+                cell[q] += fftM[off + q];
+            if (ns)
+            {
+                double *cn = localM_noshadow.RawCell(p, t);
+                for (int q = 0; q < 16; ++q)
+                    cn[q] += fftMns[off + q];
+            }
+        }
+    return true;
 }
 
 bool HandlerPO::HandleOrientationsToLocalGpuMultiK(const std::vector<PreparedOrientation> &prepared,

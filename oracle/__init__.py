@@ -268,3 +268,24 @@ def thetas_m11(batch: BeamBatch, grid_n_az: int, az_step: float, theta_rad, wave
                            abi.ptr(np.ascontiguousarray(th), C.c_double), n,
                            1 if singular else 0, abi.ptr(out, C.c_double))
     return out
+
+
+def phi_upsample_fft(low: np.ndarray, n_full: int) -> np.ndarray:
+    """Azimuth upsampling of the reference's FFT-phi path, restated with numpy
+    FFTs: fft_upsample_phi_arr2d_impl and fft_phi_pad_kernel
+    (src/cuda/GpuDiffraction.cu:3206-3320, :794-814).  Every (zenith row,
+    element) series over the n_low azimuth bins of low [n_low, rows, 16] is
+    transformed, bin k goes to frequency k (k <= n_low/2) or k - n_low, scaled
+    by 1/n_low and placed in an n_full-bin spectrum (negative frequencies at
+    n_full + f), transformed back unnormalised (cuFFT's inverse), and the
+    real part is returned as [n_full, rows, 16]."""
+    low = np.asarray(low, dtype=np.float64)
+    n_low = low.shape[0]
+    X = np.fft.fft(low, axis=0)
+    Y = np.zeros((n_full,) + low.shape[1:], dtype=np.complex128)
+    for k in range(n_low):
+        f = k if k <= n_low // 2 else k - n_low
+        d = f if f >= 0 else n_full + f
+        if 0 <= d < n_full:
+            Y[d] = X[k] / n_low
+    return np.real(np.fft.ifft(Y, axis=0) * n_full)

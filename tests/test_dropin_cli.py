@@ -12,16 +12,17 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DROPIN = os.path.join(ROOT, "mbs_fast_b200", "_lib", "mbs_po_b200")
 REFCLI = os.path.join(ROOT, "oracle", "_ref", "mbs_po_ref")
+REFGPU = os.path.join(ROOT, "oracle", "_ref", "mbs_po_gpu_ref_fp64")
 
 ARGS = ["--method", "po", "--particle", "1", "100", "40", "--refractive-index", "1.3116", "1e-9",
         "--wavelength-um", "0.532", "--max-reflections", "4", "--sobol", "64",
         "--scattering-grid", "0", "180", "48", "180", "--close"]
 
 
-def _run(binary, backend, out, env_extra=None):
+def _run(binary, backend, out, env_extra=None, extra_args=()):
     env = dict(os.environ)
     env.update(env_extra or {})
-    r = subprocess.run([binary] + ARGS + ["--backend", backend, "--output", out],
+    r = subprocess.run([binary] + ARGS + list(extra_args) + ["--backend", backend, "--output", out],
                        capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
     name = os.path.basename(out)
@@ -53,3 +54,22 @@ def test_dropin_matches_reference_cli(tmp_path):
                              {"MBS_GPU_TIMING": "1", "MBS_B200_PRECISION": "fp32c"})
     assert "path=b200-fp32c" in log32
     assert _wl2(f32, ref) < 2e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFGPU)),
+                    reason="drop-in or the reference's CUDA build not built")
+def test_dropin_fft_phi_matches_reference_cuda_build(tmp_path):
+    """--fft: the reference's CUDA build (its own FFT-phi path, cuFFT) and the
+    drop-in (direct evaluation on the reduced azimuth grid and the device
+    interpolation of this library) on the same command line; both FP64."""
+    ref, ref_i, ref_log = _run(REFGPU, "gpu", str(tmp_path / "ref"), extra_args=["--fft"])
+    assert "FFT angular interpolation" in ref_log
+    gpu, gpu_i, log = _run(DROPIN, "gpu", str(tmp_path / "gpu"), {"MBS_GPU_TIMING": "1"},
+                           extra_args=["--fft"])
+    assert "path=b200-fp64" in log and "nPhiOut=48" in log
+    assert gpu.shape == ref.shape
+    np.testing.assert_array_equal(gpu[:, :2], ref[:, :2])
+    assert _wl2(gpu, ref) < 1e-7
+    for k in ("Cext", "Csca"):
+        assert abs(float(gpu_i[k]) / float(ref_i[k]) - 1) < 1e-7, k
