@@ -435,7 +435,8 @@ def run_refgpu(args):
     FP64 and FP32C), on the D=40 um, L=100 um column with N Sobol orientations
     and the headline grid.  Diffraction time is the sum of the "GPU timing
     diffract" lines (MBS_GPU_TIMING=1) of each run: kernels and the whole
-    call (packing, copies, kernels, accumulation)."""
+    call (packing, copies, kernels, accumulation), each binary timed on its
+    second run."""
     import re
     import subprocess
     import tempfile
@@ -456,6 +457,10 @@ def run_refgpu(args):
             out[name] = {"unavailable": "not built"}
             continue
         env = dict(os.environ, MBS_GPU_TIMING="1", **env_extra)
+        # one untimed run first: the first process on a fresh device pays
+        # one-off costs (module loading, first allocations) in its calls
+        subprocess.run([binary] + cli + ["--output", os.path.join(tempfile.mkdtemp(), "w")],
+                       capture_output=True, text=True, env=env, timeout=1800)
         d = tempfile.mkdtemp()
         t0 = time.perf_counter()
         r = subprocess.run([binary] + cli + ["--output", os.path.join(d, "o")], capture_output=True,
