@@ -98,6 +98,28 @@ class Proposal:
         return u, v, w
 
 
+def proposal_density(prop: "Proposal", u, v) -> np.ndarray:
+    """Density g(u, v) of a proposal on the unit square (C^2 times the
+    probability of the point's cell; the uniform density is 1)."""
+    C = prop.cells
+    r = np.clip((np.asarray(u) * C).astype(np.int64), 0, C - 1)
+    c = np.clip((np.asarray(v) * C).astype(np.int64), 0, C - 1)
+    return C * C * prop.prob[r, c]
+
+
+def balance_weights(prop: "Proposal", n_pilot: int, pilot_uv, main_uv):
+    """Weights that combine a plain pilot (n_pilot points from the uniform
+    density) and N points from the proposal into one unbiased estimate of the
+    average (the balance heuristic of multiple importance sampling): every
+    point x, whichever sampler drew it, gets 1 / (n_pilot + N g(x)), so
+    E[sum] = n_pilot int f/(n_pilot+Ng) + N int f g/(n_pilot+Ng) = int f.
+    Returns (pilot weights, main weights)."""
+    n_main = len(main_uv[0])
+    wp = 1.0 / (n_pilot + n_main * proposal_density(prop, *pilot_uv))
+    wm = 1.0 / (n_pilot + n_main * proposal_density(prop, *main_uv))
+    return wp, wm
+
+
 def uniform_proposal(cells: int = 128) -> Proposal:
     return Proposal(np.full((cells, cells), 1.0 / (cells * cells)), learned=False)
 
@@ -204,24 +226,50 @@ def orientation_sample_batch(cfg, u, v, w, beta_sym: float, gamma_sym: float):
     return B.trace(cfg, beta, gamma, w)
 
 
-def train_proposal(handler, cfg, n_pilot: int, rows_mask=None, pilot_seed: int = 777,
-                   cells: int = 128, mix: float = 0.8, epochs: int = 400, min_r2: float = 0.2,
-                   device: int = 0, precision: int = 1):
+@dataclass
+class TrainedProposal:
+    """A proposal with its pilot run: the pilot's points (u, v) and
+    per-orientation rows [n_pilot, n_t, 16] (orientation weight 1), which
+    balance_weights lets the final estimate reuse, and the seconds spent in
+    the pilot (tracing and device rows) and in the network fit."""
+    proposal: Proposal
+    fit_r2: float
+    pilot_u: np.ndarray
+    pilot_v: np.ndarray
+    pilot_rows: np.ndarray
+    pilot_s: float
+    fit_s: float
+
+
+def train_proposal_with_pilot(handler, cfg, n_pilot: int, rows_mask=None, pilot_seed: int = 777,
+                              cells: int = 128, mix: float = 0.8, epochs: int = 400,
+                              batch: int = 256, min_r2: float = 0.2, device: int = 0,
+                              precision: int = 1) -> TrainedProposal:
     """Pilot run (plain Sobol, per-orientation rows on the handler's grid),
-    network training on the log importance, proposal table.  Returns
-    (proposal, fit R^2, seconds spent)."""
+    network training on the log importance, proposal table."""
     import time
     from . import beams as B
     t0 = time.perf_counter()
     bs, gs, _ = B.symmetry(cfg)
     u, v, _ = plain_sobol(n_pilot, seed=pilot_seed)
-    batch = orientation_sample_batch(cfg, u, v, np.ones(n_pilot), bs, gs)
-    rows = handler.orientation_rows(batch, precision=precision)
+    pb = orientation_sample_batch(cfg, u, v, np.ones(n_pilot), bs, gs)
+    rows = handler.orientation_rows(pb, precision=precision)
+    t1 = time.perf_counter()
     logh = variance_targets(rows, rows_mask)
     lp = LearnedProposal(bs, gs, device=device)
     try:
-        r2 = lp.fit(u, v, logh, epochs=epochs)
+        r2 = lp.fit(u, v, logh, epochs=epochs, batch=batch)
         prop = lp.proposal(cells=cells, mix=mix, min_r2=min_r2)
     finally:
         lp.close()
-    return prop, r2, time.perf_counter() - t0
+    return TrainedProposal(prop, r2, u, v, rows, t1 - t0, time.perf_counter() - t1)
+
+
+def train_proposal(handler, cfg, n_pilot: int, rows_mask=None, pilot_seed: int = 777,
+                   cells: int = 128, mix: float = 0.8, epochs: int = 400, min_r2: float = 0.2,
+                   device: int = 0, precision: int = 1):
+    """train_proposal_with_pilot without the pilot data.  Returns
+    (proposal, fit R^2, seconds spent)."""
+    t = train_proposal_with_pilot(handler, cfg, n_pilot, rows_mask, pilot_seed, cells, mix, epochs,
+                                  min_r2=min_r2, device=device, precision=precision)
+    return t.proposal, t.fit_r2, t.pilot_s + t.fit_s

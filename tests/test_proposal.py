@@ -48,6 +48,30 @@ def test_importance_weights_are_unbiased():
         assert abs(np.mean(ests) - exact) < 0.01 * exact + 1e-3, exact
 
 
+def test_pilot_and_proposal_combined_by_balance_weights_are_unbiased():
+    """Plain pilot points and proposal points together, each weighted
+    1 / (n_pilot + N g(x)): the weighted sum estimates the average, and the
+    weights of a constant integrand sum to one on average."""
+    prop = _peaked()
+    n_pilot, N = 1024, 2048
+    for f, exact in ((lambda u, v: np.ones_like(u), 1.0), (lambda u, v: u * v, 0.25),
+                     (lambda u, v: np.exp(-((u - 0.8) ** 2 + (v - 0.3) ** 2) / 0.01), 0.01 * np.pi)):
+        ests = []
+        for seed in range(8):
+            pu, pv, _ = PR.plain_sobol(n_pilot, seed=100 + seed)
+            u, v, _ = prop.sample(N, seed=seed)
+            wp, wm = PR.balance_weights(prop, n_pilot, (pu, pv), (u, v))
+            assert np.all(wp > 0) and np.all(wm > 0)
+            ests.append(np.sum(wp * f(pu, pv)) + np.sum(wm * f(u, v)))
+        assert abs(np.mean(ests) - exact) < 0.01 * exact + 1e-3, exact
+    # a density read back at the cell centres is the tabulated one
+    C = prop.cells
+    c = (np.arange(C) + 0.5) / C
+    U, V = np.meshgrid(c, c, indexing="ij")
+    np.testing.assert_allclose(PR.proposal_density(prop, U.ravel(), V.ravel()),
+                               (C * C * prop.prob).ravel(), rtol=1e-14)
+
+
 def test_uniform_fallback_is_plain_sobol():
     prop = PR.uniform_proposal(128)
     assert not prop.learned
