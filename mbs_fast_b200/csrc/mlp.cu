@@ -30,6 +30,7 @@ constexpr int kH = MBS_MLP_HIDDEN;   // 128
 constexpr int kIn = MBS_MLP_IN;      // 4
 constexpr int kInPad = 16;           // K of the first layer, padded for the MMA
 constexpr int kTile = 128;           // M of one tcgen05.mma tile (batch rows padded to it)
+constexpr int kTileN = 32;           // N of one CTA's tile: four CTAs share a 128-wide layer
 constexpr int kTileK = 128;          // K staged per round
 constexpr int kGemmSmem = 2 * kTile * kTileK * 2 + 1024;   // A, B tiles (BF16) + barrier
 
@@ -118,16 +119,66 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase)
 // N tiles, y over M tiles; 128 threads, thread i owns accumulator row i
 // (tensor-memory lane i).  On a barrier timeout *err is set and the CTA
 // frees its tensor memory and returns without storing.
+// Stages the rows x kt operand tile whose element (r, k) is
+// p[(row0 + r) * rs + (k0 + k) * ks] into shared memory in the K-major core-
+// matrix layout (kmajor_off); rows at or beyond row_limit read as zero.
+// Operands contiguous along K move in 16-byte vectors (one core-matrix row
+// each); operands contiguous along the rows move in 16-byte vectors of 8 rows
+// at one k; anything else element by element.  Every path is unrolled so a
+// thread keeps several global loads in flight.
+__device__ __forceinline__ void stage_operand(unsigned char *dst, const bf16 *p, long rs, long ks,
+                                              int row0, int rows, int row_limit, int k0, int kt)
+{
+    const bool aligned = (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+    if (ks == 1 && (rs & 7) == 0 && aligned) {
+        const int kc = kt >> 3;
+        const int n = rows * kc;
+#pragma unroll 4
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            const int r = v / kc, c = v - r * kc;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (row0 + r < row_limit)
+                val = *reinterpret_cast<const uint4 *>(p + (long)(row0 + r) * rs + k0 + c * 8);
+            *reinterpret_cast<uint4 *>(dst + kmajor_off(r, c * 8, kt)) = val;
+        }
+    } else if (rs == 1 && (ks & 7) == 0 && aligned && (rows & 7) == 0 && (row0 & 7) == 0
+               && (row_limit & 7) == 0) {
+        const int rc = rows >> 3;
+        const int n = kt * rc;
+#pragma unroll 4
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            const int k = v / rc, r = (v - k * rc) * 8;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (row0 + r < row_limit)
+                val = *reinterpret_cast<const uint4 *>(p + (long)(row0 + r) + (long)(k0 + k) * ks);
+            const bf16 *e = reinterpret_cast<const bf16 *>(&val);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                *reinterpret_cast<bf16 *>(dst + kmajor_off(r + j, k, kt)) = e[j];
+        }
+    } else {
+        const bf16 zero = __float2bfloat16(0.f);
+#pragma unroll 4
+        for (int i = threadIdx.x; i < rows * kt; i += blockDim.x) {
+            const int r = i / kt, k = i - r * kt;
+            *reinterpret_cast<bf16 *>(dst + kmajor_off(r, k, kt)) =
+                row0 + r < row_limit ? p[(long)(row0 + r) * rs + (long)(k0 + k) * ks] : zero;
+        }
+    }
+}
+
+constexpr int kGemmThreads = 256;   // 8 warps: all stage, two warpgroups read TMEM
+
 template <int MODE>
-__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, Mat A, Mat B, GemmOut o, int *err)
+__global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, Mat A, Mat B, GemmOut o, int *err)
 {
     extern __shared__ __align__(1024) unsigned char gsm[];
     bf16 *sA = reinterpret_cast<bf16 *>(gsm);
     bf16 *sB = reinterpret_cast<bf16 *>(gsm + kTile * kTileK * 2);
     uint64_t *bar = reinterpret_cast<uint64_t *>(gsm + 2 * kTile * kTileK * 2);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
-    const int m0 = blockIdx.y * kTile, n0 = blockIdx.x * kTile;
-    const int nt = min(kTile, N - n0);                   // multiple of 16
+    const int m0 = blockIdx.y * kTile, n0 = blockIdx.x * kTileN;
+    const int nt = min(kTileN, N - n0);                  // multiple of 16
     const int ncols = nt <= 32 ? 32 : (nt <= 64 ? 64 : 128);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 0) {
@@ -142,23 +193,14 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, Mat A, Mat B,
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = *tslot;
     const uint32_t idesc = umma_idesc(kTile, nt);
-    const bf16 zero = __float2bfloat16(0.f);
     uint32_t phase = 0;
     bool ok = true;
     for (int k0 = 0; k0 < K && ok; k0 += kTileK) {
         const int kt = min(kTileK, K - k0);              // multiple of 16
-        // stage A (kTile x kt) and B (nt x kt) in the K-major layout
-        for (int i = threadIdx.x; i < kTile * kt; i += blockDim.x) {
-            const int r = i / kt, k = i - r * kt;
-            const int gm = m0 + r, gk = k0 + k;
-            *reinterpret_cast<bf16 *>(reinterpret_cast<unsigned char *>(sA) + kmajor_off(r, k, kt)) =
-                gm < M ? A.p[gm * A.sr + gk * A.sc] : zero;
-        }
-        for (int i = threadIdx.x; i < nt * kt; i += blockDim.x) {
-            const int r = i / kt, k = i - r * kt;
-            *reinterpret_cast<bf16 *>(reinterpret_cast<unsigned char *>(sB) + kmajor_off(r, k, kt)) =
-                B.p[(k0 + k) * B.sr + (n0 + r) * B.sc];
-        }
+        // stage A (kTile x kt: element (m, k) = A.p[m sr + k sc]) and B
+        // (nt x kt: element (n, k) = B.p[k sr + n sc]) in the K-major layout
+        stage_operand(reinterpret_cast<unsigned char *>(sA), A.p, A.sr, A.sc, m0, kTile, M, k0, kt);
+        stage_operand(reinterpret_cast<unsigned char *>(sB), B.p, B.sc, B.sr, n0, nt, n0 + nt, k0, kt);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -187,10 +229,13 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, Mat A, Mat B,
             atomicExch(err, 1);
         mbar_wait(smem_u32(bar), phase ^ 1u);   // let any MMA in flight finish, bounded
     } else {
-        const int r = m0 + warp * 32 + lane;
-        for (int c0 = 0; c0 < nt; c0 += 16) {
+        // warp w reads TMEM lanes 32 (w % 4) .. + 31 (its lane quarter); the
+        // two warpgroups take alternate 16-column chunks
+        const int wq = warp & 3, wg = warp >> 2;
+        const int r = m0 + wq * 32 + lane;
+        for (int c0 = wg * 16; c0 < nt; c0 += 32) {
             uint32_t v[16];
-            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            const uint32_t ta = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)c0;
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
                          "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
                          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
@@ -267,27 +312,49 @@ __global__ void k_head_bwd(const float *y, const float *t, int n, int bpad, cons
 }
 
 // Column sums of a [rows][cols] BF16 matrix, fixed row order: out[c].
-__global__ void k_colsum_bf16(const bf16 *x, int rows, int cols, float *out)
+// Column sums in fixed order: block b sums columns 32 b .. 32 b + 31, its 8
+// row groups g (threadIdx.x / 32) take rows g, g + 8, ... in turn, and the
+// group sums are added in group order.  Launch with 256 threads and
+// ceil(cols / 32) blocks.
+__global__ void __launch_bounds__(256) k_colsum_bf16(const bf16 *x, int rows, int cols, float *out)
 {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols)
-        return;
+    __shared__ float part[8][32];
+    const int cl = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const int c = blockIdx.x * 32 + cl;
     float s = 0.f;
-    for (int r = 0; r < rows; ++r)
-        s += __bfloat162float(x[(long)r * cols + c]);
-    out[c] = s;
+    if (c < cols)
+        for (int r = g; r < rows; r += 8)
+            s += __bfloat162float(x[(long)r * cols + c]);
+    part[g][cl] = s;
+    __syncthreads();
+    if (g == 0 && c < cols) {
+        float t = part[0][cl];
+        for (int k = 1; k < 8; ++k)
+            t += part[k][cl];
+        out[c] = t;
+    }
 }
 
 // Head gradients: gw4[j] = sum_b dy_b H3[b][j] (j < 128), gb4 = sum_b dy_b.
-__global__ void k_head_grad(const float *dy, const bf16 *h3, int bpad, float *grad)
+// (fixed order as k_colsum_bf16: block b covers outputs j = 32 b .. 32 b + 31,
+// output kH is gb4; launch with 256 threads and kH / 32 + 1 blocks)
+__global__ void __launch_bounds__(256) k_head_grad(const float *dy, const bf16 *h3, int bpad, float *grad)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j > kH)
-        return;
+    __shared__ float part[8][32];
+    const int jl = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const int j = blockIdx.x * 32 + jl;
     float s = 0.f;
-    for (int b = 0; b < bpad; ++b)
-        s += j < kH ? dy[b] * __bfloat162float(h3[(long)b * kH + j]) : dy[b];
-    grad[j < kH ? ow4 + j : ob4] = s;
+    if (j <= kH)
+        for (int b = g; b < bpad; b += 8)
+            s += j < kH ? dy[b] * __bfloat162float(h3[(long)b * kH + j]) : dy[b];
+    part[g][jl] = s;
+    __syncthreads();
+    if (g == 0 && j <= kH) {
+        float t = part[0][jl];
+        for (int k = 1; k < 8; ++k)
+            t += part[k][jl];
+        grad[j < kH ? ow4 + j : ob4] = t;
+    }
 }
 
 // W1 gradient: the first kIn columns of the padded [128][16] product.
@@ -434,7 +501,7 @@ int ensure_acts(mbs_mlp *net, int rows)
     return 0;
 }
 
-dim3 tiles(int M, int N) { return dim3((N + kTile - 1) / kTile, (M + kTile - 1) / kTile); }
+dim3 tiles(int M, int N) { return dim3((N + kTileN - 1) / kTileN, (M + kTile - 1) / kTile); }
 
 // Device flag set by a GEMM whose tensor-core barrier wait ran out (the
 // third int of the network's scalar scratch).
@@ -460,7 +527,7 @@ void gemm(cudaStream_t s, int M, int N, int K, Mat A, Mat B, GemmOut o, int *err
         cudaFuncSetAttribute(k_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
         attr = true;
     }
-    k_gemm<MODE><<<tiles(M, N), 128, kGemmSmem, s>>>(M, N, K, A, B, o, err);
+    k_gemm<MODE><<<tiles(M, N), kGemmThreads, kGemmSmem, s>>>(M, N, K, A, B, o, err);
 }
 
 // Forward pass of n samples already in net->q (device); train keeps the
@@ -493,13 +560,13 @@ int backward_dev(mbs_mlp *net, int n)
     cudaStream_t s = net->stream;
     k_head_bwd<<<(bp * kH + 255) / 256, 256, 0, s>>>(net->y, net->t, n, bp, net->params, net->z3,
                                                      net->dy, net->dz3);
-    k_head_grad<<<1, 160, 0, s>>>(net->dy, net->h3, bp, net->grad);
+    k_head_grad<<<kH / 32 + 1, 256, 0, s>>>(net->dy, net->h3, bp, net->grad);
     GemmOut o{};
     // layer 3: dW3 = dZ3^T H2, db3 = colsum dZ3, dZ2 = (dZ3 W3) * gelu'(Z2)
     o.ldo = kH; o.f = net->grad + oW3;
     gemm<kModeF32>(s, kH, kH, bp, Mat{net->dz3, 1, kH},
                    Mat{net->h2, kH, 1}, o, mlp_err(net));
-    k_colsum_bf16<<<1, kH, 0, s>>>(net->dz3, bp, kH, net->grad + ob3);
+    k_colsum_bf16<<<(kH + 31) / 32, 256, 0, s>>>(net->dz3, bp, kH, net->grad + ob3);
     o = GemmOut{}; o.ldo = kH; o.zin = net->z2; o.h = net->dz2;
     gemm<kModeBwd>(s, bp, kH, kH, Mat{net->dz3, kH, 1},
                    Mat{net->w3, kH, 1}, o, mlp_err(net));
@@ -507,7 +574,7 @@ int backward_dev(mbs_mlp *net, int n)
     o = GemmOut{}; o.ldo = kH; o.f = net->grad + oW2;
     gemm<kModeF32>(s, kH, kH, bp, Mat{net->dz2, 1, kH},
                    Mat{net->h1, kH, 1}, o, mlp_err(net));
-    k_colsum_bf16<<<1, kH, 0, s>>>(net->dz2, bp, kH, net->grad + ob2);
+    k_colsum_bf16<<<(kH + 31) / 32, 256, 0, s>>>(net->dz2, bp, kH, net->grad + ob2);
     o = GemmOut{}; o.ldo = kH; o.zin = net->z1; o.h = net->dz1;
     gemm<kModeBwd>(s, bp, kH, kH, Mat{net->dz2, kH, 1},
                    Mat{net->w2, kH, 1}, o, mlp_err(net));
@@ -516,7 +583,7 @@ int backward_dev(mbs_mlp *net, int n)
     gemm<kModeF32>(s, kH, kInPad, bp, Mat{net->dz1, 1, kH},
                    Mat{net->x0, kInPad, 1}, o, mlp_err(net));
     k_pack_w1_grad<<<(kH * kIn + 127) / 128, 128, 0, s>>>(net->gw1p, net->grad);
-    k_colsum_bf16<<<1, kH, 0, s>>>(net->dz1, bp, kH, net->grad + ob1);
+    k_colsum_bf16<<<(kH + 31) / 32, 256, 0, s>>>(net->dz1, bp, kH, net->grad + ob1);
     MK(cudaGetLastError(), "mlp backward launch");
     return 0;
 }
