@@ -266,7 +266,7 @@ def run_proposal(args):
     tper = {m: [] for m in modes}
     for N in Ns:
         acc = {m: {k: [] for k in regions} for m in modes}
-        for seed in (1, 2):
+        for seed in (1, 2, 3, 4):
             u, v, w = prop.sample(N, seed=seed)
             wp, wm = PR.balance_weights(prop, n_pilot, (tp.pilot_u, tp.pilot_v), (u, v))
             for m, (uu, vv, ww), prec in (("plain_fp64", PR.plain_sobol(N, seed=seed), abi.FP64),
@@ -285,7 +285,7 @@ def run_proposal(args):
            "unit": "s", "higher_is_better": False, "impl": "b200", "n_gpus": 1,
            "config": {"workload": "hexagonal column D=40um L=100um, 1 deg zenith rows x %d azimuth bins; learned "
                                   "proposal (MLP 4-128-128-128-1, BF16 tensor-core training) on "
-                                  "the backscattering rows; 2 scrambles per N" % args.n_phi,
+                                  "the backscattering rows; 4 scrambles per N" % args.n_phi,
                       "orientations": Ns, "reference_orientations": 65536, "pilot_orientations": n_pilot,
                       "epochs": args.proposal_epochs},
            "fit_r2": r2, "proposal_train_s": t_train, "pilot_s": tp.pilot_s, "fit_s": tp.fit_s,
