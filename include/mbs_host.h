@@ -61,8 +61,9 @@ double mbs_host_batch_extinction(const mbs_host_batch *batch, int o);
 double mbs_host_batch_trace_seconds(const mbs_host_batch *batch);
 /* Time split of the batch's production: out3[0] = seconds in the tracer
  * (rotation, shadow beam, ScatterLight) and out3[1] = seconds in
- * PrepareBeams, both summed over the worker threads; out3[2] = wall seconds
- * of packing the prepared orientations into the flat batch. */
+ * PrepareBeams, both summed over the worker threads; out3[2] = seconds of
+ * packing into the flat batch (per-orientation appends summed over the
+ * threads, plus the final gather in orientation order). */
 int    mbs_host_batch_phase_seconds(const mbs_host_batch *batch, double *out3);
 void   mbs_host_batch_free(mbs_host_batch *batch);
 

@@ -29,6 +29,73 @@ mbs_po_beams MbsPackedBeams::view(bool with_raw) const
     return v;
 }
 
+namespace
+{
+
+// One beam into slot b of the (already sized) arrays: vertices from v,
+// absorption paths from a (advanced past them).  Returns the beam's vertex
+// count.
+int pack_beam(const PreparedBeam &pb, bool with_raw, MbsPackedBeams &out, int64_t b, int64_t v,
+              int64_t &a)
+{
+    const BeamEdgeData &ed = pb.edgeData;
+    const int nv = ed.nVertices;
+    out.vert_offsets[b] = v;
+    for (int e = 0; e < nv; ++e)
+    {
+        out.vx[v + e] = ed.x[e];
+        out.vy[v + e] = ed.y[e];
+        // slope_* is only written by PrecomputeEdgeData where the
+        // edge is valid (Handler.cpp:677-690); 0 marks the rest.
+        out.slope_yx[v + e] = ed.edge_valid_x[e] ? ed.slope_yx[e] : 0.0;
+        out.slope_xy[v + e] = ed.edge_valid_y[e] ? ed.slope_xy[e] : 0.0;
+        out.edge_flags[v + e] =
+            (uint8_t)((ed.edge_valid_x[e] ? MBS_PO_EDGE_VALID_X : 0u)
+                    | (ed.edge_valid_y[e] ? MBS_PO_EDGE_VALID_Y : 0u));
+    }
+    double *g = &out.beam_geom[(size_t)b * MBS_PO_GEOM_STRIDE];
+    g[MBS_PO_G_BD + 0] = pb.bdx;  g[MBS_PO_G_BD + 1] = pb.bdy;  g[MBS_PO_G_BD + 2] = pb.bdz;
+    g[MBS_PO_G_HOR + 0] = pb.horAx; g[MBS_PO_G_HOR + 1] = pb.horAy; g[MBS_PO_G_HOR + 2] = pb.horAz;
+    g[MBS_PO_G_VER + 0] = pb.verAx; g[MBS_PO_G_VER + 1] = pb.verAy; g[MBS_PO_G_VER + 2] = pb.verAz;
+    g[MBS_PO_G_CEN + 0] = pb.cenx; g[MBS_PO_G_CEN + 1] = pb.ceny; g[MBS_PO_G_CEN + 2] = pb.cenz;
+    g[MBS_PO_G_AREA] = pb.beam_area;
+    g[MBS_PO_G_NT + 0] = pb.pNTx; g[MBS_PO_G_NT + 1] = pb.pNTy; g[MBS_PO_G_NT + 2] = pb.pNTz;
+    g[MBS_PO_G_NP + 0] = pb.pNPx; g[MBS_PO_G_NP + 1] = pb.pNPy; g[MBS_PO_G_NP + 2] = pb.pNPz;
+    g[MBS_PO_G_NXDT + 0] = pb.pnxDTx; g[MBS_PO_G_NXDT + 1] = pb.pnxDTy; g[MBS_PO_G_NXDT + 2] = pb.pnxDTz;
+    g[MBS_PO_G_NXDP + 0] = pb.pnxDPx; g[MBS_PO_G_NXDP + 1] = pb.pnxDPy; g[MBS_PO_G_NXDP + 2] = pb.pnxDPz;
+    g[MBS_PO_G_JP + 0] = pb.jp00r; g[MBS_PO_G_JP + 1] = pb.jp00i;
+    g[MBS_PO_G_JP + 2] = pb.jp01r; g[MBS_PO_G_JP + 3] = pb.jp01i;
+    g[MBS_PO_G_JP + 4] = pb.jp10r; g[MBS_PO_G_JP + 5] = pb.jp10i;
+    g[MBS_PO_G_JP + 6] = pb.jp11r; g[MBS_PO_G_JP + 7] = pb.jp11i;
+    g[MBS_PO_G_OPATH] = pb.origBeam.opticalPath;
+    out.beam_flags[b] = pb.isExternal ? (uint8_t)MBS_PO_BEAM_EXTERNAL : (uint8_t)0;
+    if (with_raw)
+    {
+        // Raw (unabsorbed, unphased) Jones and phase path/sign for
+        // size rescaling, as GpuDiffraction.cu:310-330 packs them.
+        double *r = &out.beam_raw[(size_t)b * MBS_PO_RAW_STRIDE];
+        const Matrix2x2c &J = pb.origBeam.J;
+        r[0] = real(J.m11); r[1] = imag(J.m11);
+        r[2] = real(J.m12); r[3] = imag(J.m12);
+        r[4] = real(J.m21); r[5] = imag(J.m21);
+        r[6] = real(J.m22); r[7] = imag(J.m22);
+        r[MBS_PO_R_PATH] = pb.isExternal ? pb.origBeam.opticalPath
+                                         : pb.info.projLenght;
+        double sign = 1.0;
+        if (pb.isExternal)
+            sign = -sign;
+        if (!pb.isExternal && (pb.origBeam.nActs & 1))
+            sign = -sign;
+        r[MBS_PO_R_SIGN] = sign;
+        out.abs_offsets[b] = a;
+        for (double path : pb.absorptionPaths)
+            out.abs_paths[a++] = path;
+    }
+    return nv;
+}
+
+}  // namespace
+
 int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
                       int start, int count, bool with_raw,
                       MbsPackedBeams &out, std::string *err)
@@ -101,61 +168,9 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
         out.extinction_ot[oi] = po.extinctionOt;
         for (const PreparedBeam &pb : po.beams)
         {
-            const BeamEdgeData &ed = pb.edgeData;
-            const int nv = ed.nVertices;
-            out.vert_offsets[b] = v;
+            const int nv = pack_beam(pb, with_raw, out, b, v, a);
             if (nv > maxNv)
                 maxNv = nv;
-            for (int e = 0; e < nv; ++e)
-            {
-                out.vx[v + e] = ed.x[e];
-                out.vy[v + e] = ed.y[e];
-                // slope_* is only written by PrecomputeEdgeData where the
-                // edge is valid (Handler.cpp:677-690); 0 marks the rest.
-                out.slope_yx[v + e] = ed.edge_valid_x[e] ? ed.slope_yx[e] : 0.0;
-                out.slope_xy[v + e] = ed.edge_valid_y[e] ? ed.slope_xy[e] : 0.0;
-                out.edge_flags[v + e] =
-                    (uint8_t)((ed.edge_valid_x[e] ? MBS_PO_EDGE_VALID_X : 0u)
-                            | (ed.edge_valid_y[e] ? MBS_PO_EDGE_VALID_Y : 0u));
-            }
-            double *g = &out.beam_geom[(size_t)b * MBS_PO_GEOM_STRIDE];
-            g[MBS_PO_G_BD + 0] = pb.bdx;  g[MBS_PO_G_BD + 1] = pb.bdy;  g[MBS_PO_G_BD + 2] = pb.bdz;
-            g[MBS_PO_G_HOR + 0] = pb.horAx; g[MBS_PO_G_HOR + 1] = pb.horAy; g[MBS_PO_G_HOR + 2] = pb.horAz;
-            g[MBS_PO_G_VER + 0] = pb.verAx; g[MBS_PO_G_VER + 1] = pb.verAy; g[MBS_PO_G_VER + 2] = pb.verAz;
-            g[MBS_PO_G_CEN + 0] = pb.cenx; g[MBS_PO_G_CEN + 1] = pb.ceny; g[MBS_PO_G_CEN + 2] = pb.cenz;
-            g[MBS_PO_G_AREA] = pb.beam_area;
-            g[MBS_PO_G_NT + 0] = pb.pNTx; g[MBS_PO_G_NT + 1] = pb.pNTy; g[MBS_PO_G_NT + 2] = pb.pNTz;
-            g[MBS_PO_G_NP + 0] = pb.pNPx; g[MBS_PO_G_NP + 1] = pb.pNPy; g[MBS_PO_G_NP + 2] = pb.pNPz;
-            g[MBS_PO_G_NXDT + 0] = pb.pnxDTx; g[MBS_PO_G_NXDT + 1] = pb.pnxDTy; g[MBS_PO_G_NXDT + 2] = pb.pnxDTz;
-            g[MBS_PO_G_NXDP + 0] = pb.pnxDPx; g[MBS_PO_G_NXDP + 1] = pb.pnxDPy; g[MBS_PO_G_NXDP + 2] = pb.pnxDPz;
-            g[MBS_PO_G_JP + 0] = pb.jp00r; g[MBS_PO_G_JP + 1] = pb.jp00i;
-            g[MBS_PO_G_JP + 2] = pb.jp01r; g[MBS_PO_G_JP + 3] = pb.jp01i;
-            g[MBS_PO_G_JP + 4] = pb.jp10r; g[MBS_PO_G_JP + 5] = pb.jp10i;
-            g[MBS_PO_G_JP + 6] = pb.jp11r; g[MBS_PO_G_JP + 7] = pb.jp11i;
-            g[MBS_PO_G_OPATH] = pb.origBeam.opticalPath;
-            out.beam_flags[b] = pb.isExternal ? (uint8_t)MBS_PO_BEAM_EXTERNAL : (uint8_t)0;
-            if (with_raw)
-            {
-                // Raw (unabsorbed, unphased) Jones and phase path/sign for
-                // size rescaling, as GpuDiffraction.cu:310-330 packs them.
-                double *r = &out.beam_raw[(size_t)b * MBS_PO_RAW_STRIDE];
-                const Matrix2x2c &J = pb.origBeam.J;
-                r[0] = real(J.m11); r[1] = imag(J.m11);
-                r[2] = real(J.m12); r[3] = imag(J.m12);
-                r[4] = real(J.m21); r[5] = imag(J.m21);
-                r[6] = real(J.m22); r[7] = imag(J.m22);
-                r[MBS_PO_R_PATH] = pb.isExternal ? pb.origBeam.opticalPath
-                                                 : pb.info.projLenght;
-                double sign = 1.0;
-                if (pb.isExternal)
-                    sign = -sign;
-                if (!pb.isExternal && (pb.origBeam.nActs & 1))
-                    sign = -sign;
-                r[MBS_PO_R_SIGN] = sign;
-                out.abs_offsets[b] = a;
-                for (double path : pb.absorptionPaths)
-                    out.abs_paths[a++] = path;
-            }
             v += nv;
             ++b;
         }
@@ -166,5 +181,48 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
     out.vert_offsets[nBeams] = v;
     if (with_raw)
         out.abs_offsets[nBeams] = (int64_t)out.abs_paths.size();
+    return MBS_PO_OK;
+}
+
+int mbs_pack_append(const PreparedOrientation &po, bool with_raw, MbsPackedBeams &part,
+                    std::string *err)
+{
+    int64_t nb = 0, nvt = 0, na = 0;
+    for (const PreparedBeam &pb : po.beams)
+    {
+        const int nv = pb.edgeData.nVertices;
+        if (!pb.edgeData.valid || nv < 3 || nv >= BeamEdgeData::MAX_EDGES)
+        {
+            if (err) *err = "beam without valid edge data (nv=" + std::to_string(nv) + ")";
+            return MBS_PO_EBEAM;
+        }
+        ++nb;
+        nvt += nv;
+        na += (int64_t)pb.absorptionPaths.size();
+    }
+    int64_t b = (int64_t)part.beam_flags.size(), v = (int64_t)part.vx.size();
+    int64_t a = (int64_t)part.abs_paths.size();
+    part.vert_offsets.resize(b + nb);
+    part.vx.resize(v + nvt);
+    part.vy.resize(v + nvt);
+    part.slope_yx.resize(v + nvt);
+    part.slope_xy.resize(v + nvt);
+    part.edge_flags.resize(v + nvt);
+    part.beam_geom.resize((size_t)(b + nb) * MBS_PO_GEOM_STRIDE);
+    part.beam_flags.resize(b + nb);
+    if (with_raw)
+    {
+        part.beam_raw.resize((size_t)(b + nb) * MBS_PO_RAW_STRIDE);
+        part.abs_offsets.resize(b + nb);
+        part.abs_paths.resize(a + na);
+    }
+    for (const PreparedBeam &pb : po.beams)
+    {
+        const int nv = pack_beam(pb, with_raw, part, b, v, a);
+        if (nv > part.max_vertices)
+            part.max_vertices = nv;
+        v += nv;
+        ++b;
+    }
     return MBS_PO_OK;
 }

@@ -39,3 +39,11 @@ struct MbsPackedBeams
 int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
                       int start, int count, bool with_raw,
                       MbsPackedBeams &out, std::string *err);
+
+// Appends one orientation's beams to `part`, whose arrays are plain
+// concatenations: vert_offsets and abs_offsets (size n_beams, no closing
+// entry) index part's own vertex and absorption-path arrays, and
+// beam_offsets, orient_weight and extinction_ot are left to the caller.  The
+// per-beam values are those of mbs_pack_prepared; same validity rule.
+int mbs_pack_append(const PreparedOrientation &po, bool with_raw, MbsPackedBeams &part,
+                    std::string *err);

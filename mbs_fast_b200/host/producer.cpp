@@ -21,6 +21,7 @@
 #include "TracerPOTotal.h"
 #include "Sobol.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -40,7 +41,8 @@ struct mbs_host_batch
     mbs_po_beams view;
     double trace_seconds = 0.0;
     // thread-summed seconds in ScatterLight (with the shadow beam) and in
-    // PrepareBeams, and wall seconds of the packing into the flat batch
+    // PrepareBeams, and seconds of packing into the flat batch (the
+    // per-orientation appends summed over threads plus the final gather)
     double phase_seconds[3] = {0.0, 0.0, 0.0};
 };
 
@@ -195,15 +197,30 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
     {
         HostSetup setup(*cfg);
         const auto t0 = std::chrono::steady_clock::now();
-        std::vector<PreparedOrientation> prepared(n_orient);
         Scattering *master = setup.tracer->m_scattering;
         master->PrepareForParallelTrace();
         bool failed = false;
+        int failCode = MBS_PO_EINVAL;
         std::string failMsg;
-        double scatterSeconds = 0.0, prepareSeconds = 0.0;
-        const int nThreads = cfg->n_threads > 0 ? cfg->n_threads : 0;
-#pragma omp parallel num_threads(nThreads > 0 ? nThreads : omp_get_max_threads())
+        double scatterSeconds = 0.0, prepareSeconds = 0.0, packSeconds = 0.0;
+        const int nThreads = cfg->n_threads > 0 ? cfg->n_threads : omp_get_max_threads();
+        // Every worker prepares into one reused PreparedOrientation and
+        // appends its flat records to its own part; the parts are gathered
+        // in orientation order at the end.  (A PreparedBeam is about 5 KB;
+        // materialising all of them at once costs more in first-touch page
+        // faults than preparing them.)
+        struct Slice
         {
+            int part = 0;
+            int64_t b0 = 0, nb = 0, v0 = 0, nv = 0, a0 = 0, na = 0;
+            double ext = 0.0;
+        };
+        std::vector<Slice> slices(n_orient);
+        std::vector<MbsPackedBeams> parts(nThreads);
+#pragma omp parallel num_threads(nThreads)
+        {
+            const int tid = omp_get_thread_num();
+            MbsPackedBeams &part = parts[tid];
             Particle localParticle = *setup.particle;
             Scattering *localScatter = master->CloneFor(&localParticle, &setup.tracer->m_incidentLight);
             PrepareHandler localHandler(&localParticle, &setup.tracer->m_incidentLight,
@@ -211,7 +228,8 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
             const bool referencePrepare = cfg->reference_prepare != 0;
             localHandler.ConfigureForThreadLocalPrepare(*setup.handler, localScatter);
             std::vector<Beam> localBeams;
-            double tScatter = 0.0, tPrepare = 0.0;
+            PreparedOrientation po;
+            double tScatter = 0.0, tPrepare = 0.0, tPack = 0.0;
 #pragma omp for schedule(dynamic, 1)
             for (int i = 0; i < n_orient; ++i)
             {
@@ -224,21 +242,47 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
                     const bool ok = localScatter->ScatterLight(0, 0, localBeams);
                     const auto b = std::chrono::steady_clock::now();
                     if (ok && referencePrepare)
-                        localHandler.PrepareBeams(localBeams, weight[i], prepared[i]);
+                        localHandler.PrepareBeams(localBeams, weight[i], po);
                     else if (ok)
-                        localHandler.Prepare(localBeams, weight[i], prepared[i]);
+                        localHandler.Prepare(localBeams, weight[i], po);
                     else
-                        prepared[i].sinZenith = weight[i];
+                    {
+                        po.beams.clear();
+                        po.sinZenith = weight[i];
+                        po.extinctionOt = 0.0;
+                    }
                     localBeams.clear();
+                    const auto c = std::chrono::steady_clock::now();
+                    Slice &sl = slices[i];
+                    sl.part = tid;
+                    sl.b0 = (int64_t)part.beam_flags.size();
+                    sl.v0 = (int64_t)part.vx.size();
+                    sl.a0 = (int64_t)part.abs_paths.size();
+                    std::string perr;
+                    const int prc = mbs_pack_append(po, true, part, &perr);
+                    if (prc != MBS_PO_OK)
+                    {
+#pragma omp critical(mbs_host_trace_err)
+                        {
+                            failed = true;
+                            failCode = prc;
+                            failMsg = perr;
+                        }
+                    }
+                    sl.nb = (int64_t)part.beam_flags.size() - sl.b0;
+                    sl.nv = (int64_t)part.vx.size() - sl.v0;
+                    sl.na = (int64_t)part.abs_paths.size() - sl.a0;
+                    sl.ext = po.extinctionOt;
                     tScatter += std::chrono::duration<double>(b - a).count();
-                    tPrepare += std::chrono::duration<double>(std::chrono::steady_clock::now() - b).count();
+                    tPrepare += std::chrono::duration<double>(c - b).count();
+                    tPack += std::chrono::duration<double>(std::chrono::steady_clock::now() - c).count();
                 }
                 catch (const std::exception &e)
                 {
 #pragma omp critical(mbs_host_trace_err)
                     {
                         failed = true;
-                        failMsg = e.what();
+                        failMsg = "tracing failed: " + std::string(e.what());
                     }
                 }
             }
@@ -247,25 +291,75 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
             {
                 scatterSeconds += tScatter;
                 prepareSeconds += tPrepare;
+                packSeconds += tPack;
             }
         }
         if (failed)
         {
-            set_err(err, errlen, "tracing failed: " + failMsg);
-            return MBS_PO_EINVAL;
+            set_err(err, errlen, failMsg);
+            return failCode;
         }
+        // gather the parts in orientation order
+        const auto tg = std::chrono::steady_clock::now();
         std::unique_ptr<mbs_host_batch> batch(new mbs_host_batch());
-        std::string perr;
-        const auto tp = std::chrono::steady_clock::now();
-        const int rc = mbs_pack_prepared(prepared, 0, n_orient, true, batch->packed, &perr);
+        MbsPackedBeams &pk = batch->packed;
+        std::vector<int64_t> B0(n_orient + 1, 0), V0(n_orient + 1, 0), A0(n_orient + 1, 0);
+        for (int i = 0; i < n_orient; ++i)
+        {
+            B0[i + 1] = B0[i] + slices[i].nb;
+            V0[i + 1] = V0[i] + slices[i].nv;
+            A0[i + 1] = A0[i] + slices[i].na;
+        }
+        const int64_t nB = B0[n_orient], nV = V0[n_orient], nA = A0[n_orient];
+        pk.beam_offsets.assign(n_orient + 1, 0);
+        pk.orient_weight.assign(n_orient, 0.0);
+        pk.extinction_ot.assign(n_orient, 0.0);
+        pk.vert_offsets.resize(nB + 1);
+        pk.vx.resize(nV);
+        pk.vy.resize(nV);
+        pk.slope_yx.resize(nV);
+        pk.slope_xy.resize(nV);
+        pk.edge_flags.resize(nV);
+        pk.beam_geom.resize((size_t)nB * MBS_PO_GEOM_STRIDE);
+        pk.beam_flags.resize(nB);
+        pk.beam_raw.resize((size_t)nB * MBS_PO_RAW_STRIDE);
+        pk.abs_offsets.resize(nB + 1);
+        pk.abs_paths.resize(nA);
+        pk.max_vertices = 0;
+        for (const MbsPackedBeams &pt : parts)
+            pk.max_vertices = std::max(pk.max_vertices, pt.max_vertices);
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nThreads)
+        for (int i = 0; i < n_orient; ++i)
+        {
+            const Slice &sl = slices[i];
+            const MbsPackedBeams &pt = parts[sl.part];
+            pk.beam_offsets[i] = B0[i];
+            pk.orient_weight[i] = weight[i];
+            pk.extinction_ot[i] = sl.ext;
+            for (int64_t k = 0; k < sl.nb; ++k)
+            {
+                pk.vert_offsets[B0[i] + k] = pt.vert_offsets[sl.b0 + k] - sl.v0 + V0[i];
+                pk.abs_offsets[B0[i] + k] = pt.abs_offsets[sl.b0 + k] - sl.a0 + A0[i];
+            }
+            std::copy_n(pt.vx.begin() + sl.v0, sl.nv, pk.vx.begin() + V0[i]);
+            std::copy_n(pt.vy.begin() + sl.v0, sl.nv, pk.vy.begin() + V0[i]);
+            std::copy_n(pt.slope_yx.begin() + sl.v0, sl.nv, pk.slope_yx.begin() + V0[i]);
+            std::copy_n(pt.slope_xy.begin() + sl.v0, sl.nv, pk.slope_xy.begin() + V0[i]);
+            std::copy_n(pt.edge_flags.begin() + sl.v0, sl.nv, pk.edge_flags.begin() + V0[i]);
+            std::copy_n(pt.beam_geom.begin() + sl.b0 * MBS_PO_GEOM_STRIDE, sl.nb * MBS_PO_GEOM_STRIDE,
+                        pk.beam_geom.begin() + B0[i] * MBS_PO_GEOM_STRIDE);
+            std::copy_n(pt.beam_flags.begin() + sl.b0, sl.nb, pk.beam_flags.begin() + B0[i]);
+            std::copy_n(pt.beam_raw.begin() + sl.b0 * MBS_PO_RAW_STRIDE, sl.nb * MBS_PO_RAW_STRIDE,
+                        pk.beam_raw.begin() + B0[i] * MBS_PO_RAW_STRIDE);
+            std::copy_n(pt.abs_paths.begin() + sl.a0, sl.na, pk.abs_paths.begin() + A0[i]);
+        }
+        pk.beam_offsets[n_orient] = nB;
+        pk.vert_offsets[nB] = nV;
+        pk.abs_offsets[nB] = nA;
         batch->phase_seconds[0] = scatterSeconds;
         batch->phase_seconds[1] = prepareSeconds;
-        batch->phase_seconds[2] = std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count();
-        if (rc != MBS_PO_OK)
-        {
-            set_err(err, errlen, perr);
-            return rc;
-        }
+        batch->phase_seconds[2] = packSeconds
+            + std::chrono::duration<double>(std::chrono::steady_clock::now() - tg).count();
         batch->view = batch->packed.view(true);
         batch->trace_seconds = std::chrono::duration<double>(
             std::chrono::steady_clock::now() - t0).count();
