@@ -59,14 +59,16 @@ def parse():
                     help="training epochs of the proposal network (workload proposal)")
     ap.add_argument("--proposal-pilot", type=int, default=2048,
                     help="plain Sobol pilot orientations of the proposal (workload proposal)")
-    ap.add_argument("--workload", default="column", choices=["column", "proposal", "aggregate", "refgpu", "mlp", "fftphi"],
+    ap.add_argument("--workload", default="column", choices=["column", "proposal", "aggregate", "refgpu", "mlp", "fftphi",
+                                                          "sizescan"],
                     help="column: the headline line (default); proposal: the learned "
                          "orientation proposal against plain Sobol at equal error; aggregate: "
                          "the non-convex 8-column aggregate (thousands of beams per "
                          "orientation), one graph-captured step per precision; refgpu: the "
                          "reference's own CUDA build against the drop-in binary, same CLI run; mlp: "
                          "training and inference of the proposal network alone; fftphi: the FFT-phi "
-                         "azimuth interpolation path against the direct evaluation")
+                         "azimuth interpolation path against the direct evaluation; sizescan: 16 "
+                         "sizes of one traced batch in one launch")
     return ap.parse_args()
 
 
@@ -448,6 +450,69 @@ def run_fftphi(args):
     print(json.dumps(line), flush=True)
 
 
+def run_sizescan(args):
+    """Size scan on the device (the multi-size path): 16 plates L = 0.2 D, D
+    log-spaced 10-200 um, m = 1.3116, 4 reflections, Sobol orientations
+    traced once at D = 10 um and rescaled on the device for every size, on
+    the non-uniform zenith grid (0.05 deg to 10 deg, 0.5 deg beyond: 541
+    rows) x 48 azimuth bins; one launch for all sizes per step, FP32C and
+    FP64, device-resident inputs (4096 orientations unless --orient is
+    given).  Reports (size, orientation) pairs per second and the FP32C
+    error against FP64 on the largest size."""
+    import torch
+    from mbs_fast_b200 import abi, beams as B
+    from mbs_fast_b200.handler import GpuHandlerPO
+    from tests import common
+    torch.cuda.set_device(0)
+    n = args.orient if args.orient != 16384 else 4096
+    cfg = common.PLATE_D10
+    bs, gs, _ = B.symmetry(cfg)
+    beta, gamma, w = B.sobol_orientations(n, bs, gs, 42)
+    batch = B.trace(cfg, beta, gamma, w)
+    grid = B.grid(0.0, 180.0, args.n_phi, 0, theta_deg=common.size_scan_theta_deg())
+    scales = common.size_scan_diameters() / 10.0
+    h = GpuHandlerPO(grid, B.wave(cfg))
+    st = h.stage_multisize(batch, scales)
+    plane = grid.n_dirs * 16
+    acc = torch.zeros(len(scales) * plane, dtype=torch.float64, device="cuda:0")
+    out = {}
+    planes = {}
+    for prec, name in ((abi.FP32C, "fp32c"), (abi.FP64, "fp64")):
+        best, ms = h.autotune(st, prec, max_orient=min(256, n))
+        for _ in range(args.warmup):
+            acc.zero_()
+            h.diffract_staged(st, acc.data_ptr(), precision=prec, stats=False)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            acc.zero_()
+            h.diffract_staged(st, acc.data_ptr(), precision=prec, stats=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_step = e0.elapsed_time(e1) / args.steps
+        pairs = n * len(scales)
+        out[name] = {"ms_per_step": ms_step, "size_orientations_per_s": pairs / (ms_step * 1e-3),
+                     "beam_dir_evals_per_s": batch.n_beams * len(scales) * grid.n_dirs / (ms_step * 1e-3),
+                     "autotune": {"variant": best, "ms_per_variant": [round(m, 3) for m in ms]}}
+        planes[name] = acc.cpu().numpy().reshape(len(scales), grid.n_az, grid.n_zen + 1, 16)
+    errs = common.element_errors(planes["fp32c"][-1], planes["fp64"][-1], grid)
+    st.free()
+    h.close()
+    line = {"metric": METRIC, "value": out["fp32c"]["size_orientations_per_s"],
+            "unit": "(size, orientation) pairs/s", "impl": "b200", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "f32+f64", "data": "synthetic (reference tracer)",
+            "config": {"workload": "size scan: 16 plates L=0.2D, D 10-200 um log-spaced, m=1.3116, "
+                                   "4 reflections, %d Sobol orientations traced at D=10 um and "
+                                   "rescaled per size, 541 zenith rows (0.05 deg to 10, 0.5 deg "
+                                   "beyond) x %d phi; one launch per step" % (n, args.n_phi),
+                       "beams_per_size": batch.n_beams, "directions": grid.n_dirs},
+            "fp32c": out["fp32c"], "fp64": out["fp64"],
+            "fp32c_error_vs_fp64_largest_size": errs}
+    print(json.dumps(line), flush=True)
+
+
 def run_refgpu(args):
     """Same-box GPU comparison at the CLI: the reference's own CUDA build
     (oracle/_ref/mbs_po_gpu_ref_{fp64,fp32}, its GpuDiffraction.cu for sm_100)
@@ -537,6 +602,9 @@ def main():
         return
     if args.workload == "aggregate":
         run_aggregate(args)
+        return
+    if args.workload == "sizescan":
+        run_sizescan(args)
         return
     if args.workload == "fftphi":
         run_fftphi(args)
