@@ -604,12 +604,15 @@ __device__ __noinline__ void near_forward_s(const DevBeam &g, const double *mom,
 //   P0, Pc, Ps: complWave (R J) parts, 4 complex entries each (see BeamRec)
 //   slab: small-phase candidate test, nearr2: FP32C near-forward zone
 
+//   zone: nonzero when some direction of the CTA's zenith tile may fall in
+//   the near-forward zone or pass the slab test (tile_zone_possible)
+
 template <typename T>
 struct BeamRegs {
     T a[6];
     T slab[4];
     float nearr2;
-    int nv, vs, gbeam;
+    int nv, vs, gbeam, zone;
 };
 
 template <typename T>
@@ -617,14 +620,58 @@ struct SBeamRaw;
 
 template <>
 struct __align__(16) SBeamRaw<float> {
-    float4 q[10];   // a0 a3 a1 a4 | a2 a5 slab0 slab1 | slab2 slab3 nearr2 nv | P[24] | gbeam vs
-                    // ((a0, a3), (a1, a4), (a2, a5): operand pairs of the packed A, B)
+    float4 q[10];   // a0 a3 a1 a4 | a2 a5 slab0 slab1 | slab2 slab3 nearr2 nv | P[24] | gbeam vs zone
+                    // ((a0, a3), (a1, a4), (a2, a5): operand pairs of the packed A, B;
+                    // P entries 2h, 2h+1 of P0, Pc, Ps as (re, re, im, im): the
+                    // real and the imaginary operand pairs of the packed Jones update)
 };
 
 template <>
 struct __align__(16) SBeamRaw<double> {
-    double2 q[18];  // a0a1 a2a3 a4a5 | slab | slab | P[24] | (nearr2,nv) (gbeam,vs)
+    double2 q[18];  // a0a1 a2a3 a4a5 | slab | slab | P[24] | (zone,nv) (gbeam,vs)
+                    // (FP64 has no near-forward zone: the nearr2 word holds the zone flag)
 };
+
+// The zenith tile of a work item seen from the stage fill: every direction
+// w = (sin t, cos t) the CTA evaluates lies within del of wc = (stc, ctc).
+struct TileZone {
+    double stc, ctc, del;
+};
+
+// Whether some direction of the tile can pass the per-pair zone tests of
+// the hot loop for a beam with azimuth-folded coefficients a (A = sin t a0
+// + cos t a1 + a2, B = sin t a3 + cos t a4 + a5): the FP32C near-forward
+// test A^2 + B^2 <= nearr2 and the slab test |A s0 + B s1| <= 1 and
+// |A s2 + B s3| <= 1.  A, B and the slab forms are affine in w, so over
+// the tile they stay within |gradient| del of their values at wc.  The
+// margins cover the hot loop's FP32 rounding of the coefficients, of
+// sin t, cos t and of the sums (below 2.5e-7 of sum |a_i| for A and B), so
+// a tile reported clear holds no pair that the per-pair tests would mark,
+// and skipping those tests there leaves every result unchanged.
+__device__ __forceinline__ bool tile_zone_possible(const double *a, const double *slab, float nearr2,
+                                                   bool f32, const TileZone &z)
+{
+    const double Ac = fma(a[0], z.stc, fma(a[1], z.ctc, a[2]));
+    const double Bc = fma(a[3], z.stc, fma(a[4], z.ctc, a[5]));
+    const double amax = fabs(a[0]) + fabs(a[1]) + fabs(a[2]) + fabs(a[3]) + fabs(a[4]) + fabs(a[5]);
+    const double marg = 1e-6 * amax + 1e-300;
+    if (f32) {
+        const double gq = sqrt(a[0] * a[0] + a[1] * a[1] + a[3] * a[3] + a[4] * a[4]);
+        const double ql = sqrt(Ac * Ac + Bc * Bc) - gq * z.del - 2.0 * marg;
+        if (!(ql > 0.0 && ql * ql > (double)nearr2 * (1.0 + 1e-5)))
+            return true;
+    }
+    bool clear = false;
+#pragma unroll
+    for (int k = 0; k < 4; k += 2) {
+        const double s0 = slab[k], s1 = slab[k + 1];
+        const double uc = fma(Ac, s0, Bc * s1);
+        const double g0 = fma(a[0], s0, a[3] * s1), g1 = fma(a[1], s0, a[4] * s1);
+        const double mu = 2.0 * marg * (fabs(s0) + fabs(s1)) + 1e-6;
+        clear = clear || fabs(uc) - sqrt(g0 * g0 + g1 * g1) * z.del > 1.0 + mu;
+    }
+    return !clear;
+}
 
 template <typename T>
 struct SVertRaw;
@@ -647,11 +694,16 @@ struct StageCfg {
 };
 
 __device__ __forceinline__ void fill_beam(const BrecRef &r, double cp, double sp, int vs, int gbeam,
-                                          SBeamRaw<float> &s)
+                                          const TileZone &z, SBeamRaw<float> &s)
 {
     float a[6], P[24];
-    a[0] = (float)(-(cp * r.ab(0) + sp * r.ab(1))); a[1] = (float)r.ab(2); a[2] = (float)r.ab(3);
-    a[3] = (float)(-(cp * r.ab(4) + sp * r.ab(5))); a[4] = (float)r.ab(6); a[5] = (float)r.ab(7);
+    const double ad[6] = {-(cp * r.ab(0) + sp * r.ab(1)), r.ab(2), r.ab(3),
+                          -(cp * r.ab(4) + sp * r.ab(5)), r.ab(6), r.ab(7)};
+    const double sl[4] = {r.slab(0), r.slab(1), r.slab(2), r.slab(3)};
+    const int zone = tile_zone_possible(ad, sl, r.nearr2(), true, z) ? 1 : 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+        a[i] = (float)ad[i];
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
         P[e] = (float)(sp * r.Q(e) + cp * r.Q(8 + e));
@@ -659,22 +711,26 @@ __device__ __forceinline__ void fill_beam(const BrecRef &r, double cp, double sp
         P[16 + e] = (float)r.Q(32 + e);
     }
     s.q[0] = make_float4(a[0], a[3], a[1], a[4]);
-    s.q[1] = make_float4(a[2], a[5], (float)r.slab(0), (float)r.slab(1));
-    s.q[2] = make_float4((float)r.slab(2), (float)r.slab(3), r.nearr2(), __int_as_float(r.nv()));
+    s.q[1] = make_float4(a[2], a[5], (float)sl[0], (float)sl[1]);
+    s.q[2] = make_float4((float)sl[2], (float)sl[3], r.nearr2(), __int_as_float(r.nv()));
 #pragma unroll
     for (int i = 0; i < 6; ++i)
-        s.q[3 + i] = make_float4(P[4 * i], P[4 * i + 1], P[4 * i + 2], P[4 * i + 3]);
-    s.q[9] = make_float4(__int_as_float(gbeam), __int_as_float(vs), 0.f, 0.f);
+        s.q[3 + i] = make_float4(P[4 * i], P[4 * i + 2], P[4 * i + 1], P[4 * i + 3]);
+    s.q[9] = make_float4(__int_as_float(gbeam), __int_as_float(vs), __int_as_float(zone), 0.f);
 }
 
 __device__ __forceinline__ void fill_beam(const BrecRef &r, double cp, double sp, int vs, int gbeam,
-                                          SBeamRaw<double> &s)
+                                          const TileZone &z, SBeamRaw<double> &s)
 {
-    s.q[0] = make_double2(-(cp * r.ab(0) + sp * r.ab(1)), r.ab(2));
-    s.q[1] = make_double2(r.ab(3), -(cp * r.ab(4) + sp * r.ab(5)));
-    s.q[2] = make_double2(r.ab(6), r.ab(7));
-    s.q[3] = make_double2(r.slab(0), r.slab(1));
-    s.q[4] = make_double2(r.slab(2), r.slab(3));
+    const double ad[6] = {-(cp * r.ab(0) + sp * r.ab(1)), r.ab(2), r.ab(3),
+                          -(cp * r.ab(4) + sp * r.ab(5)), r.ab(6), r.ab(7)};
+    const double sl[4] = {r.slab(0), r.slab(1), r.slab(2), r.slab(3)};
+    const int zone = tile_zone_possible(ad, sl, 0.f, false, z) ? 1 : 0;
+    s.q[0] = make_double2(ad[0], ad[1]);
+    s.q[1] = make_double2(ad[2], ad[3]);
+    s.q[2] = make_double2(ad[4], ad[5]);
+    s.q[3] = make_double2(sl[0], sl[1]);
+    s.q[4] = make_double2(sl[2], sl[3]);
 #pragma unroll
     for (int e = 0; e < 8; e += 2) {
         s.q[5 + e / 2] = make_double2(sp * r.Q(e) + cp * r.Q(8 + e), sp * r.Q(e + 1) + cp * r.Q(9 + e));
@@ -682,8 +738,7 @@ __device__ __forceinline__ void fill_beam(const BrecRef &r, double cp, double sp
                                       -(cp * r.Q(17 + e) + sp * r.Q(25 + e)));
         s.q[13 + e / 2] = make_double2(r.Q(32 + e), r.Q(33 + e));
     }
-    s.q[17] = make_double2(__hiloint2double(r.nv(), __float_as_int(r.nearr2())),
-                           __hiloint2double(vs, gbeam));
+    s.q[17] = make_double2(__hiloint2double(r.nv(), zone), __hiloint2double(vs, gbeam));
 }
 
 // FP32C: p0 carries the range-reduction constant 1.5*2^29 + 1/2, so the
@@ -712,6 +767,7 @@ __device__ __forceinline__ void load_beam(const SBeamRaw<float> &s, BeamRegs<flo
     b.nv = __float_as_int(q2.w);
     b.gbeam = __float_as_int(q9.x);
     b.vs = __float_as_int(q9.y);
+    b.zone = __float_as_int(q9.z);
 }
 
 __device__ __forceinline__ void load_beam(const SBeamRaw<double> &s, BeamRegs<double> &b)
@@ -719,7 +775,8 @@ __device__ __forceinline__ void load_beam(const SBeamRaw<double> &s, BeamRegs<do
     const double2 q0 = s.q[0], q1 = s.q[1], q2 = s.q[2], q3 = s.q[3], q4 = s.q[4], q17 = s.q[17];
     b.a[0] = q0.x; b.a[1] = q0.y; b.a[2] = q1.x; b.a[3] = q1.y; b.a[4] = q2.x; b.a[5] = q2.y;
     b.slab[0] = q3.x; b.slab[1] = q3.y; b.slab[2] = q4.x; b.slab[3] = q4.y;
-    b.nearr2 = __int_as_float(__double2loint(q17.x));
+    b.nearr2 = 0.f;
+    b.zone = __double2loint(q17.x);
     b.nv = __double2hiint(q17.x);
     b.vs = __double2hiint(q17.y);
     b.gbeam = __double2loint(q17.y);
@@ -730,7 +787,7 @@ __device__ __forceinline__ void load_P(const SBeamRaw<float> &s, float *P)
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         const float4 q = s.q[3 + i];
-        P[4 * i] = q.x; P[4 * i + 1] = q.y; P[4 * i + 2] = q.z; P[4 * i + 3] = q.w;
+        P[4 * i] = q.x; P[4 * i + 1] = q.z; P[4 * i + 2] = q.y; P[4 * i + 3] = q.w;
     }
 }
 
@@ -748,9 +805,20 @@ __device__ __forceinline__ void load_P_pair(const SBeamRaw<float> &s, int h, flo
                                             float *ps)
 {
     const float4 a = s.q[3 + h], b = s.q[5 + h], c = s.q[7 + h];
-    p0[0] = a.x; p0[1] = a.y; p0[2] = a.z; p0[3] = a.w;
-    pc[0] = b.x; pc[1] = b.y; pc[2] = b.z; pc[3] = b.w;
-    ps[0] = c.x; ps[1] = c.y; ps[2] = c.z; ps[3] = c.w;
+    p0[0] = a.x; p0[1] = a.z; p0[2] = a.y; p0[3] = a.w;
+    pc[0] = b.x; pc[1] = b.z; pc[2] = b.y; pc[3] = b.w;
+    ps[0] = c.x; ps[1] = c.z; ps[2] = c.y; ps[3] = c.w;
+}
+
+// FP32C packed form of load_P_pair: (re 2h, re 2h+1) and (im 2h, im 2h+1)
+// operand pairs of P0, Pc and Ps, straight from the record's layout.
+__device__ __forceinline__ void load_P_packed(const SBeamRaw<float> &s, int h, float2 &p0r, float2 &p0i,
+                                              float2 &pcr, float2 &pci, float2 &psr, float2 &psi)
+{
+    const float4 a = s.q[3 + h], b = s.q[5 + h], c = s.q[7 + h];
+    p0r = make_float2(a.x, a.y); p0i = make_float2(a.z, a.w);
+    pcr = make_float2(b.x, b.y); pci = make_float2(b.z, b.w);
+    psr = make_float2(c.x, c.y); psi = make_float2(c.z, c.w);
 }
 
 __device__ __forceinline__ void load_P_pair(const SBeamRaw<double> &s, int h, double *p0, double *pc,
@@ -1222,6 +1290,7 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
     T *rslot = rsm + threadIdx.x;
     const int items_per_chunk = P.n_az * P.tiles_per_row;
     __shared__ int s_item;
+    __shared__ double s_zdel[TPB / 32];
 
     // Persistent: take work items until none are left, so CTAs of uneven
     // cost (rare FP64 pairs, ragged beam counts) balance across the SMs.
@@ -1264,6 +1333,21 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
         ct2[d] = make_float2((float)ctT[d], (float)ctT[d]);
     }
     const size_t G = (size_t)P.n_az * P.n_t;
+    // spread of the tile's directions around its middle row, for the zone
+    // flags of the stage fill (read there after the fill's first barrier)
+    {
+        const int tm = min(tile * kDirs + kDirs / 2, P.n_t - 1);
+        const double stc = P.st[tm], ctc = P.ct[tm];
+        double dd = 0.0;
+#pragma unroll
+        for (int d = 0; d < DPT; ++d)
+            dd = fmax(dd, (st[d] - stc) * (st[d] - stc) + (ct[d] - ctc) * (ct[d] - ctc));
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+            dd = fmax(dd, __shfl_xor_sync(0xffffffffu, dd, off));
+        if ((threadIdx.x & 31) == 0)
+            s_zdel[threadIdx.x >> 5] = dd;
+    }
 
     for (int o = o0; o < o1; ++o) {
         JonesAcc<T> J[DPT], Jn[NS ? DPT : 1];
@@ -1292,8 +1376,20 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
             const int nb = be - bs;
             const int nvs = P.vbeg[be] - vb0;
             __syncthreads();   // previous stage fully consumed
+            TileZone tz;
+            {
+                const int tm = min(tile * kDirs + kDirs / 2, P.n_t - 1);
+                double dd = 0.0;
+#pragma unroll
+                for (int w = 0; w < TPB / 32; ++w)
+                    dd = fmax(dd, s_zdel[w]);
+                tz.stc = P.st[tm];
+                tz.ctc = P.ct[tm];
+                tz.del = sqrt(dd) * (1.0 + 1e-12);
+            }
             for (int i = threadIdx.x; i < nb; i += TPB)
-                fill_beam(BrecRef{P.brec + bs + i, P.brec_stride}, cp, sp, P.vbeg[bs + i] - vb0, bs + i, sb[i]);
+                fill_beam(BrecRef{P.brec + bs + i, P.brec_stride}, cp, sp, P.vbeg[bs + i] - vb0, bs + i, tz,
+                          sb[i]);
             for (int i = threadIdx.x; i < nvs; i += TPB)
                 fill_vert(VrecRef{P.vrec + vb0 + i, P.vrec_stride}, cp, sp, sv[i]);
             __syncthreads();
@@ -1313,7 +1409,7 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
             for (int j = j0; j < j1; ++j) {
                 BeamRegs<T> b;
                 load_beam(sb[j], b);
-                T X1[DPT], X2[DPT], sr[DPT], si[DPT], mn[DPT], mden[DPT];
+                T X1[DPT], X2[DPT], sr[DPT], si[DPT], mn[DPT], mden[DPT], Av[DPT], Bv[DPT];
                 bool useX[DPT], rare[DPT];
 #pragma unroll
                 for (int d = 0; d < DPT; ++d) {
@@ -1332,10 +1428,21 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                     X1[d] = useX[d] ? B : A;
                     X2[d] = useX[d] ? A : B;
                     mden[d] = useX[d] ? B : -A;          // x branch: 1/B, y branch: -1/A
-                    const bool near = kF32 && (float)(A * A + B * B) <= b.nearr2;
-                    const bool cand = fabs(fma(A, b.slab[0], B * b.slab[1])) <= T(1)
-                                   && fabs(fma(A, b.slab[2], B * b.slab[3])) <= T(1);
-                    rare[d] = general[d] || near || cand;
+                    Av[d] = A;
+                    Bv[d] = B;
+                    rare[d] = general[d];
+                }
+                // the zone tests only where the stage fill found the tile
+                // may reach the zone (warp-uniform: one beam per iteration)
+                if (b.zone) {
+#pragma unroll
+                    for (int d = 0; d < DPT; ++d) {
+                        const T A = Av[d], B = Bv[d];
+                        const bool near = kF32 && (float)(A * A + B * B) <= b.nearr2;
+                        const bool cand = fabs(fma(A, b.slab[0], B * b.slab[1])) <= T(1)
+                                       && fabs(fma(A, b.slab[2], B * b.slab[3])) <= T(1);
+                        rare[d] = rare[d] || near || cand;
+                    }
                 }
                 if constexpr (kF32) {
                     EdgeHead<DPT> eh;
@@ -1365,30 +1472,34 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                 // J += s x (P0 + cos t Pc + sin t Ps), two complex entries at a time
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    T p0[4], pc[4], ps[4];
-                    load_P_pair(sb[j], h, p0, pc, ps);
                     if constexpr (kF32 && !NS) {
-                        // packed (re, im) pairs: R = P0 + cos t Pc + sin t Ps, then
-                        // J += s R as (-s_i, s_i) (R_i, R_r) + (s_r, s_r) (R_r, R_i),
-                        // the scalar form's operations lane by lane
+                        // entries 2h and 2h+1 side by side: R = P0 + cos t Pc + sin t Ps
+                        // as (re, re) and (im, im) pairs, then J_re += -s_i R_i + s_r R_r
+                        // and J_im += s_i R_r + s_r R_i, the scalar form's operations
+                        // lane by lane (no operand pair needs its halves swapped)
+                        float2 p0r, p0i, pcr, pci, psr, psi;
+                        load_P_packed(sb[j], h, p0r, p0i, pcr, pci, psr, psi);
 #pragma unroll
                         for (int d = 0; d < DPT; ++d) {
                             const float2 srr = make_float2(s_r[d], s_r[d]);
-                            const float2 nsi = make_float2(-s_i[d], s_i[d]);
-#pragma unroll
-                            for (int e = 0; e < 2; ++e) {
-                                const int q = 4 * h + 2 * e;
-                                const float2 R = __ffma2_rn(st2[d], make_float2(ps[2 * e], ps[2 * e + 1]),
-                                                            __ffma2_rn(ct2[d], make_float2(pc[2 * e], pc[2 * e + 1]),
-                                                                       make_float2(p0[2 * e], p0[2 * e + 1])));
-                                float2 jv = make_float2(J[d].b[q], J[d].b[q + 1]);
-                                jv = __ffma2_rn(nsi, make_float2(R.y, R.x), jv);
-                                jv = __ffma2_rn(srr, R, jv);
-                                J[d].b[q] = jv.x;
-                                J[d].b[q + 1] = jv.y;
-                            }
+                            const float2 sii = make_float2(s_i[d], s_i[d]);
+                            const float2 nsi = make_float2(-s_i[d], -s_i[d]);
+                            const float2 Rr = __ffma2_rn(st2[d], psr, __ffma2_rn(ct2[d], pcr, p0r));
+                            const float2 Ri = __ffma2_rn(st2[d], psi, __ffma2_rn(ct2[d], pci, p0i));
+                            float2 jr = make_float2(J[d].b[4 * h], J[d].b[4 * h + 2]);
+                            float2 ji = make_float2(J[d].b[4 * h + 1], J[d].b[4 * h + 3]);
+                            jr = __ffma2_rn(nsi, Ri, jr);
+                            jr = __ffma2_rn(srr, Rr, jr);
+                            ji = __ffma2_rn(sii, Rr, ji);
+                            ji = __ffma2_rn(srr, Ri, ji);
+                            J[d].b[4 * h] = jr.x;
+                            J[d].b[4 * h + 2] = jr.y;
+                            J[d].b[4 * h + 1] = ji.x;
+                            J[d].b[4 * h + 3] = ji.y;
                         }
                     } else {
+                        T p0[4], pc[4], ps[4];
+                        load_P_pair(sb[j], h, p0, pc, ps);
 #pragma unroll
                         for (int d = 0; d < DPT; ++d) {
 #pragma unroll
