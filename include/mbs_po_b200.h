@@ -157,6 +157,19 @@ int mbs_po_set_wave(mbs_po_ctx *ctx, const mbs_po_wave *wave);
 int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
                     double *M_accum, double *Mns_accum, mbs_po_stats *stats);
 
+/* The same call without the host addition: *M_out (and *Mns_out, when
+ * Mns_out is non-NULL, for the sums over non-external beams) receive
+ * pointers to this call's weighted Mueller sums in the context's
+ * page-locked host buffer, [n_az*(n_zen+1)*16] doubles each, valid until
+ * the next call on ctx; NULL when the batch holds no beams.  For callers
+ * whose accumulators are not one flat array -- the reference's Arr2D keeps
+ * every 4x4 cell in its own allocation (src/math/PhysMtr.cpp:6-17) -- so the
+ * result reaches them in one pass instead of a flat addition and a second
+ * pass.  Drop-in form of HandleOrientationsToLocalGpu
+ * (GpuDiffraction.cu:4159-4778, accumulation at 4751-4766). */
+int mbs_po_diffract_pinned(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
+                           const double **M_out, const double **Mns_out, mbs_po_stats *stats);
+
 /* Device-resident path: stage a batch once (H2D + device layout), then run
  * it any number of times.  M_accum_dev / Mns_accum_dev are DEVICE pointers to
  * [n_az*(n_zen+1)*16] doubles, accumulated (+=) on `stream` (a cudaStream_t,

@@ -161,6 +161,37 @@ int ensure_arena(mbs_po_ctx *ctx, Arena &a, size_t bytes, const char *what)
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Context-owned arenas that are reused call after call (the upload area and
+// the host entry points' staged batch).  Every earlier use of them has
+// completed when they grow (stage_into and the host entry points end with a
+// stream synchronisation), so the old block is released and the new one
+// taken in stream order on `st`: unlike cudaFree, that waits for no other
+// work on the device -- in the reference's CLI, tracer threads run their own
+// kernels while a diffraction call stages its batch.  They grow to at least
+// twice the request and four times the old size, so batches that grow call
+// by call (SelectGpuOrientationBatchSize doubles them) reallocate rarely.
+int grow_arena(mbs_po_ctx *ctx, Arena &a, size_t bytes, const char *what, cudaStream_t st)
+{
+    if (bytes <= a.cap && a.base)
+        return MBS_PO_OK;
+    if (a.base) {
+        cudaError_t e = cudaFreeAsync(a.base, st);
+        if (e != cudaSuccess)
+            return fail(ctx, MBS_PO_ECUDA, std::string("cudaFreeAsync ") + what + ": " + cudaGetErrorString(e));
+    }
+    a.base = nullptr;
+    const size_t want = std::max<size_t>({(size_t)2 * bytes, (size_t)4 * a.cap, (size_t)1 << 20});
+    const size_t cap = (want + ((size_t)1 << 21) - 1) & ~(((size_t)1 << 21) - 1);
+    a.cap = 0;
+    cudaError_t e = cudaMallocAsync(&a.base, cap, st);
+    if (e != cudaSuccess) {
+        a.base = nullptr;
+        return fail(ctx, MBS_PO_ENOMEM, std::string("cudaMallocAsync ") + what + ": " + cudaGetErrorString(e));
+    }
+    a.cap = cap;
+    return MBS_PO_OK;
+}
+
 void staged_release(mbs_po_staged *s)
 {
     cudaFree(s->arena.base);
@@ -410,7 +441,7 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     const size_t off_ao = off_raw + align256(scales ? nB * MBS_PO_RAW_STRIDE * 8 : 0);
     const size_t off_ap = off_ao + align256(has_abs ? (nB + 1) * 8 : 0);
     const size_t raw_bytes = off_ap + align256(nAbs * 8);
-    if ((rc = ensure_arena(ctx, ctx->raw, raw_bytes, "staging")))
+    if ((rc = grow_arena(ctx, ctx->raw, raw_bytes, "staging", st)))
         return rc;
     unsigned char *raw = (unsigned char *)ctx->raw.base;
     // device records (nI instances)
@@ -424,7 +455,8 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     const size_t o_boff = o_vbeg + align256((iB + 1) * sizeof(int32_t));
     const size_t o_w = o_boff + align256((iO + 1) * sizeof(int32_t));
     const size_t bytes = o_w + align256(std::max<int64_t>(iO, 1) * sizeof(double));
-    if ((rc = ensure_arena(ctx, s->arena, bytes, "staged batch")))
+    if ((rc = (s == &ctx->host_staged ? grow_arena(ctx, s->arena, bytes, "staged batch", st)
+                                      : ensure_arena(ctx, s->arena, bytes, "staged batch"))))
         return rc;
     unsigned char *base = (unsigned char *)s->arena.base;
     s->beams = (DevBeam *)(base + o_beams);
@@ -884,10 +916,18 @@ int run_phi_interp(mbs_po_ctx *ctx, const double *low, int n_low, int n_rows, do
 // (one size instance only): the planes are interpolated from the grid's
 // n_az azimuth bins to n_full bins on the device first, and the caller's
 // planes are [n_full][n_zen+1][16].
+// With `view` set, nothing is added into M_accum / Mns_accum: view[0] (and
+// view[1] when no-shadow sums are asked for by a non-null Mns_accum) receive
+// pointers to the planes in the page-locked result buffer, or NULL when the
+// batch holds nothing to add.
 int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scales, int n_scales,
                   double k_rephase, int precision, double *M_accum, double *Mns_accum,
-                  mbs_po_stats *stats, int n_full = 0)
+                  mbs_po_stats *stats, int n_full = 0, const double **view = nullptr)
 {
+    if (view) {
+        view[0] = nullptr;
+        view[1] = nullptr;
+    }
     if (!ctx || !beams || !M_accum)
         return fail(ctx, MBS_PO_EINVAL, "null argument");
     if (!ctx->has_grid || !ctx->has_wave)
@@ -942,11 +982,16 @@ int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scal
     float h2d = 0.f, d2h = 0.f;
     cudaEventElapsedTime(&h2d, ctx->ev[3], ctx->ev[4]);
     cudaEventElapsedTime(&d2h, ctx->ev[5], ctx->ev[7]);
-    for (size_t i = 0; i < n_out; ++i)
-        M_accum[i] += ctx->hres[i];
-    if (ns)
+    if (view) {
+        view[0] = ctx->hres;
+        view[1] = ns ? ctx->hres + n_out : nullptr;
+    } else {
         for (size_t i = 0; i < n_out; ++i)
-            Mns_accum[i] += ctx->hres[n_out + i];
+            M_accum[i] += ctx->hres[i];
+        if (ns)
+            for (size_t i = 0; i < n_out; ++i)
+                Mns_accum[i] += ctx->hres[n_out + i];
+    }
     if (stats) {
         stats->h2d_ms = h2d;
         stats->d2h_ms = d2h;
@@ -961,6 +1006,29 @@ extern "C" int mbs_po_diffract(mbs_po_ctx *ctx, const mbs_po_beams *beams, int p
                                double *M_accum, double *Mns_accum, mbs_po_stats *stats)
 {
     return diffract_host(ctx, beams, nullptr, 0, 0.0, precision, M_accum, Mns_accum, stats);
+}
+
+extern "C" int mbs_po_diffract_pinned(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,
+                                      const double **M_out, const double **Mns_out, mbs_po_stats *stats)
+{
+    if (M_out)
+        *M_out = nullptr;
+    if (Mns_out)
+        *Mns_out = nullptr;
+    if (!ctx)
+        return MBS_PO_EINVAL;
+    if (!M_out)
+        return fail(ctx, MBS_PO_EINVAL, "null argument");
+    // a non-null dummy accumulator selects the no-shadow sums; nothing is
+    // written through either in view mode
+    double dummy = 0.0;
+    const double *view[2] = {nullptr, nullptr};
+    const int rc = diffract_host(ctx, beams, nullptr, 0, 0.0, precision, &dummy, Mns_out ? &dummy : nullptr,
+                                 stats, 0, view);
+    *M_out = view[0];
+    if (Mns_out)
+        *Mns_out = view[1];
+    return rc;
 }
 
 extern "C" int mbs_po_diffract_fft_phi(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,

@@ -41,6 +41,8 @@ def lib() -> C.CDLL:
         L.mbs_po_set_wave.argtypes = [vp, C.POINTER(abi.Wave)]
         L.mbs_po_diffract.argtypes = [vp, C.POINTER(abi.Beams), C.c_int, abi._dp, abi._dp,
                                       C.POINTER(abi.Stats)]
+        L.mbs_po_diffract_pinned.argtypes = [vp, C.POINTER(abi.Beams), C.c_int,
+                                             C.POINTER(abi._dp), C.POINTER(abi._dp), C.POINTER(abi.Stats)]
         L.mbs_po_stage.argtypes = [vp, C.POINTER(abi.Beams), C.POINTER(vp)]
         L.mbs_po_staged_free.argtypes = [vp, vp]
         L.mbs_po_diffract_staged.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -144,6 +146,23 @@ class GpuHandlerPO:
             return False
         self._call(rc, "mbs_po_diffract")
         return True
+
+    def diffract_pinned(self, batch: BeamBatch, noshadow: bool = False,
+                        precision: int = abi.FP64):
+        """mbs_po_diffract_pinned: this call's Mueller sums as copies of the
+        library's page-locked planes, (M, M_noshadow or None); (None, None)
+        when the batch holds no beams."""
+        b = batch.as_c(with_raw=False)
+        m, mn = abi._dp(), abi._dp()
+        rc = lib().mbs_po_diffract_pinned(self.ctx, C.byref(b), precision, C.byref(m),
+                                          C.byref(mn) if noshadow else None, C.byref(self.last_stats))
+        self._call(rc, "mbs_po_diffract_pinned")
+        shape = (self.grid.n_az, self.grid.n_zen + 1, 16)
+        n = shape[0] * shape[1] * shape[2]
+
+        def grab(ptr):
+            return np.ctypeslib.as_array(ptr, (n,)).reshape(shape).copy() if ptr else None
+        return grab(m), grab(mn)
 
     # -- HandlerPO::HandleOrientationsToLocalGpuFftPhi ----------------------
     @staticmethod

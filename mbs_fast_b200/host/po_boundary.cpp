@@ -197,6 +197,22 @@ static int current_device()
     return dev;
 }
 
+// Adds a [n_az][n_rows][16] plane into the caller's Arr2D, whose cells are
+// separate allocations (PhysMtr.cpp:6-17): one pass, azimuth rows spread over
+// the OpenMP threads (serial when the caller is itself a parallel region).
+static void add_plane(const double *plane, Arr2D &M, int nAz, int nRows)
+{
+#pragma omp parallel for schedule(static) if (nAz >= 8)
+    for (int p = 0; p < nAz; ++p)
+        for (int t = 0; t < nRows; ++t)
+        {
+            const double *m = plane + ((size_t)p * nRows + t) * 16;
+            double *cell = M.RawCell(p, t);
+            for (int q = 0; q < 16; ++q)
+                cell[q] += m[q];
+        }
+}
+
 static bool diffract_range(HandlerPO &h, const ScatteringRange &sphere,
                            const std::vector<PreparedOrientation> &prepared,
                            int start, int count, Arr2D &localM,
@@ -219,33 +235,21 @@ static bool diffract_range(HandlerPO &h, const ScatteringRange &sphere,
     if (!HandlerPOBoundary::Prepare(h, sphere, HandlerPOWaveAccess::Get(h, 0.0), device))
         return false;
     BoundaryContext &c = g_ctx;
-    const size_t n = (size_t)nAz * (nZen + 1) * 16;
-    c.M.assign(n, 0.0);
-    if (computeNoShadow)
-        c.Mns.assign(n, 0.0);
     mbs_po_stats st;
     std::memset(&st, 0, sizeof(st));
-    const int rc = mbs_po_diffract(c.ctx, &view, precision_from_env(), c.M.data(),
-                                   computeNoShadow ? c.Mns.data() : nullptr, &st);
+    // the sums stay in the library's page-locked buffer and are added into
+    // the Arr2D cells in one pass
+    const double *Mv = nullptr, *Mnv = nullptr;
+    const int rc = mbs_po_diffract_pinned(c.ctx, &view, precision_from_env(), &Mv,
+                                          computeNoShadow ? &Mnv : nullptr, &st);
     if (rc == MBS_PO_EBEAM)
         return false;
     if (!report(rc, "diffraction"))
         return false;
-    for (int p = 0; p < nAz; ++p)
-        for (int t = 0; t <= nZen; ++t)
-        {
-            const double *m = &c.M[((size_t)p * (nZen + 1) + t) * 16];
-            double *cell = localM.RawCell(p, t);
-            for (int q = 0; q < 16; ++q)
-                cell[q] += m[q];
-            if (computeNoShadow)
-            {
-                const double *mn = &c.Mns[((size_t)p * (nZen + 1) + t) * 16];
-                double *cn = localM_noshadow.RawCell(p, t);
-                for (int q = 0; q < 16; ++q)
-                    cn[q] += mn[q];
-            }
-        }
+    if (Mv)
+        add_plane(Mv, localM, nAz, nZen + 1);
+    if (Mnv)
+        add_plane(Mnv, localM_noshadow, nAz, nZen + 1);
     if (timing)
     {
         const double pack = std::chrono::duration<double, std::milli>(t1 - t0).count();
@@ -297,20 +301,11 @@ static bool diffract_scaled(HandlerPO &h, const ScatteringRange &sphere,
     if (!report(rc, "multi-size diffraction"))
         return false;
     for (size_t s = 0; s < scales.size(); ++s)
-        for (int p = 0; p < nAz; ++p)
-            for (int t = 0; t <= nZen; ++t)
-            {
-                const size_t off = s * plane + ((size_t)p * (nZen + 1) + t) * 16;
-                double *cell = Ms[s]->RawCell(p, t);
-                for (int q = 0; q < 16; ++q)
-                    cell[q] += c.M[off + q];
-                if (Mns)
-                {
-                    double *cn = (*Mns)[s]->RawCell(p, t);
-                    for (int q = 0; q < 16; ++q)
-                        cn[q] += c.Mns[off + q];
-                }
-            }
+    {
+        add_plane(c.M.data() + s * plane, *Ms[s], nAz, nZen + 1);
+        if (Mns)
+            add_plane(c.Mns.data() + s * plane, *(*Mns)[s], nAz, nZen + 1);
+    }
     if (env_is("MBS_GPU_TIMING", "1"))
         std::fprintf(stderr,
                      "GPU timing multik path=b200-%s orient=%d sizes=%zu beams=%lld nAz=%d nZen=%d "
@@ -551,20 +546,9 @@ bool HandlerPO::HandleOrientationsToLocalGpuFftPhi(const std::vector<PreparedOri
                          est, m_fftTolerance, nCheck);
         }
     }
-    for (int p = 0; p < nFull; ++p)
-        for (int t = 0; t < nRows; ++t)
-        {
-            const size_t off = ((size_t)p * nRows + t) * 16;
-            double *cell = localM.RawCell(p, t);
-            for (int q = 0; q < 16; ++q)
-                cell[q] += fftM[off + q];
-            if (ns)
-            {
-                double *cn = localM_noshadow.RawCell(p, t);
-                for (int q = 0; q < 16; ++q)
-                    cn[q] += fftMns[off + q];
-            }
-        }
+    add_plane(fftM.data(), localM, nFull, nRows);
+    if (ns)
+        add_plane(fftMns.data(), localM_noshadow, nFull, nRows);
     return true;
 }
 

@@ -149,6 +149,27 @@ def test_fixed_orientation_config0():
     h.close()
 
 
+def test_pinned_result_equals_host_accumulation(hex_case):
+    """mbs_po_diffract_pinned hands back exactly what mbs_po_diffract adds
+    (both precisions, with and without the no-shadow sums); an empty batch
+    gives no planes."""
+    cfg, batch, grid, wave, h, _, _ = hex_case
+    for prec in (abi.FP64, abi.FP32C):
+        M, Mns = h.new_mueller(), h.new_mueller()
+        assert h.handle_orientations_to_local_gpu(batch, M, Mns, precision=prec)
+        a, an = h.diffract_pinned(batch, noshadow=True, precision=prec)
+        np.testing.assert_array_equal(a, M)
+        np.testing.assert_array_equal(an, Mns)
+        # without no-shadow sums the launch shape differs: compare with the
+        # plain host call
+        M1 = h.new_mueller()
+        assert h.handle_orientations_to_local_gpu(batch, M1, precision=prec)
+        b, bn = h.diffract_pinned(batch, precision=prec)
+        np.testing.assert_array_equal(b, M1)
+        assert bn is None
+    assert h.diffract_pinned(batch.select(0, 0)) == (None, None)
+
+
 def test_edge_cases(hex_case):
     cfg, batch, grid, wave, h, _, _ = hex_case
     # empty batch: nothing added
