@@ -176,6 +176,18 @@ int mbs_po_diffract_pinned(mbs_po_ctx *ctx, const mbs_po_beams *beams, int preci
  * NULL for the legacy default stream). */
 int mbs_po_stage(mbs_po_ctx *ctx, const mbs_po_beams *beams, mbs_po_staged **out);
 int mbs_po_staged_free(mbs_po_ctx *ctx, mbs_po_staged *staged);
+/* Re-fill a staged batch with another host batch, in the device memory it
+ * already holds (grown in stream order when the new batch needs more).  For
+ * producers that stage batch after batch: a ring of staged batches re-filled
+ * this way stops allocating once its slots have grown and never frees,
+ * where mbs_po_staged_free + mbs_po_stage release memory (cudaFree waits for
+ * all work on the device, the next batch's diffraction included) and take
+ * it again.  Every diffraction that reads `staged` must have completed
+ * before the call (synchronise its stream, or an event recorded after it).
+ * On failure the staged batch holds no orientations until it is re-filled.
+ * No counterpart in the reference, which uploads every batch anew
+ * (GpuDiffraction.cu:4159-4778). */
+int mbs_po_restage(mbs_po_ctx *ctx, const mbs_po_beams *beams, mbs_po_staged *staged);
 int mbs_po_diffract_staged(mbs_po_ctx *ctx, const mbs_po_staged *staged,
                            int precision, double *M_accum_dev,
                            double *Mns_accum_dev, void *stream,

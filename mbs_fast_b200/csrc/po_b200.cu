@@ -78,6 +78,7 @@ struct mbs_po_staged {
     int max_nv = 0;
     int n_sets = 1;                // output planes (size instances)
     int orient_per_set = 0;
+    bool reused = false;           // re-filled by mbs_po_restage: grows like a context arena
 };
 
 struct mbs_po_ctx {
@@ -455,8 +456,8 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     const size_t o_boff = o_vbeg + align256((iB + 1) * sizeof(int32_t));
     const size_t o_w = o_boff + align256((iO + 1) * sizeof(int32_t));
     const size_t bytes = o_w + align256(std::max<int64_t>(iO, 1) * sizeof(double));
-    if ((rc = (s == &ctx->host_staged ? grow_arena(ctx, s->arena, bytes, "staged batch", st)
-                                      : ensure_arena(ctx, s->arena, bytes, "staged batch"))))
+    if ((rc = (s == &ctx->host_staged || s->reused ? grow_arena(ctx, s->arena, bytes, "staged batch", st)
+                                                   : ensure_arena(ctx, s->arena, bytes, "staged batch"))))
         return rc;
     unsigned char *base = (unsigned char *)s->arena.base;
     s->beams = (DevBeam *)(base + o_beams);
@@ -810,6 +811,28 @@ extern "C" int mbs_po_stage(mbs_po_ctx *ctx, const mbs_po_beams *beams, mbs_po_s
     }
     *out = s;
     return MBS_PO_OK;
+}
+
+extern "C" int mbs_po_restage(mbs_po_ctx *ctx, const mbs_po_beams *beams, mbs_po_staged *s)
+{
+    if (!ctx)
+        return MBS_PO_EINVAL;
+    if (!s || !beams)
+        return fail(ctx, MBS_PO_EINVAL, "null argument");
+    s->reused = true;
+    int rc = stage_into(ctx, beams, s, ctx->stream);
+    if (!rc) {
+        const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess)
+            rc = cuda_fail(ctx, e, "restage sync");
+    }
+    if (rc) {   // nothing usable is left in it until the next successful restage
+        s->n_orient = 0;
+        s->n_beams = s->n_verts = 0;
+        s->orient_per_set = 0;
+        s->n_sets = 1;
+    }
+    return rc;
 }
 
 extern "C" int mbs_po_staged_free(mbs_po_ctx *ctx, mbs_po_staged *s)

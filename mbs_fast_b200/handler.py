@@ -45,6 +45,7 @@ def lib() -> C.CDLL:
                                              C.POINTER(abi._dp), C.POINTER(abi._dp), C.POINTER(abi.Stats)]
         L.mbs_po_stage.argtypes = [vp, C.POINTER(abi.Beams), C.POINTER(vp)]
         L.mbs_po_staged_free.argtypes = [vp, vp]
+        L.mbs_po_restage.argtypes = [vp, C.POINTER(abi.Beams), vp]
         L.mbs_po_diffract_staged.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.POINTER(abi.Stats)]
         L.mbs_po_extinction.argtypes = [vp, C.POINTER(abi.Beams), abi._dp]
@@ -79,7 +80,10 @@ class Staged:
     def __init__(self, handler: "GpuHandlerPO", handle: C.c_void_p, batch: BeamBatch):
         self._h = handler
         self.handle = handle
-        self.n_sets = int(lib().mbs_po_staged_sets(handle))
+        self._count(batch)
+
+    def _count(self, batch: BeamBatch) -> None:
+        self.n_sets = int(lib().mbs_po_staged_sets(self.handle))
         self.n_orient = batch.n_orient * self.n_sets
         self.n_beams = batch.n_beams * self.n_sets
         self.n_verts = batch.n_verts * self.n_sets
@@ -360,6 +364,15 @@ class GpuHandlerPO:
         b = batch.as_c(with_raw=False)
         self._call(lib().mbs_po_stage(self.ctx, C.byref(b), C.byref(h)), "mbs_po_stage")
         return Staged(self, h, batch)
+
+    def restage(self, staged: Staged, batch: BeamBatch) -> Staged:
+        """mbs_po_restage: re-fill `staged` with `batch` in the device memory
+        it holds (every diffraction reading it must have completed)."""
+        b = batch.as_c(with_raw=False)
+        rc = lib().mbs_po_restage(self.ctx, C.byref(b), staged.handle)
+        staged._count(batch if rc == 0 else batch.select(0, 0))
+        self._call(rc, "mbs_po_restage")
+        return staged
 
     def diffract_staged(self, staged: Staged, m_dev_ptr: int, mns_dev_ptr: int | None = None,
                         precision: int = abi.FP64, stream: int = 0,

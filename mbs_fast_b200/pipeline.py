@@ -51,29 +51,35 @@ def orientation_average(handler, cfg, beta, gamma, weight, precision: int = abi.
     t0 = time.perf_counter()
     th = threading.Thread(target=producer, daemon=True)
     th.start()
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    staged = []
+    cur = torch.cuda.current_stream(dev)
+    stream = cur.cuda_stream
+    # a ring of depth + 1 staged batches, each re-filled (mbs_po_restage) once
+    # the stream has passed the diffraction that read it: the next batch is
+    # staged while the previous ones diffract, and nothing is freed (cudaFree
+    # would wait for the whole device) or allocated once the slots have grown
+    ring = []
     n_beams = 0
     while True:
         b = q.get()
         if b is None:
             break
         n_beams += b.n_beams
-        st = handler.stage(b)
+        if len(ring) > depth:
+            st, ev = ring.pop(0)
+            ev.synchronize()
+            handler.restage(st, b)
+        else:
+            st = handler.stage(b)
+        # stats=False: the call neither times nor waits for its kernels
         handler.diffract_staged(st, acc.data_ptr(), acc_ns.data_ptr() if noshadow else None,
-                                precision=precision, stream=stream)
-        staged.append(st)
-        # keep at most `depth` staged batches alive (their records are in use
-        # until the stream passes them)
-        if len(staged) > depth:
-            torch.cuda.current_stream(dev).synchronize()
-            for s_ in staged[:-1]:
-                s_.free()
-            staged = staged[-1:]
+                                precision=precision, stream=stream, stats=False)
+        ev = torch.cuda.Event()
+        ev.record(cur)
+        ring.append((st, ev))
     th.join()
-    torch.cuda.current_stream(dev).synchronize()
-    for s_ in staged:
-        s_.free()
+    cur.synchronize()
+    for st, _ in ring:
+        st.free()
     if err:
         raise err[0]
     wall = time.perf_counter() - t0

@@ -101,6 +101,39 @@ def test_staged_path_equals_host_path(hex_case):
     st.free()
 
 
+def test_restage_equals_fresh_stage(hex_case):
+    """mbs_po_restage re-fills a staged batch (smaller, larger, then smaller
+    batches than it held) with results bitwise equal to a freshly staged
+    batch; a malformed batch is rejected and leaves nothing to diffract."""
+    import torch
+    cfg, batch, grid, wave, h, _, _ = hex_case
+    n = grid.n_az * (grid.n_zen + 1) * 16
+
+    def run(st):
+        dev = torch.zeros(n, dtype=torch.float64, device="cuda:0")
+        torch.cuda.synchronize()
+        h.diffract_staged(st, dev.data_ptr(), precision=abi.FP32C)
+        torch.cuda.synchronize()
+        return dev.cpu().numpy()
+
+    ring = h.stage(batch.select(2, 3))
+    bigger = common.sobol_batch("hex40x100", 24)
+    for b in (batch.select(0, 2), bigger, batch, batch.select(5, 1)):
+        fresh = h.stage(b)
+        np.testing.assert_array_equal(run(h.restage(ring, b)), run(fresh))
+        assert ring.n_orient == b.n_orient and ring.n_beams == b.n_beams
+        fresh.free()
+    bad = batch.select(0, 1)
+    bad.vert_offsets = bad.vert_offsets.copy()
+    bad.vert_offsets[1] = bad.vert_offsets[0] + 2
+    bad.vert_offsets[2:] = np.maximum(bad.vert_offsets[2:], bad.vert_offsets[1])
+    with pytest.raises(Exception):
+        h.restage(ring, bad)
+    assert not run(ring).any()
+    np.testing.assert_array_equal(run(h.restage(ring, batch)), run(h.stage(batch)))
+    ring.free()
+
+
 def test_extinction_on_device(hex_case):
     cfg, batch, grid, wave, h, _, _ = hex_case
     cext = h.extinction(batch)
