@@ -95,3 +95,50 @@ def test_extinction_known_answers_gpu():
         cext = h.extinction(batch).sum() / batch.orient_weight.sum()
         h.close()
         assert abs(cext / case["cext"] - 1) <= case["rel_tol"], case["case"]
+
+
+# The reference's basic functional test (tests/run_tests.sh:129-146): hexagonal
+# column D = H = 10 um, m = 1.31, 6 reflections, 256 Sobol orientations, grid
+# 48 x 90: Q_sca = 2.05 +/- 10 %.  For a non-absorbing particle the reference
+# reports C_sca = C_ext from the optical theorem over the mean projected area
+# (IntegralCharacteristics.cpp:128-137, 161-163); for a convex particle that mean
+# is a quarter of the surface area (Cauchy), here with the circumscribed
+# diameter of Hexagonal.cpp:54 (side = D / 2).
+QSCA_CFG = B.ParticleConfig(particle_type=1, p=(10.0, 10.0), ri_re=1.31, ri_im=0.0,
+                            wavelength=0.532, max_reflections=6)
+QSCA_EXPECTED, QSCA_REL_TOL = 2.05, 0.10
+
+
+def _qsca_batch():
+    bs, gs, _ = B.symmetry(QSCA_CFG)
+    beta, gamma, w = B.sobol_orientations(256, bs, gs, 42)
+    return B.trace(QSCA_CFG, beta, gamma, w)
+
+
+def _mean_projected_area():
+    side, height = 10.0 / 2, 10.0
+    surface = 2 * (3 * np.sqrt(3) / 2) * side ** 2 + 6 * side * height
+    return surface / 4
+
+
+def test_qsca_known_answer_host():
+    """Q_sca of the reference's functional test from the reference tracer's
+    optical-theorem extinction and from the oracle's restatement."""
+    batch = _qsca_batch()
+    area = _mean_projected_area()
+    q_tracer = batch.extinction_ot.sum() / batch.orient_weight.sum() / area
+    q_oracle = oracle.po_extinction(batch, B.wave(QSCA_CFG)).sum() / batch.orient_weight.sum() / area
+    print("Q_sca tracer", q_tracer, "oracle", q_oracle)
+    assert abs(q_tracer / QSCA_EXPECTED - 1) <= QSCA_REL_TOL
+    assert abs(q_oracle / QSCA_EXPECTED - 1) <= QSCA_REL_TOL
+
+
+@pytest.mark.gpu
+def test_qsca_known_answer_gpu():
+    """The same Q_sca from the device extinction kernel."""
+    from mbs_fast_b200.handler import GpuHandlerPO
+    batch = _qsca_batch()
+    h = GpuHandlerPO(B.grid(0.0, 180.0, 48, 90), B.wave(QSCA_CFG))
+    q = h.extinction(batch).sum() / batch.orient_weight.sum() / _mean_projected_area()
+    h.close()
+    assert abs(q / QSCA_EXPECTED - 1) <= QSCA_REL_TOL
