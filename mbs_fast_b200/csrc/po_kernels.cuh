@@ -1291,6 +1291,7 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
     const int items_per_chunk = P.n_az * P.tiles_per_row;
     __shared__ int s_item;
     __shared__ double s_zdel[TPB / 32];
+    __shared__ int s_rwarp[TPB / 32], s_rbase[TPB], s_rok[TPB];   // the spread FP64 pass
 
     // Persistent: take work items until none are left, so CTAs of uneven
     // cost (rare FP64 pairs, ragged beam counts) balance across the SMs.
@@ -1535,35 +1536,119 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                 }
             }
             }
-            // FP64 pass over this thread's marked pairs of the stage.
-            const int words = (nb + 31) >> 5;
+            // FP64 pass over the stage's marked pairs, spread over all the
+            // CTA's threads: a pair's owner (the thread whose direction it
+            // is) seldom has company in its warp, so per-owner loops left most
+            // lanes idle and the CTA waiting at the next stage for its
+            // busiest warp.  The marked pairs are numbered owner by owner in
+            // the owners' (direction, beam) order; in rounds of TPB, thread i
+            // evaluates pair r0 + i into its result slot, then every owner
+            // adds its own results in that order, the order of a per-owner
+            // loop, so the sums are the same bit for bit.
+            {
+                const int words = (nb + 31) >> 5;
+                const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+                int cnt = 0;
 #pragma unroll
-            for (int d = 0; d < DPT; ++d) {
-                for (int w = 0; w < words; ++w) {
-                    uint32_t m = rmask[(d * kMaskWords + w) * TPB + threadIdx.x];
-                    while (m) {
-                        const int j = w * 32 + __ffs(m) - 1;
-                        m &= m - 1;
+                for (int d = 0; d < DPT; ++d)
+                    for (int w = 0; w < words; ++w)
+                        cnt += __popc(rmask[(d * kMaskWords + w) * TPB + threadIdx.x]);
+                int incl = cnt;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, off);
+                    if (lane >= off)
+                        incl += v;
+                }
+                if (lane == 31)
+                    s_rwarp[warp] = incl;
+                __syncthreads();   // the warp totals and every thread's masks are visible
+                int base = incl - cnt, total = 0;
+#pragma unroll
+                for (int w2 = 0; w2 < TPB / 32; ++w2) {
+                    const int v = s_rwarp[w2];
+                    base += w2 < warp ? v : 0;
+                    total += v;
+                }
+                s_rbase[threadIdx.x] = base;
+                __syncthreads();
+                // the owner's cursor over its own marked pairs
+                int cd = 0, cw = 0;
+                uint32_t cm = words > 0 ? rmask[threadIdx.x] : 0u;
+                for (int r0 = 0; r0 < total; r0 += TPB) {
+                    const int q = r0 + threadIdx.x;
+                    int okv = 0;
+                    if (q < total) {
+                        int lo = 0, hi = TPB - 1;   // owner: the last o with s_rbase[o] <= q
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (s_rbase[mid] <= q) lo = mid; else hi = mid - 1;
+                        }
+                        const int o = lo;
+                        int k = q - s_rbase[o], od = 0, j = 0;
+                        bool found = false;
+                        for (int d2 = 0; d2 < DPT && !found; ++d2)
+                            for (int w = 0; w < words && !found; ++w) {
+                                uint32_t m = rmask[(d2 * kMaskWords + w) * TPB + o];
+                                const int c = __popc(m);
+                                if (k < c) {
+                                    for (int i = 0; i < k; ++i)
+                                        m &= m - 1;
+                                    j = w * 32 + __ffs(m) - 1;
+                                    od = d2;
+                                    found = true;
+                                } else {
+                                    k -= c;
+                                }
+                            }
+                        const int to = tile * kDirs + od * TPB + o;   // < n_t: marked pairs are active
+                        const double sto = P.st[to], cto = P.ct[to];
+                        const bool gen = P.row_kind[to] == 2;
+                        const T stTo = (T)sto, ctTo = (T)cto;
                         BeamRegs<T> b;
                         load_beam(sb[j], b);
-                        const T A = fma(stT[d], b.a[0], fma(ctT[d], b.a[1], b.a[2]));
-                        const T B = fma(stT[d], b.a[3], fma(ctT[d], b.a[4], b.a[5]));
-                        const bool near = kF32 && !general[d] && (float)(A * A + B * B) <= b.nearr2;
+                        const T A = fma(stTo, b.a[0], fma(ctTo, b.a[1], b.a[2]));
+                        const T B = fma(stTo, b.a[3], fma(ctTo, b.a[4], b.a[5]));
+                        const bool near = kF32 && !gen && (float)(A * A + B * B) <= b.nearr2;
                         const bool cand = fabs(fma(A, b.slab[0], B * b.slab[1])) <= T(1)
                                        && fabs(fma(A, b.slab[2], B * b.slab[3])) <= T(1);
-                        const bool ok = (general[d] || near || cand)
-                                      ? beam_rare<T>(P, b.gbeam, &sb[j], p, t[d], near, rslot, TPB)
-                                      : beam_sing<T>(P, &sb[j], sv, vb0, st[d], ct[d], rslot, TPB);
-                        if (ok) {
+                        okv = ((gen || near || cand)
+                                   ? beam_rare<T>(P, b.gbeam, &sb[j], p, to, near, rslot, TPB)
+                                   : beam_sing<T>(P, &sb[j], sv, vb0, sto, cto, rslot, TPB)) ? 1 : 0;
+                    }
+                    s_rok[threadIdx.x] = okv;
+                    __syncthreads();   // this round's results are in the slots
+                    const int q0 = max(base, r0), q1 = min(base + cnt, r0 + TPB);
+                    for (int qq = q0; qq < q1; ++qq) {
+                        while (cm == 0u) {
+                            if (++cw == words) {
+                                cw = 0;
+                                ++cd;
+                            }
+                            cm = rmask[(cd * kMaskWords + cw) * TPB + threadIdx.x];
+                        }
+                        const int j = cw * 32 + __ffs(cm) - 1;
+                        cm &= cm - 1;
+                        const int slot = qq - r0;
+                        if (s_rok[slot]) {
                             T dj[8];
 #pragma unroll
-                            for (int q = 0; q < 8; ++q)
-                                dj[q] = rslot[q * TPB];
-                            J[d].add(dj);
-                            if (NS && !(P.beams[b.gbeam].flags & MBS_PO_BEAM_EXTERNAL))
-                                Jn[NS ? d : 0].add(dj);
+                            for (int i = 0; i < 8; ++i)
+                                dj[i] = rsm[slot + i * TPB];
+#pragma unroll
+                            for (int d2 = 0; d2 < DPT; ++d2)
+                                if (d2 == cd) {
+                                    J[d2].add(dj);
+                                    if (NS) {
+                                        BeamRegs<T> bj;
+                                        load_beam(sb[j], bj);
+                                        if (!(P.beams[bj.gbeam].flags & MBS_PO_BEAM_EXTERNAL))
+                                            Jn[NS ? d2 : 0].add(dj);
+                                    }
+                                }
                         }
                     }
+                    __syncthreads();   // the slots are read before the next round
                 }
             }
             if (kF32) {
