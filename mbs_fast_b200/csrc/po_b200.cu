@@ -106,6 +106,7 @@ struct mbs_po_ctx {
     int *d_status = nullptr;      // [0] pack status, [1] work counter of the diffraction kernel
     mbs_po_staged host_staged;   // reused by mbs_po_diffract
     cudaEvent_t ev[8] = {};
+    cudaEvent_t partial_done = nullptr;   // recorded after each launch that used `partial`
     int variant[2] = {0, 0};     // chosen launch shape per precision
 };
 
@@ -161,6 +162,36 @@ int ensure_arena(mbs_po_ctx *ctx, Arena &a, size_t bytes, const char *what)
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// The orientation-chunk partials grow with the batch (more chunks) and are
+// used on the caller's stream.  The old block is released in stream order on
+// `st` after the last launch that used it (the partial_done event, recorded
+// after each use on whatever stream that was), and the new one taken in
+// stream order, at least twice the old size: a cudaFree here waits for all
+// work on the device, in the reference's CLI the tracer threads' kernels too.
+int grow_partial(mbs_po_ctx *ctx, size_t n, cudaStream_t st)
+{
+    if (n <= ctx->partial_cap && ctx->partial)
+        return MBS_PO_OK;
+    cudaError_t e = cudaSuccess;
+    if (ctx->partial) {
+        e = cudaStreamWaitEvent(st, ctx->partial_done, 0);
+        if (e == cudaSuccess)
+            e = cudaFreeAsync(ctx->partial, st);
+        if (e != cudaSuccess)
+            return fail(ctx, MBS_PO_ECUDA, std::string("releasing the partials: ") + cudaGetErrorString(e));
+    }
+    ctx->partial = nullptr;
+    const size_t want = std::max<size_t>(n, 2 * ctx->partial_cap);
+    ctx->partial_cap = 0;
+    e = cudaMallocAsync((void **)&ctx->partial, want * sizeof(double), st);
+    if (e != cudaSuccess) {
+        ctx->partial = nullptr;
+        return fail(ctx, MBS_PO_ENOMEM, std::string("cudaMallocAsync partials: ") + cudaGetErrorString(e));
+    }
+    ctx->partial_cap = want;
+    return MBS_PO_OK;
+}
 
 // Context-owned arenas that are reused call after call (the upload area and
 // the host entry points' staged batch).  Every earlier use of them has
@@ -257,6 +288,8 @@ extern "C" int mbs_po_create(mbs_po_ctx **out, int device)
     for (int i = 0; i < 8 && e == cudaSuccess; ++i)
         e = cudaEventCreate(&ctx->ev[i]);
     if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&ctx->partial_done, cudaEventDisableTiming);
+    if (e == cudaSuccess)
         e = cudaMalloc((void **)&ctx->d_status, 64);
     if (e != cudaSuccess) {
         delete ctx;
@@ -286,6 +319,8 @@ extern "C" int mbs_po_destroy(mbs_po_ctx *ctx)
     staged_release(&ctx->host_staged);
     for (int i = 0; i < 8; ++i)
         if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    if (ctx->partial_done)
+        cudaEventDestroy(ctx->partial_done);
     if (ctx->stream)
         cudaStreamDestroy(ctx->stream);
     if (ctx->side)
@@ -662,7 +697,7 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     const LaunchPlan L = plan_launch(nAz, nT, per_set, V.tpb * V.dpt, V.minb, n_sets);
     const size_t plane = (size_t)16 * G;
     int rc;
-    if ((rc = ensure(ctx, ctx->partial, ctx->partial_cap, plane * L.n_chunks * (ns ? 2 : 1), "partials")))
+    if ((rc = grow_partial(ctx, plane * L.n_chunks * (ns ? 2 : 1), st)))
         return rc;
     KParams P;
     P.beams = s->beams;
@@ -725,6 +760,7 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
         CK(cudaGetLastError(), "reduce launch");
         ++launches;
     }
+    CK(cudaEventRecord(ctx->partial_done, st), "event");
     CK(cudaEventRecord(ctx->ev[2], st), "event");
     if (stats) {
         CK(cudaEventSynchronize(ctx->ev[2]), "event sync");
