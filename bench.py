@@ -747,8 +747,8 @@ def main():
         "e2e_with_tracing": {"value": batch.n_orient / tp["wall_s"], "unit": "orientations/s",
                              "wall_s": tp["wall_s"], "host_trace_s": tp["trace_s"],
                              "what": "reference tracer and restated PrepareBeams on all host "
-                                     "cores, batches of 1024, overlapped with FP32C diffraction "
-                                     "on the device"},
+                                     "cores but one (which stages the batches), batches of 1024, "
+                                     "overlapped with FP32C diffraction on the device"},
         "gpu_launches": launches,
         "autotune": tuned,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
