@@ -134,6 +134,23 @@ def test_restage_equals_fresh_stage(hex_case):
     ring.free()
 
 
+def test_growing_batches_on_one_context(hex_case):
+    """Host calls whose batches grow and shrink on one context (the upload
+    area, the staged batch and the chunk partials grow in stream order
+    between them) give bitwise the results of a fresh context per batch."""
+    cfg, batch, grid, wave, h, _, _ = hex_case
+    big = common.sobol_batch("hex40x100", 40)
+    for prec in (abi.FP64, abi.FP32C):
+        for b in (big.select(0, 2), big.select(2, 8), big, big.select(7, 3)):
+            M = h.new_mueller()
+            assert h.handle_orientations_to_local_gpu(b, M, precision=prec)
+            fresh = GpuHandlerPO(grid, wave)
+            R = fresh.new_mueller()
+            assert fresh.handle_orientations_to_local_gpu(b, R, precision=prec)
+            fresh.close()
+            np.testing.assert_array_equal(M, R)
+
+
 def test_extinction_on_device(hex_case):
     cfg, batch, grid, wave, h, _, _ = hex_case
     cext = h.extinction(batch)
