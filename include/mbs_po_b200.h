@@ -282,8 +282,9 @@ int mbs_po_extinction(mbs_po_ctx *ctx, const mbs_po_beams *beams,
                       double *cext_out);
 
 /* Upper bound on the orientations per call that fit `mem_fraction` of the
- * device's free memory.  Replaces HandlerPO::SelectGpuOrientationBatchSize
- * (reference GpuDiffraction.cu:2948-3029). */
+ * device's free memory.  Reads only n_orient, beam_offsets and vert_offsets
+ * of `beams` (the other arrays may be NULL).  Replaces
+ * HandlerPO::SelectGpuOrientationBatchSize (reference GpuDiffraction.cu:2948-3029). */
 int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams,
                         int start, int max_count, double mem_fraction,
                         int *count_out);

@@ -44,6 +44,9 @@ struct BoundaryContext
     mbs_po_wave wave{};
     bool waveSet = false;
     std::vector<double> M, Mns;
+    // the main path's packed batch, kept between calls so that its pages are
+    // not allocated and first touched again on every call
+    MbsPackedBeams packed;
 
     ~BoundaryContext()
     {
@@ -221,7 +224,7 @@ static bool diffract_range(HandlerPO &h, const ScatteringRange &sphere,
     const bool timing = env_is("MBS_GPU_TIMING", "1");
     const auto t0 = std::chrono::steady_clock::now();
     const int nAz = sphere.nAzimuth, nZen = sphere.nZenith;
-    MbsPackedBeams packed;
+    MbsPackedBeams &packed = g_ctx.packed;
     std::string err;
     const int prc = mbs_pack_prepared(prepared, start, count, false, packed, &err);
     if (prc == MBS_PO_EBEAM)
@@ -612,13 +615,33 @@ int HandlerPO::SelectGpuOrientationBatchSize(const std::vector<PreparedOrientati
 {
     if (maxCount <= 1)
         return std::max(1, maxCount);
-    MbsPackedBeams packed;
-    if (mbs_pack_prepared(prepared, start, maxCount, false, packed, nullptr) != MBS_PO_OK)
+    if (start < 0 || start > (int)prepared.size())
         return std::max(1, maxCount);
+    // the selector reads only the orientations' beam and vertex counts: build
+    // those, not the whole packed batch; a beam without valid edge data keeps
+    // the full count, as a failed packing did
+    const int n = std::min(maxCount, (int)prepared.size() - start);
+    std::vector<int64_t> bo(n + 1, 0), vo(1, 0);
+    for (int oi = 0; oi < n; ++oi)
+    {
+        for (const PreparedBeam &pb : prepared[start + oi].beams)
+        {
+            const int nv = pb.edgeData.nVertices;
+            if (!pb.edgeData.valid || nv < 3 || nv >= BeamEdgeData::MAX_EDGES)
+                return std::max(1, maxCount);
+            vo.push_back(vo.back() + nv);
+        }
+        bo[oi + 1] = (int64_t)vo.size() - 1;
+    }
     if (!HandlerPOBoundary::Prepare(*this, m_sphere, HandlerPOWaveAccess::Get(*this, 0.0),
                                     current_device()))
         return std::max(1, maxCount);
-    const mbs_po_beams view = packed.view(false);
+    mbs_po_beams view{};
+    view.n_orient = n;
+    view.n_beams = bo[n];
+    view.n_verts = vo.back();
+    view.beam_offsets = bo.data();
+    view.vert_offsets = vo.data();
     int count = maxCount;
     if (mbs_po_select_batch(g_ctx.ctx, &view, 0, maxCount, mem_fraction(), &count) != MBS_PO_OK)
         return std::max(1, maxCount);
