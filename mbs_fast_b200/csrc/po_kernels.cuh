@@ -1237,8 +1237,11 @@ __device__ __noinline__ bool beam_sing(const KParams &P, const SBeamRaw<T> *sbr,
 // Accumulator of the coherent Jones sum of one orientation for one
 // direction.  FP32: plain sums over blocks of kFlushEvery beams in
 // registers, folded into a Kahan-compensated running sum kept in shared
-// memory (s, c with stride) at every block end.  FP64: plain sums.
-constexpr int kFlushEvery = 16;
+// memory (s, c with stride) at every block end.  FP64: plain sums.  Blocks
+// of 32 beams: against 16 the step is 1.7 % shorter and the FP32C error
+// against FP64 unchanged (it comes from the FP32 trigonometry, not from the
+// block sums).
+constexpr int kFlushEvery = 32;
 
 template <typename T>
 struct JonesAcc {
