@@ -16,12 +16,22 @@ the orientation average, in the FP32-compensated precision.
   e2e   : the same through the public C-ABI call mbs_po_diffract with pinned
           host buffers: H2D of the beam arrays, kernels, D2H of the Mueller
           grid, every step.
-The FP64 path runs once on the same batch as the error reference.
+  roofline : algorithmic flop / the diffraction kernel's CUDA-event time
+          against the measured FFMA peak (and the nominal one); the plain
+          FP64 kernel against the measured DFMA peak.
+  parity_vs_reference : FP64 and FP32C through the C ABI against the
+          reference's own CPU result on the cpu_baseline sample (M11, the
+          normalised elements, C_sca, g, C_ext).
+  reference_gpu : the reference's own CUDA build against the drop-in binary
+          on the same box, kernels and whole calls.
+The FP64 path runs once on the whole batch as the error reference and the
+plain FP64 batched path's time.
 
 --impl reference times the reference's own CPU implementation of the path
 (HandlerPO::HandleBeamsToLocal + AddToMuellerLocal under OpenMP, built from
-the reference sources into oracle/_ref) on a bounded sample of the same
-orientations, with every host thread.
+the reference sources into oracle/_ref, its tracer and PrepareBeams making
+the beams) on a bounded sample of the same orientations, with every host
+thread.  --gpus N without a torchrun environment starts N ranks itself.
 """
 from __future__ import annotations
 
@@ -55,6 +65,12 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=48, help="orientations in the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error reference")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-refgpu", action="store_true",
+                    help="skip the same-box comparison with the reference's CUDA build")
+    ap.add_argument("--refgpu-orient", type=int, default=1024,
+                    help="orientations of the same-box comparison with the reference's CUDA build")
+    ap.add_argument("--launch-selftest", action="store_true",
+                    help="ranks only exchange one gloo all-reduce (tests the --gpus N launcher on the CPU)")
     ap.add_argument("--proposal-epochs", type=int, default=400,
                     help="training epochs of the proposal network (workload proposal)")
     ap.add_argument("--proposal-pilot", type=int, default=2048,
@@ -80,9 +96,12 @@ def dist_env():
 
 
 def build_inputs(args, rank, world):
-    from mbs_fast_b200 import beams as B
-    cfg = B.ParticleConfig(particle_type=1, p=(100.0, 40.0), ri_re=1.3116, ri_im=1e-9,
-                           wavelength=0.532, max_reflections=4)
+    from mbs_fast_b200 import beams as B, workloads as W
+    cfg = W.COLUMN_40x100
+    if world > 1:
+        # ranks share the host cores (torchrun also sets OMP_NUM_THREADS=1)
+        import dataclasses
+        cfg = dataclasses.replace(cfg, n_threads=max(1, (os.cpu_count() or 1) // world))
     bs, gs, _ = B.symmetry(cfg)
     beta, gamma, w = B.sobol_orientations(args.orient, bs, gs, 42)
     # weak scaling: every rank owns its own contiguous orientation shard of
@@ -168,61 +187,100 @@ def measured_peaks() -> dict:
         return {}
 
 
-def cpu_baseline(cfg, batch, args) -> dict:
-    """Reference CPU path (oracle/_ref) on a bounded sample, all host threads."""
+def reference_sample(cfg, batch, args):
+    """The reference's CPU path (oracle/_ref, all host threads) on a bounded
+    sample of the batch: the first --cpu-sample orientations on the full grid.
+    Returns (cpu_baseline dict, the reference's Mueller grid, its C_ext per
+    orientation, the sample), or the restatement's figures when the
+    reference library is absent."""
     import oracle
     n = min(args.cpu_sample, batch.n_orient)
     sample = batch.select(0, n)
     spec = (0.0, 180.0, args.n_phi, args.n_theta)
     if oracle.have_reference():
-        _, _, _, sec = oracle.ref_batch(cfg, spec, sample, n_threads=0)
+        M_ref, _, cext_ref, sec = oracle.ref_batch(cfg, spec, sample, n_threads=0)
         kind = "reference"
     else:
         from mbs_fast_b200 import beams as B
         t0 = time.perf_counter()
-        oracle.po_diffract(sample, B.grid(*spec), B.wave(cfg), n_threads=0)
+        M_ref = oracle.po_diffract(sample, B.grid(*spec), B.wave(cfg), n_threads=0)
         sec = time.perf_counter() - t0
+        cext_ref = oracle.po_extinction(sample, B.wave(cfg))
         kind = "port"
-    return {"value": n / sec, "unit": "orientations/s", "cores": os.cpu_count(), "kind": kind,
+    base = {"value": n / sec, "unit": "orientations/s", "cores": os.cpu_count(), "kind": kind,
             "sample": f"{n} of the {batch.n_orient} orientations on the full "
                       f"{args.n_phi}x{args.n_theta + 1} grid ({sec:.2f} s)",
             "beam_dir_evals_per_s": sample.n_beams * args.n_phi * (args.n_theta + 1) / sec}
+    return base, M_ref, cext_ref, sample
+
+
+def parity_vs_reference(h, sample, M_ref, cext_ref) -> dict:
+    """FP64 and FP32C results of the reference's sample, diffracted through
+    the C ABI, against the reference's own CPU result of the same
+    orientations: M11, the normalised elements, C_sca, g and C_ext (device
+    extinction kernel against the reference's ComputeForwardExtinctionOt)."""
+    from mbs_fast_b200 import abi, metrics
+    out = {"orientations": sample.n_orient}
+    cext = h.extinction(sample)
+    for prec, name in ((abi.FP64, "fp64"), (abi.FP32C, "fp32c")):
+        M = h.new_mueller()
+        h.handle_orientations_to_local_gpu(sample, M, precision=prec)
+        out[name] = metrics.compare(h, M, M_ref, cext, cext_ref)
+    return out
 
 
 def run_reference(args):
+    """The reference's own CPU implementation of the path on the host cores:
+    its tracer and PrepareBeams build the orientations' beams (untimed), its
+    OpenMP HandleBeamsToLocal + AddToMuellerLocal loop is timed, every host
+    thread, on a bounded sample of the headline workload's orientations."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     import oracle
-    cfg, batch, grid, wave, _ = build_inputs(
-        argparse.Namespace(**{**vars(args), "orient": max(args.cpu_sample, 8)}), 0, 1)
+    from mbs_fast_b200 import workloads as W
+    cfg = W.COLUMN_40x100
+    n = max(1, args.cpu_sample)
     spec = (0.0, 180.0, args.n_phi, args.n_theta)
-    n = min(args.cpu_sample, batch.n_orient)
-    sample = batch.select(0, n)
     kind = "reference" if oracle.have_reference() else "port"
-    for _ in range(args.warmup if args.warmup < 2 else 1):
-        oracle.ref_batch(cfg, spec, sample.select(0, 2), n_threads=0) if kind == "reference" else None
-    times = []
-    for _ in range(args.steps):
-        if kind == "reference":
-            _, _, _, sec = oracle.ref_batch(cfg, spec, sample, n_threads=0)
-        else:
+    if kind == "reference":
+        beta, gamma, w = oracle.ref_orientations(cfg, args.orient, 42)
+        beta, gamma, w = beta[:n], gamma[:n], w[:n]
+        for _ in range(min(args.warmup, 1)):
+            oracle.ref_run(cfg, spec, beta[:2], gamma[:2], w[:2])
+        times = []
+        for _ in range(args.steps):
+            _, _, _, _, td = oracle.ref_run(cfg, spec, beta, gamma, w)
+            times.append(td)
+        n_beams = None
+    else:
+        from mbs_fast_b200 import beams as B
+        bs, gs, _ = B.symmetry(cfg)
+        beta, gamma, w = B.sobol_orientations(args.orient, bs, gs, 42)
+        sample = B.trace(cfg, beta[:n], gamma[:n], w[:n])
+        grid, wave = B.grid(*spec), B.wave(cfg)
+        times = []
+        for _ in range(args.steps):
             t0 = time.perf_counter()
             oracle.po_diffract(sample, grid, wave, n_threads=0)
-            sec = time.perf_counter() - t0
-        times.append(sec)
+            times.append(time.perf_counter() - t0)
+        n_beams = sample.n_beams
     sec = float(np.mean(times))
     v = n / sec
     line = {"metric": METRIC, "value": v, "unit": "orientations/s", "n_gpus": 0, "impl": "reference",
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (beams from the reference tracer)",
+            "data": "synthetic (beams from the reference's own tracer and PrepareBeams)",
             "config": {"workload": WORKLOAD, "sample_orientations": n},
             "cpu_baseline": {"value": v, "unit": "orientations/s", "cores": os.cpu_count(),
-                             "kind": kind, "sample": f"{n} orientations per step on the full grid"},
+                             "kind": kind,
+                             "sample": f"the first {n} of the {args.orient} Sobol orientations per "
+                                       f"step on the full {args.n_phi}x{args.n_theta + 1} grid; "
+                                       "diffraction phase timed"},
             "e2e": {"value": v, "unit": "orientations/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0},
-            "beam_dir_evals_per_s": sample.n_beams * args.n_phi * (args.n_theta + 1) / sec}
+                    "d2h_bytes_per_step": 0}}
+    if n_beams:
+        line["beam_dir_evals_per_s"] = n_beams * args.n_phi * (args.n_theta + 1) / sec
     print(json.dumps(line), flush=True)
 
 
@@ -317,12 +375,12 @@ def run_aggregate(args):
     import tempfile
     import torch
     from mbs_fast_b200 import abi, beams as B
+    from mbs_fast_b200 import workloads as W
     from mbs_fast_b200.handler import GpuHandlerPO
-    from tests import common
     torch.cuda.set_device(0)
     n = args.orient if args.orient != 16384 else 32
     path = os.path.join(tempfile.mkdtemp(), "agg8.particle")
-    cfg = common.aggregate_config(path)
+    cfg = W.aggregate_config(path)
     bs, gs, _ = B.symmetry(cfg)
     beta, gamma, w = B.sobol_orientations(n, bs, gs, 42)
     t0 = time.perf_counter()
@@ -384,12 +442,11 @@ def run_fftphi(args):
     of the azimuth-averaged rows and of the grid against the direct result."""
     import torch
     from mbs_fast_b200 import abi, beams as B
+    from mbs_fast_b200 import metrics, workloads as W
     from mbs_fast_b200.handler import GpuHandlerPO
-    from tests import common
     torch.cuda.set_device(0)
     n = args.orient if args.orient != 16384 else 2048
-    cfg = B.ParticleConfig(particle_type=1, p=(100.0, 40.0), ri_re=1.3116, ri_im=1e-9,
-                           wavelength=0.532, max_reflections=4)
+    cfg = W.COLUMN_40x100
     bs, gs, _ = B.symmetry(cfg)
     beta, gamma, w = B.sobol_orientations(n, bs, gs, 42)
     batch = B.trace(cfg, beta, gamma, w)
@@ -431,9 +488,8 @@ def run_fftphi(args):
     ms_direct, ms_fft = timed(direct), timed(fft)
     Md = acc_f.cpu().numpy().reshape(full.n_az, rows, 16)
     Mi = acc_i.cpu().numpy().reshape(full.n_az, rows, 16)
-    errs = common.element_errors(Mi, Md, full)
-    errs["weighted_L2_rows"] = common.weighted_l2(Mi, Md, full)
-    errs["L2_grid"] = common.grid_l2(Mi, Md)
+    errs = metrics.compare(hf, Mi, Md)
+    errs["L2_grid"] = float(np.sqrt(np.sum((Mi - Md) ** 2) / max(np.sum(Md ** 2), 1e-300)))
     for s_ in (sf, sl):
         s_.free()
     hf.close()
@@ -461,16 +517,16 @@ def run_sizescan(args):
     error against FP64 on the largest size."""
     import torch
     from mbs_fast_b200 import abi, beams as B
+    from mbs_fast_b200 import metrics, workloads as W
     from mbs_fast_b200.handler import GpuHandlerPO
-    from tests import common
     torch.cuda.set_device(0)
     n = args.orient if args.orient != 16384 else 4096
-    cfg = common.PLATE_D10
+    cfg = W.PLATE_D10
     bs, gs, _ = B.symmetry(cfg)
     beta, gamma, w = B.sobol_orientations(n, bs, gs, 42)
     batch = B.trace(cfg, beta, gamma, w)
-    grid = B.grid(0.0, 180.0, args.n_phi, 0, theta_deg=common.size_scan_theta_deg())
-    scales = common.size_scan_diameters() / 10.0
+    grid = B.grid(0.0, 180.0, args.n_phi, 0, theta_deg=W.size_scan_theta_deg())
+    scales = W.size_scan_diameters() / 10.0
     h = GpuHandlerPO(grid, B.wave(cfg))
     st = h.stage_multisize(batch, scales)
     plane = grid.n_dirs * 16
@@ -496,7 +552,7 @@ def run_sizescan(args):
                      "beam_dir_evals_per_s": batch.n_beams * len(scales) * grid.n_dirs / (ms_step * 1e-3),
                      "autotune": {"variant": best, "ms_per_variant": [round(m, 3) for m in ms]}}
         planes[name] = acc.cpu().numpy().reshape(len(scales), grid.n_az, grid.n_zen + 1, 16)
-    errs = common.element_errors(planes["fp32c"][-1], planes["fp64"][-1], grid)
+    errs = metrics.compare(h, planes["fp32c"][-1], planes["fp64"][-1])
     st.free()
     h.close()
     line = {"metric": METRIC, "value": out["fp32c"]["size_orientations_per_s"],
@@ -513,39 +569,39 @@ def run_sizescan(args):
     print(json.dumps(line), flush=True)
 
 
-def run_refgpu(args):
+REFGPU_BINARIES = {
+    "reference_fp64": ("oracle/_ref/mbs_po_gpu_ref_fp64", {}),
+    "reference_fp32": ("oracle/_ref/mbs_po_gpu_ref_fp32", {}),
+    "b200_fp64": ("mbs_fast_b200/_lib/mbs_po_b200", {"MBS_B200_PRECISION": "fp64"}),
+    "b200_fp32c": ("mbs_fast_b200/_lib/mbs_po_b200", {"MBS_B200_PRECISION": "fp32c"}),
+}
+
+
+def reference_gpu_compare(n: int, n_phi: int, n_theta: int, warm: bool = True) -> dict:
     """Same-box GPU comparison at the CLI: the reference's own CUDA build
-    (oracle/_ref/mbs_po_gpu_ref_{fp64,fp32}, its GpuDiffraction.cu for sm_100)
-    against the drop-in binary (the same CLI with this library underneath,
-    FP64 and FP32C), on the D=40 um, L=100 um column with N Sobol orientations
-    and the headline grid.  Diffraction time is the sum of the "GPU timing
-    diffract" lines (MBS_GPU_TIMING=1) of each run: kernels and the whole
-    call (packing, copies, kernels, accumulation), each binary timed on its
-    second run."""
+    (its GpuDiffraction.cu for sm_100, FP64 and FP32) against the drop-in
+    binary (the same CLI with this library underneath, FP64 and FP32C), on
+    the D=40 um, L=100 um column with n Sobol orientations.  Per binary: the
+    sums of the "GPU timing diffract" lines (MBS_GPU_TIMING=1) of one run,
+    kernels and whole calls (packing, copies, kernels, accumulation), and the
+    process wall time; with `warm`, after one untimed run (the first
+    process on a fresh device pays one-off costs)."""
     import re
-    import subprocess
     import tempfile
-    n = args.orient if args.orient != 16384 else 2048
     cli = ["--method", "po", "--particle", "1", "100", "40", "--refractive-index", "1.3116", "1e-9",
            "--wavelength-um", "0.532", "--max-reflections", "4", "--sobol", str(n),
-           "--scattering-grid", "0", "180", str(args.n_phi), str(args.n_theta), "--close",
+           "--scattering-grid", "0", "180", str(n_phi), str(n_theta), "--close",
            "--backend", "gpu"]
-    runs = {"reference_fp64": (os.path.join(ROOT, "oracle", "_ref", "mbs_po_gpu_ref_fp64"), {}),
-            "reference_fp32": (os.path.join(ROOT, "oracle", "_ref", "mbs_po_gpu_ref_fp32"), {}),
-            "b200_fp64": (os.path.join(ROOT, "mbs_fast_b200", "_lib", "mbs_po_b200"),
-                          {"MBS_B200_PRECISION": "fp64"}),
-            "b200_fp32c": (os.path.join(ROOT, "mbs_fast_b200", "_lib", "mbs_po_b200"),
-                           {"MBS_B200_PRECISION": "fp32c"})}
     out = {}
-    for name, (binary, env_extra) in runs.items():
+    for name, (rel, env_extra) in REFGPU_BINARIES.items():
+        binary = os.path.join(ROOT, rel)
         if not os.path.exists(binary):
             out[name] = {"unavailable": "not built"}
             continue
         env = dict(os.environ, MBS_GPU_TIMING="1", **env_extra)
-        # one untimed run first: the first process on a fresh device pays
-        # one-off costs (module loading, first allocations) in its calls
-        subprocess.run([binary] + cli + ["--output", os.path.join(tempfile.mkdtemp(), "w")],
-                       capture_output=True, text=True, env=env, timeout=1800)
+        if warm:
+            subprocess.run([binary] + cli + ["--output", os.path.join(tempfile.mkdtemp(), "w")],
+                           capture_output=True, text=True, env=env, timeout=1800)
         d = tempfile.mkdtemp()
         t0 = time.perf_counter()
         r = subprocess.run([binary] + cli + ["--output", os.path.join(d, "o")], capture_output=True,
@@ -556,20 +612,25 @@ def run_refgpu(args):
         kern = sum(float(m) for ln in lines for m in re.findall(r"kernels=([0-9.]+)ms", ln))
         tot = sum(float(m) for ln in lines for m in re.findall(r"total=([0-9.]+)ms", ln))
         out[name] = {"rc": r.returncode, "calls": len(lines), "kernel_ms": kern, "call_ms": tot,
-                     "orientations_per_s_kernel": n / (kern * 1e-3) if kern else None,
-                     "orientations_per_s_call": n / (tot * 1e-3) if tot else None,
                      "process_wall_s": wall}
+    for prec, ref, mine in (("fp64", "reference_fp64", "b200_fp64"), ("fp32", "reference_fp32", "b200_fp32c")):
+        a, b = out.get(ref, {}), out.get(mine, {})
+        if a.get("kernel_ms") and b.get("kernel_ms"):
+            out[prec + "_kernel_speedup"] = a["kernel_ms"] / b["kernel_ms"]
+        if a.get("call_ms") and b.get("call_ms"):
+            out[prec + "_call_speedup"] = a["call_ms"] / b["call_ms"]
+        if a.get("process_wall_s") and b.get("process_wall_s"):
+            out[prec + "_process_speedup"] = a["process_wall_s"] / b["process_wall_s"]
+    return out
+
+
+def run_refgpu(args):
+    """reference_gpu_compare as its own workload (2048 orientations unless
+    --orient is given)."""
+    n = args.orient if args.orient != 16384 else 2048
     line = {"metric": METRIC, "unit": "orientations/s", "impl": "b200-vs-reference-gpu",
             "config": {"workload": WORKLOAD.replace("16384", str(n)), "orientations": n},
-            "runs": out}
-    ref, mine = out.get("reference_fp64", {}), out.get("b200_fp64", {})
-    if ref.get("kernel_ms") and mine.get("kernel_ms"):
-        line["fp64_kernel_speedup_vs_reference"] = ref["kernel_ms"] / mine["kernel_ms"]
-        line["fp64_call_speedup_vs_reference"] = ref["call_ms"] / mine["call_ms"]
-    r32, m32 = out.get("reference_fp32", {}), out.get("b200_fp32c", {})
-    if r32.get("kernel_ms") and m32.get("kernel_ms"):
-        line["fp32_kernel_speedup_vs_reference"] = r32["kernel_ms"] / m32["kernel_ms"]
-        line["fp32_call_speedup_vs_reference"] = r32["call_ms"] / m32["call_ms"]
+            "runs": reference_gpu_compare(n, args.n_phi, args.n_theta)}
     print(json.dumps(line), flush=True)
 
 
@@ -592,8 +653,61 @@ def run_mlp(args):
                       "forward_s": t2 - t1, "loss": loss}), flush=True)
 
 
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one
+# full-size FP32C diffraction launch of the headline workload, from the
+# capture summarised in profiles/po_diffract_kernel_f32_traffic_hexcol40x100_16384orient.md
+# (None until measured for the current kernel).
+FP32C_LAUNCH_DRAM_BYTES = None
+
+
+def nominal_peaks(clock_mhz: float | None) -> dict:
+    """B200 nominal FP32 and FP64 FMA peaks at the given SM clock: 148 SMs x
+    128 FP32 lanes (64 FP64 lanes) x 2 flop."""
+    f = (clock_mhz or 1965.0) * 1e6
+    return {"fp32_tflops": 148 * 128 * 2 * f / 1e12, "fp64_tflops": 148 * 64 * 2 * f / 1e12,
+            "sm_mhz": clock_mhz or 1965.0}
+
+
+def launch_ranks(args) -> int:
+    """--gpus N without a torchrun environment: run this script once per GPU
+    under torch.distributed.run (one process per GPU, rendezvous on
+    127.0.0.1) with the same arguments; rank 0 prints the line."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def run_launch_selftest(args):
+    """Ranks started by launch_ranks check their environment and exchange one
+    all-reduce (gloo on the CPU): the multi-process plumbing of --gpus N
+    without a GPU."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    rank, world, local = dist_env()
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    t = torch.tensor([float(rank + 1)])
+    dist.all_reduce(t)
+    mx = torch.tensor([float(rank)])
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"launch_selftest": True, "world": world, "sum": float(t.item()),
+                          "max_rank": float(mx.item()), "gpus_arg": args.gpus}), flush=True)
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(launch_ranks(args))
+    if args.launch_selftest:
+        run_launch_selftest(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -622,7 +736,7 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    from mbs_fast_b200 import abi
+    from mbs_fast_b200 import abi, metrics
     from mbs_fast_b200.handler import GpuHandlerPO
 
     t0 = time.perf_counter()
@@ -634,13 +748,14 @@ def main():
     acc = torch.zeros(G * 16, dtype=torch.float64, device=f"cuda:{local}")
     stream = torch.cuda.current_stream().cuda_stream
 
-    m11_err = None
     # launch-shape autotuner on a slice of the batch (untimed)
     tuned = {}
     for prec, name in ((abi.FP32C, "fp32c"), (abi.FP64, "fp64")):
         best, ms = h.autotune(staged, prec, max_orient=min(256, batch.n_orient))
         tuned[name] = {"variant": best, "ms_per_variant": [round(m, 3) for m in ms]}
-    fp64_ms = None
+    # plain FP64 batched path: the error reference and the denominator of
+    # the wall-time comparison (one full pass, device-timed)
+    fp64_ms = fp64_kernel_ms = None
     M64 = None
     if not args.no_fp64:
         ref = torch.zeros_like(acc)
@@ -648,7 +763,9 @@ def main():
         h.diffract_staged(staged, ref.data_ptr(), precision=abi.FP64, stream=stream, stats=st)
         torch.cuda.synchronize()
         fp64_ms = st.kernel_ms + st.reduce_ms
+        fp64_kernel_ms = st.kernel_ms
         M64 = ref.cpu().numpy().reshape(grid.n_az, grid.n_zen + 1, 16)
+        del ref
 
     stats = abi.Stats()
     for _ in range(args.warmup):
@@ -671,7 +788,7 @@ def main():
         acc.zero_()
         h.diffract_staged(staged, acc.data_ptr(), precision=abi.FP32C, stream=stream, stats=stats)
         kernel_ms.append(stats.kernel_ms)
-        launches += stats.launches + 1      # diffraction + reduce, + the accumulator clear
+        launches += stats.launches + 1      # diffraction + reduce (+ pole rows), + the accumulator clear
     ev1.record()
     torch.cuda.synchronize()
     step_ms = ev0.elapsed_time(ev1) / args.steps
@@ -682,7 +799,7 @@ def main():
         step_ms = float(t.item())
     M32 = acc.cpu().numpy().reshape(grid.n_az, grid.n_zen + 1, 16)
 
-    # ---- timed region: end-to-end through the public C ABI ----
+    # ---- timed region: end-to-end through the public C ABI, every step ----
     pinned = pin_batch(batch)
     Mh = np.zeros((grid.n_az, grid.n_zen + 1, 16))
     h.handle_orientations_to_local_gpu(pinned, Mh, precision=abi.FP32C)   # warm
@@ -690,7 +807,7 @@ def main():
     if world > 1:
         torch.distributed.barrier()
     e2e_t = []
-    for _ in range(max(1, min(args.steps, 3))):
+    for _ in range(args.steps):
         Mh[:] = 0.0
         t1 = time.perf_counter()
         h.handle_orientations_to_local_gpu(pinned, Mh, precision=abi.FP32C)
@@ -715,19 +832,33 @@ def main():
                         batch=1024)
     _, _, tp = orientation_average(h, cfg, beta_o, gamma_o, w_o, precision=abi.FP32C, batch=1024)
 
-    # ---- error vs FP64 on the same orientations ----
-    if M64 is not None:
-        from tests import common
-        errs = common.element_errors(M32, M64, grid)
-        errs["weighted_L2_all16"] = common.weighted_l2(M32, M64, grid)
-        m11_err = errs
+    # ---- error of FP32C against the plain FP64 path on the same orientations ----
+    m11_err = metrics.compare(h, M32, M64) if M64 is not None else None
 
     flops = algorithmic_flops(batch, G)
     kern_s = float(np.mean(kernel_ms)) * 1e-3
     peak = h.probe_fp32_peak()
+    peak64 = h.probe_fp64_peak()
+    nom = nominal_peaks(clocks.get("sm_mhz"))
     achieved = flops / kern_s / 1e12
     total_orient = batch.n_orient * world
     value = total_orient / (step_ms * 1e-3)
+    traffic = FP32C_LAUNCH_DRAM_BYTES
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None,
+                "traffic": traffic,
+                "traffic_unit": "bytes per launch (ncu DRAM read + write)",
+                "algorithmic_bytes": int(batch.n_beams * 432 + batch.n_verts * 48 + G * 16 * 8),
+                "peak_source": "measured FFMA probe of this device (MEASURED_PEAKS.json has no FP32 entry)",
+                "nominal_peak": nom["fp32_tflops"], "frac_of_nominal": achieved / nom["fp32_tflops"],
+                "work": "12*nv+168 flop per beam-direction + 100 per orientation-direction"}
+    if fp64_kernel_ms:
+        a64 = flops / (fp64_kernel_ms * 1e-3) / 1e12
+        roofline["fp64"] = {"kernel": "po_diffract_kernel<double> (plain FP64 path)", "achieved": a64,
+                            "peak": peak64, "frac": a64 / peak64 if peak64 else None,
+                            "nominal_peak": nom["fp64_tflops"],
+                            "frac_of_nominal": a64 / nom["fp64_tflops"],
+                            "peak_source": "measured DFMA probe of this device"}
     line = {
         "metric": METRIC, "value": value, "unit": "orientations/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
@@ -742,8 +873,10 @@ def main():
         "m11_error_vs_fp64": m11_err,
         "fp64_ms_per_step": fp64_ms,
         "fp64_orientations_per_s": (batch.n_orient / (fp64_ms * 1e-3)) if fp64_ms else None,
+        "fp32c_speedup_vs_fp64": (fp64_ms / step_ms) if fp64_ms else None,
         "e2e": {"value": total_orient / e2e_s, "unit": "orientations/s",
-                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes},
+                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
+                "timed_calls": len(e2e_t)},
         "e2e_with_tracing": {"value": batch.n_orient / tp["wall_s"], "unit": "orientations/s",
                              "wall_s": tp["wall_s"], "host_trace_s": tp["trace_s"],
                              "what": "reference tracer and restated PrepareBeams on all host "
@@ -751,16 +884,17 @@ def main():
                                      "overlapped with FP32C diffraction on the device"},
         "gpu_launches": launches,
         "autotune": tuned,
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
-                     "peak_source": "measured FFMA probe (MEASURED_PEAKS.json has no FP32 entry)",
-                     "work": "12*nv+168 flop per beam-direction + 100 per orientation-direction"},
+        "roofline": roofline,
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(cfg, batch, args)
+        base, M_ref, cext_ref, sample = reference_sample(cfg, batch, args)
+        line["cpu_baseline"] = base
+        line["parity_vs_reference"] = parity_vs_reference(h, sample, M_ref, cext_ref)
     staged.free()
     h.close()
+    if rank == 0 and not args.no_refgpu:
+        line["reference_gpu"] = reference_gpu_compare(args.refgpu_orient, args.n_phi, args.n_theta)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:

@@ -38,6 +38,17 @@ int mbs_mlp_create(mbs_mlp **out, int device, uint64_t seed);
 int mbs_mlp_destroy(mbs_mlp *net);
 const char *mbs_mlp_last_error(const mbs_mlp *net);
 
+/* Watchdog of the tensor-core GEMMs (no counterpart in the reference).
+ * Every GEMM waits on its MMA-completion barrier for at most `poll_limit`
+ * polls (<= 0: the default 2^22); when the wait runs out the kernel sets the
+ * network's device error flag, waits (bounded) for any MMA in flight, frees
+ * its tensor memory and returns without storing, and the call fails with
+ * "tensor-core barrier wait timed out" (mbs_mlp_last_error); the network
+ * stays usable.  skip_mma != 0 is the test hook that exercises this path:
+ * the GEMMs then issue no MMA and no commit, so the barrier never completes
+ * and no asynchronous operation is pending when the wait gives up. */
+int mbs_mlp_set_watchdog(mbs_mlp *net, int poll_limit, int skip_mma);
+
 /* FP32 master parameters, flat order above (host arrays of
  * MBS_MLP_N_PARAMS floats).  set_params also refreshes the BF16 copies and
  * clears the Adam state. */

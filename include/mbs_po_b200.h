@@ -304,8 +304,19 @@ int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams,
  *     Mns_accum_dev) exceeds the array are rejected with MBS_PO_ERANGE; when
  *     the array holds fewer orientation chunks than the default plan uses,
  *     the call runs fewer, larger chunks.
+ *   - Throughput: the default plan uses up to 64 orientation chunks (about
+ *     32 work items per resident CTA); when fewer chunk planes fit in the
+ *     array the call runs fewer, larger chunks and fewer work items.  On the
+ *     48 x 1801 grid (11 MB per plane) one chunk fits with no-shadow sums
+ *     (240 work items for about 444 resident CTAs: under half the device
+ *     busy) and three without.  Grids get the full 64 chunks only up to
+ *     4,096 directions (2,048 with no-shadow sums); the largest grid
+ *     accepted has 262,142 directions (131,071 with no-shadow sums).
  *   - The first call on a device resolves the array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *     (cudaGetSymbolAddress) and keeps it for the life of the process; make
+ *     that first call before any stream capture.  cudaDeviceReset (or
+ *     anything else that destroys the device's primary context) invalidates
+ *     the kept address: do not call this entry point after it.
  *   - Every call shares the array and overwrites what the last call left;
  *     calls that overlap on the GPU (other streams, other host threads, other
  *     contexts on the same device) race on it and must be serialised. */
@@ -329,6 +340,10 @@ int mbs_po_set_variant(mbs_po_ctx *ctx, int precision, int variant);
  * FFMA chains on every SM), the denominator of the diffraction kernels'
  * roofline fraction.  No counterpart in the reference. */
 int mbs_po_probe_fp32_peak(mbs_po_ctx *ctx, double *tflops);
+/* Measured FP64 FMA throughput in TFLOP/s (independent DFMA chains), the
+ * denominator of the FP64 diffraction kernel's roofline fraction.  No
+ * counterpart in the reference. */
+int mbs_po_probe_fp64_peak(mbs_po_ctx *ctx, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -99,10 +99,13 @@ __device__ __forceinline__ uint32_t kmajor_off(int row, int k, int kt)
     return (uint32_t)((row >> 3) * (kt * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-// Bounded wait on an mbarrier phase; false when it did not complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase)
+// Bounded wait on an mbarrier phase (at most `limit` polls); false when it
+// did not complete.
+constexpr int kDefaultPollLimit = 1 << 22;
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, int limit)
 {
-    for (int it = 0; it < (1 << 22); ++it) {
+    for (int it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred P1;\n\t"
                      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -169,8 +172,17 @@ __device__ __forceinline__ void stage_operand(unsigned char *dst, const bf16 *p,
 
 constexpr int kGemmThreads = 256;   // 8 warps: all stage, two warpgroups read TMEM
 
+// Watchdog of the tensor-core barrier waits: the device error flag, the
+// poll limit, and (test hook) whether to leave out the MMAs and their
+// commit, so that the wait runs out with no asynchronous operation pending.
+struct Watch {
+    int *err;
+    int poll_limit;
+    int skip_mma;
+};
+
 template <int MODE>
-__global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, Mat A, Mat B, GemmOut o, int *err)
+__global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, Mat A, Mat B, GemmOut o, Watch w)
 {
     extern __shared__ __align__(1024) unsigned char gsm[];
     bf16 *sA = reinterpret_cast<bf16 *>(gsm);
@@ -203,7 +215,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, Mat 
         stage_operand(reinterpret_cast<unsigned char *>(sB), B.p, B.sc, B.sr, n0, nt, n0 + nt, k0, kt);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && !w.skip_mma) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB), sbo = (uint32_t)kt * 16;
             for (int s = 0; s < kt / 16; ++s) {
@@ -219,15 +231,15 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm(int M, int N, int K, Mat 
                          :: "r"(smem_u32(bar)) : "memory");
         }
         // the tiles may be overwritten once the MMAs that read them are done
-        ok = mbar_wait(smem_u32(bar), phase);
+        ok = mbar_wait(smem_u32(bar), phase, w.poll_limit);
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;");
         __syncthreads();
     }
     if (!ok) {
         if (threadIdx.x == 0)
-            atomicExch(err, 1);
-        mbar_wait(smem_u32(bar), phase ^ 1u);   // let any MMA in flight finish, bounded
+            atomicExch(w.err, 1);
+        mbar_wait(smem_u32(bar), phase ^ 1u, w.poll_limit);   // let any MMA in flight finish, bounded
     } else {
         // warp w reads TMEM lanes 32 (w % 4) .. + 31 (its lane quarter); the
         // two warpgroups take alternate 16-column chunks
@@ -447,6 +459,8 @@ struct mbs_mlp {
     float *z1 = nullptr, *z2 = nullptr, *z3 = nullptr;
     float *y = nullptr, *t = nullptr, *dy = nullptr, *q = nullptr;
     float *gw1p = nullptr, *scalar = nullptr;
+    int poll_limit = kDefaultPollLimit;   // mbs_mlp_set_watchdog
+    int skip_mma = 0;
 };
 
 namespace {
@@ -507,6 +521,8 @@ dim3 tiles(int M, int N) { return dim3((N + kTileN - 1) / kTileN, (M + kTile - 1
 // third int of the network's scalar scratch).
 int *mlp_err(mbs_mlp *net) { return reinterpret_cast<int *>(net->scalar) + 2; }
 
+Watch watch(mbs_mlp *net) { return Watch{mlp_err(net), net->poll_limit, net->skip_mma}; }
+
 // Reset before a call's kernels, checked after its final synchronisation.
 int check_err(mbs_mlp *net)
 {
@@ -520,14 +536,14 @@ int check_err(mbs_mlp *net)
 }
 
 template <int MODE>
-void gemm(cudaStream_t s, int M, int N, int K, Mat A, Mat B, GemmOut o, int *err)
+void gemm(cudaStream_t s, int M, int N, int K, Mat A, Mat B, GemmOut o, Watch w)
 {
     static bool attr = false;   // the dynamic shared-memory limit, once per instantiation
     if (!attr) {
         cudaFuncSetAttribute(k_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
         attr = true;
     }
-    k_gemm<MODE><<<tiles(M, N), kGemmThreads, kGemmSmem, s>>>(M, N, K, A, B, o, err);
+    k_gemm<MODE><<<tiles(M, N), kGemmThreads, kGemmSmem, s>>>(M, N, K, A, B, o, w);
 }
 
 // Forward pass of n samples already in net->q (device); train keeps the
@@ -541,13 +557,13 @@ int forward_dev(mbs_mlp *net, int n)
     o.ldo = kH;
     o.bias = net->params + ob1; o.z = net->z1; o.h = net->h1;
     gemm<kModeFwd>(s, bp, kH, kInPad, Mat{net->x0, kInPad, 1},
-                   Mat{net->w1p, 1, kInPad}, o, mlp_err(net));
+                   Mat{net->w1p, 1, kInPad}, o, watch(net));
     o.bias = net->params + ob2; o.z = net->z2; o.h = net->h2;
     gemm<kModeFwd>(s, bp, kH, kH, Mat{net->h1, kH, 1},
-                   Mat{net->w2, 1, kH}, o, mlp_err(net));
+                   Mat{net->w2, 1, kH}, o, watch(net));
     o.bias = net->params + ob3; o.z = net->z3; o.h = net->h3;
     gemm<kModeFwd>(s, bp, kH, kH, Mat{net->h2, kH, 1},
-                   Mat{net->w3, 1, kH}, o, mlp_err(net));
+                   Mat{net->w3, 1, kH}, o, watch(net));
     k_head_fwd<<<(n + 7) / 8, 256, 0, s>>>(net->h3, net->params, n, net->y);
     MK(cudaGetLastError(), "mlp forward launch");
     return 0;
@@ -565,23 +581,23 @@ int backward_dev(mbs_mlp *net, int n)
     // layer 3: dW3 = dZ3^T H2, db3 = colsum dZ3, dZ2 = (dZ3 W3) * gelu'(Z2)
     o.ldo = kH; o.f = net->grad + oW3;
     gemm<kModeF32>(s, kH, kH, bp, Mat{net->dz3, 1, kH},
-                   Mat{net->h2, kH, 1}, o, mlp_err(net));
+                   Mat{net->h2, kH, 1}, o, watch(net));
     k_colsum_bf16<<<(kH + 31) / 32, 256, 0, s>>>(net->dz3, bp, kH, net->grad + ob3);
     o = GemmOut{}; o.ldo = kH; o.zin = net->z2; o.h = net->dz2;
     gemm<kModeBwd>(s, bp, kH, kH, Mat{net->dz3, kH, 1},
-                   Mat{net->w3, kH, 1}, o, mlp_err(net));
+                   Mat{net->w3, kH, 1}, o, watch(net));
     // layer 2
     o = GemmOut{}; o.ldo = kH; o.f = net->grad + oW2;
     gemm<kModeF32>(s, kH, kH, bp, Mat{net->dz2, 1, kH},
-                   Mat{net->h1, kH, 1}, o, mlp_err(net));
+                   Mat{net->h1, kH, 1}, o, watch(net));
     k_colsum_bf16<<<(kH + 31) / 32, 256, 0, s>>>(net->dz2, bp, kH, net->grad + ob2);
     o = GemmOut{}; o.ldo = kH; o.zin = net->z1; o.h = net->dz1;
     gemm<kModeBwd>(s, bp, kH, kH, Mat{net->dz2, kH, 1},
-                   Mat{net->w2, kH, 1}, o, mlp_err(net));
+                   Mat{net->w2, kH, 1}, o, watch(net));
     // layer 1
     o = GemmOut{}; o.ldo = kInPad; o.f = net->gw1p;
     gemm<kModeF32>(s, kH, kInPad, bp, Mat{net->dz1, 1, kH},
-                   Mat{net->x0, kInPad, 1}, o, mlp_err(net));
+                   Mat{net->x0, kInPad, 1}, o, watch(net));
     k_pack_w1_grad<<<(kH * kIn + 127) / 128, 128, 0, s>>>(net->gw1p, net->grad);
     k_colsum_bf16<<<(kH + 31) / 32, 256, 0, s>>>(net->dz1, bp, kH, net->grad + ob1);
     MK(cudaGetLastError(), "mlp backward launch");
@@ -648,6 +664,15 @@ extern "C" int mbs_mlp_destroy(mbs_mlp *net)
     if (net->stream)
         cudaStreamDestroy(net->stream);
     delete net;
+    return 0;
+}
+
+extern "C" int mbs_mlp_set_watchdog(mbs_mlp *net, int poll_limit, int skip_mma)
+{
+    if (!net)
+        return -1;
+    net->poll_limit = poll_limit > 0 ? poll_limit : kDefaultPollLimit;
+    net->skip_mma = skip_mma ? 1 : 0;
     return 0;
 }
 

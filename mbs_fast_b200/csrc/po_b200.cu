@@ -83,6 +83,12 @@ struct mbs_po_staged {
 
 struct mbs_po_ctx {
     int device = 0;
+    // stream-ordered allocations of the growing scratch (partials, upload
+    // area, re-filled staged batches) come from this context's own pool,
+    // which keeps freed blocks (release threshold: never) instead of
+    // returning them to the driver at every synchronisation: a growth step
+    // then re-uses pool memory instead of mapping new pages
+    cudaMemPool_t pool = nullptr;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;          // polar-row kernel, concurrent
     std::string err;
@@ -184,7 +190,7 @@ int grow_partial(mbs_po_ctx *ctx, size_t n, cudaStream_t st)
     ctx->partial = nullptr;
     const size_t want = std::max<size_t>(n, 2 * ctx->partial_cap);
     ctx->partial_cap = 0;
-    e = cudaMallocAsync((void **)&ctx->partial, want * sizeof(double), st);
+    e = cudaMallocFromPoolAsync((void **)&ctx->partial, want * sizeof(double), ctx->pool, st);
     if (e != cudaSuccess) {
         ctx->partial = nullptr;
         return fail(ctx, MBS_PO_ENOMEM, std::string("cudaMallocAsync partials: ") + cudaGetErrorString(e));
@@ -215,7 +221,7 @@ int grow_arena(mbs_po_ctx *ctx, Arena &a, size_t bytes, const char *what, cudaSt
     const size_t want = std::max<size_t>({(size_t)2 * bytes, (size_t)4 * a.cap, (size_t)1 << 20});
     const size_t cap = (want + ((size_t)1 << 21) - 1) & ~(((size_t)1 << 21) - 1);
     a.cap = 0;
-    cudaError_t e = cudaMallocAsync(&a.base, cap, st);
+    cudaError_t e = cudaMallocFromPoolAsync(&a.base, cap, ctx->pool, st);
     if (e != cudaSuccess) {
         a.base = nullptr;
         return fail(ctx, MBS_PO_ENOMEM, std::string("cudaMallocAsync ") + what + ": " + cudaGetErrorString(e));
@@ -291,7 +297,20 @@ extern "C" int mbs_po_create(mbs_po_ctx **out, int device)
         e = cudaEventCreateWithFlags(&ctx->partial_done, cudaEventDisableTiming);
     if (e == cudaSuccess)
         e = cudaMalloc((void **)&ctx->d_status, 64);
+    if (e == cudaSuccess) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        e = cudaMemPoolCreate(&ctx->pool, &props);
+        uint64_t keep = ~(uint64_t)0;
+        if (e == cudaSuccess)
+            e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (e != cudaSuccess) {
+        if (ctx->pool)
+            cudaMemPoolDestroy(ctx->pool);
         delete ctx;
         return MBS_PO_ECUDA;
     }
@@ -325,6 +344,10 @@ extern "C" int mbs_po_destroy(mbs_po_ctx *ctx)
         cudaStreamDestroy(ctx->stream);
     if (ctx->side)
         cudaStreamDestroy(ctx->side);
+    // staged batches the caller still holds keep their blocks; the pool's
+    // resources go once the last of them is freed
+    if (ctx->pool)
+        cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return MBS_PO_OK;
 }
@@ -1411,20 +1434,26 @@ extern "C" int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams, i
     return MBS_PO_OK;
 }
 
-extern "C" int mbs_po_probe_fp32_peak(mbs_po_ctx *ctx, double *tflops)
+namespace {
+
+// Best of three timed launches (after one warm-up) of a probe kernel of
+// independent FMA chains, 16 x 8 FMAs per thread and iteration.
+template <typename T>
+int probe_peak(mbs_po_ctx *ctx, void (*kern)(T *, int, T, T), double *tflops)
 {
     if (!ctx || !tflops)
         return MBS_PO_EINVAL;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    float *out = nullptr;
-    CK(cudaMalloc((void **)&out, (size_t)sms * 64 * sizeof(float)), "cudaMalloc probe");
-    const int blocks = sms * 8, threads = 256, iters = 4096;
+    T *out = nullptr;
+    const int blocks = sms * 8, threads = 256;
+    const int iters = sizeof(T) == 4 ? 4096 : 2048;
+    CK(cudaMalloc((void **)&out, (size_t)blocks * sizeof(T)), "cudaMalloc probe");
     double best = 0.0;
     for (int rep = 0; rep < 4; ++rep) {
         cudaEventRecord(ctx->ev[0], ctx->stream);
-        po_fp32_probe_kernel<<<blocks, threads, 0, ctx->stream>>>(out, iters, 0.999999f, 1e-6f);
+        kern<<<blocks, threads, 0, ctx->stream>>>(out, iters, (T)0.999999, (T)1e-6);
         cudaEventRecord(ctx->ev[1], ctx->stream);
         cudaError_t e = cudaEventSynchronize(ctx->ev[1]);
         if (e != cudaSuccess) {
@@ -1440,6 +1469,18 @@ extern "C" int mbs_po_probe_fp32_peak(mbs_po_ctx *ctx, double *tflops)
     cudaFree(out);
     *tflops = best;
     return MBS_PO_OK;
+}
+
+}  // namespace
+
+extern "C" int mbs_po_probe_fp32_peak(mbs_po_ctx *ctx, double *tflops)
+{
+    return probe_peak<float>(ctx, po_fp32_probe_kernel, tflops);
+}
+
+extern "C" int mbs_po_probe_fp64_peak(mbs_po_ctx *ctx, double *tflops)
+{
+    return probe_peak<double>(ctx, po_fp64_probe_kernel, tflops);
 }
 
 // ------------------------------------------------- allocation-free variant --

@@ -206,50 +206,7 @@ __device__ __forceinline__ bool small_phase_factor(const DevVert *v, int nv, dou
     return true;
 }
 
-// ---------------------------------------------------------------- FP32 math
-
-// sin and cos of 2*pi*u, u in turns (FP64).  The FP64 add of 1.5*2^29 to
-// 4u + 1/2 leaves round(4u) mod 4 in mantissa bits 23-24 and the remaining
-// quarter-turn fraction in bits 0-22, so the reduced argument is exact to
-// 2^-23 quarter turns without an FP64->FP32 conversion.
-__device__ __forceinline__ void reduce_quarter(double u, float &x, int &q)
-{
-    const double t = fma(u, 4.0, kMagic29 + 0.5);
-    const unsigned lo = (unsigned)__double2loint(t);
-    q = (int)((lo >> 23) & 3u);
-    x = (__int_as_float(0x3F800000u | (lo & 0x007FFFFFu)) - 1.5f) * 1.57079632679489662f;
-}
-
-// Hardware (MUFU) sine/cosine of the reduced argument |x| <= pi/4.
-__device__ __forceinline__ void sincos_quarter_mufu(float x, int q, float &s, float &c)
-{
-    float sx, cx;
-    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(sx) : "f"(x));
-    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(cx) : "f"(x));
-    const float ss = (q & 1) ? cx : sx;
-    const float cc = (q & 1) ? sx : cx;
-    s = (q & 2) ? -ss : ss;
-    c = ((q + 1) & 2) ? -cc : cc;
-}
-
-// FMA-pipe sine/cosine of |x| <= pi/4: Taylor to x^9 (error < 2e-9) and
-// x^8 (error < 3e-8), coefficients 1/n! rounded to float.
-__device__ __forceinline__ void sincos_quarter_poly(float x, int q, float &s, float &c)
-{
-    const float x2 = x * x;
-    float ps = fmaf(x2, 2.7557319e-06f, -1.9841270e-04f);
-    ps = fmaf(ps, x2, 8.3333333e-03f);
-    ps = fmaf(ps, x2, -1.6666667e-01f);
-    const float sx = fmaf(x * x2, ps, x);
-    float pc = fmaf(x2, 2.4801587e-05f, -1.3888889e-03f);
-    pc = fmaf(pc, x2, 4.1666668e-02f);
-    pc = fmaf(pc, x2, -0.5f);
-    const float cx = fmaf(x2, pc, 1.0f);
-    const float ss = (q & 1) ? cx : sx;
-    const float cc = (q & 1) ? sx : cx;
-    s = (q & 2) ? -ss : ss;
-    c = ((q + 1) & 2) ? -cc : cc;
-}
+// ---------------------------------------------------------- Jones -> Mueller
 
 // Jones -> Mueller times weight, added into out[16] (Mueller.hpp:37-87).
 template <typename T>

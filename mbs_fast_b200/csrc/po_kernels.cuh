@@ -2080,4 +2080,28 @@ __global__ void __launch_bounds__(256) po_fp32_probe_kernel(float *out, int iter
         out[blockIdx.x] = s;
 }
 
+// Independent DFMA chains: this device's FP64 FMA throughput, the
+// denominator of the FP64 diffraction kernel's roofline fraction.
+__global__ void __launch_bounds__(256) po_fp64_probe_kernel(double *out, int iters, double a, double b)
+{
+    double x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        x[i] = threadIdx.x * 1e-3 + i;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                x[i] = fma(x[i], a, b);
+        }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        s += x[i];
+    if (s == 1234.5)
+        out[blockIdx.x] = s;
+}
+
 }  // namespace mbs

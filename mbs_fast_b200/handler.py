@@ -52,6 +52,7 @@ def lib() -> C.CDLL:
         L.mbs_po_select_batch.argtypes = [vp, C.POINTER(abi.Beams), C.c_int, C.c_int, C.c_double,
                                           C.POINTER(C.c_int)]
         L.mbs_po_probe_fp32_peak.argtypes = [vp, abi._dp]
+        L.mbs_po_probe_fp64_peak.argtypes = [vp, abi._dp]
         L.mbs_po_autotune.argtypes = [vp, vp, C.c_int, C.c_int, C.POINTER(C.c_int), abi._dp, C.c_int]
         L.mbs_po_set_variant.argtypes = [vp, C.c_int, C.c_int]
         L.mbs_po_diffract_staged_noalloc.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_void_p,
@@ -332,6 +333,12 @@ class GpuHandlerPO:
         """Measured FP32 FMA throughput of this device, TFLOP/s."""
         v = C.c_double()
         self._call(lib().mbs_po_probe_fp32_peak(self.ctx, C.byref(v)), "mbs_po_probe_fp32_peak")
+        return v.value
+
+    def probe_fp64_peak(self) -> float:
+        """Measured FP64 FMA throughput of this device, TFLOP/s."""
+        v = C.c_double()
+        self._call(lib().mbs_po_probe_fp64_peak(self.ctx, C.byref(v)), "mbs_po_probe_fp64_peak")
         return v.value
 
     def diffract_staged_noalloc(self, staged: Staged, m_dev_ptr: int,

@@ -243,27 +243,31 @@ static bool diffract_range(HandlerPO &h, const ScatteringRange &sphere,
     // the sums stay in the library's page-locked buffer and are added into
     // the Arr2D cells in one pass
     const double *Mv = nullptr, *Mnv = nullptr;
+    const auto t2 = std::chrono::steady_clock::now();
     const int rc = mbs_po_diffract_pinned(c.ctx, &view, precision_from_env(), &Mv,
                                           computeNoShadow ? &Mnv : nullptr, &st);
     if (rc == MBS_PO_EBEAM)
         return false;
     if (!report(rc, "diffraction"))
         return false;
+    const auto t3 = std::chrono::steady_clock::now();
     if (Mv)
         add_plane(Mv, localM, nAz, nZen + 1);
     if (Mnv)
         add_plane(Mnv, localM_noshadow, nAz, nZen + 1);
     if (timing)
     {
-        const double pack = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        const double total = std::chrono::duration<double, std::milli>(
-            std::chrono::steady_clock::now() - t0).count();
+        const auto t4 = std::chrono::steady_clock::now();
+        auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
         std::fprintf(stderr,
                      "GPU timing diffract path=b200-%s orient=%d beams=%lld nAz=%d nZen=%d "
-                     "pack=%.3fms h2d+stage=%.3fms kernels=%.3fms reduce=%.3fms total=%.3fms\n",
+                     "pack=%.3fms h2d+stage=%.3fms kernels=%.3fms reduce=%.3fms total=%.3fms "
+                     "setup=%.3fms call=%.3fms add=%.3fms\n",
                      precision_from_env() == MBS_PO_FP32C ? "fp32c" : "fp64",
-                     view.n_orient, (long long)view.n_beams, nAz, nZen, pack, st.h2d_ms,
-                     st.kernel_ms, st.reduce_ms, total);
+                     view.n_orient, (long long)view.n_beams, nAz, nZen, ms(t0, t1), st.h2d_ms,
+                     st.kernel_ms, st.reduce_ms, ms(t0, t4), ms(t1, t2), ms(t2, t3), ms(t3, t4));
     }
     return true;
 }

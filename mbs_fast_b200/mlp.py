@@ -28,6 +28,7 @@ def lib() -> C.CDLL:
         L.mbs_mlp_loss_grad.argtypes = [vp, _fp, _fp, C.c_int, _fp, _fp]
         L.mbs_mlp_train.argtypes = [vp, _fp, _fp, C.c_int, C.c_int, C.c_int, C.c_float,
                                     C.c_uint64, _fp]
+        L.mbs_mlp_set_watchdog.argtypes = [vp, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -72,6 +73,12 @@ class ProposalNet:
         p = _f32(p)
         assert p.shape == (N_PARAMS,)
         self._call(lib().mbs_mlp_set_params(self.h, abi.ptr(p, C.c_float)), "mbs_mlp_set_params")
+
+    def set_watchdog(self, poll_limit: int = 0, skip_mma: bool = False) -> None:
+        """Poll limit of the GEMMs' barrier waits (0: default); skip_mma is
+        the test hook that makes the waits run out (mbs_mlp_set_watchdog)."""
+        self._call(lib().mbs_mlp_set_watchdog(self.h, poll_limit, int(skip_mma)),
+                   "mbs_mlp_set_watchdog")
 
     def forward(self, q) -> np.ndarray:
         q = _f32(q).reshape(-1, 4)

@@ -75,6 +75,7 @@ def _ref_lib():
         _ref.mbs_ref_fixed.argtypes = [cfgp, C.POINTER(GridSpec), C.c_double, C.c_double,
                                        C.c_double, abi._dp, abi._dp]
         _ref.mbs_ref_jones_kat.argtypes = [C.c_int, abi._dp, abi._dp, abi._dp, abi._dp]
+        _ref.mbs_ref_orientations.argtypes = [cfgp, C.c_int, C.c_uint, abi._dp, abi._dp, abi._dp]
     return _ref
 
 
@@ -164,6 +165,18 @@ def ref_run(cfg: ParticleConfig, gridspec: tuple, beta, gamma, weight, alpha=Non
     if rc != 0:
         raise RuntimeError("mbs_ref_run failed")
     return M, Mns, cext, tt.value, td.value
+
+
+def ref_orientations(cfg: ParticleConfig, n: int, seed: int = 42):
+    """Sobol orientations (beta, gamma, weight) over the particle's symmetry
+    domain from the reference's own code (TraceFromSobolSeed)."""
+    lib = _ref_lib()
+    beta, gamma, w = np.empty(n), np.empty(n), np.empty(n)
+    c = cfg.as_c()
+    if lib.mbs_ref_orientations(C.byref(c), n, seed, abi.ptr(beta, C.c_double),
+                                abi.ptr(gamma, C.c_double), abi.ptr(w, C.c_double)) != 0:
+        raise RuntimeError("mbs_ref_orientations failed")
+    return beta, gamma, w
 
 
 def ref_batch(cfg: ParticleConfig, gridspec: tuple, batch: BeamBatch, n_threads: int = 0):

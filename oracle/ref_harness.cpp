@@ -17,6 +17,11 @@
 //                    (HandlerPO.cpp:1102-1608) for one orientation.
 //   mbs_ref_jones_kat  the reference's Jones->Mueller known-answer check
 //                    (tests/test_mueller_direct.cpp), returning both results.
+//   mbs_ref_orientations  the Owen-scrambled Sobol orientations of
+//                    TracerPOTotal::TraceFromSobolSeed over the particle's
+//                    symmetry domain, from the reference's own Sobol2D and
+//                    particle classes (so the reference arm of the bench needs
+//                    nothing from this repository's producer).
 #include "mbs_po_b200.h"
 
 #include "HandlerPOTotal.h"
@@ -27,6 +32,7 @@
 #include "HexagonalAggregate.h"
 #include "TracerPOTotal.h"
 #include "Mueller.hpp"
+#include "Sobol.h"
 
 #include <chrono>
 #include <cmath>
@@ -255,6 +261,37 @@ int threads_or_all(int n)
 }
 
 }  // namespace
+
+extern "C" int mbs_ref_orientations(const mbs_ref_config *cfg, int n, unsigned seed,
+                                    double *beta, double *gamma, double *weight)
+{
+    if (!cfg || n <= 0 || !beta || !gamma || !weight)
+        return -1;
+    try
+    {
+        const mbs_ref_gridspec gs = {0.0, 180.0, 1, 1, nullptr};
+        RefSetup s(*cfg, gs);
+        const Symmetry &sym = s.particle->GetSymmetry();
+        // TracerPOTotal.cpp:5476-5488: beta = acos(1 - (1 - cos beta_sym) u),
+        // gamma = gamma_sym v, equal weights
+        Sobol2D sobol(seed);
+        std::vector<double> su, sv;
+        sobol.generate(n, su, sv);
+        const double cb = std::cos(sym.beta);
+        for (int i = 0; i < n; ++i)
+        {
+            beta[i] = std::acos(1.0 - (1.0 - cb) * su[i]);
+            gamma[i] = sym.gamma * sv[i];
+            weight[i] = 1.0 / n;
+        }
+        return 0;
+    }
+    catch (const std::exception &e)
+    {
+        std::fprintf(stderr, "mbs_ref_orientations: %s\n", e.what());
+        return -1;
+    }
+}
 
 extern "C" int mbs_ref_run(const mbs_ref_config *cfg, const mbs_ref_gridspec *gs,
                            int n, const double *beta, const double *gamma,

@@ -15,11 +15,13 @@ import functools
 import numpy as np
 
 from mbs_fast_b200 import beams as B
+from mbs_fast_b200 import workloads as W
 
-HEX_COLUMN_40x100 = B.ParticleConfig(particle_type=1, p=(100.0, 40.0), ri_re=1.3116, ri_im=1e-9,
-                                     wavelength=0.532, max_reflections=4)
-HEX_COLUMN_10x20 = B.ParticleConfig(particle_type=1, p=(20.0, 10.0), ri_re=1.3116, ri_im=0.0,
-                                    wavelength=0.532, max_reflections=4)
+from mbs_fast_b200.workloads import PLATE_D10, aggregate_config, size_scan_diameters, \
+    size_scan_theta_deg  # noqa: F401  (shared with bench.py)
+
+HEX_COLUMN_40x100 = W.COLUMN_40x100
+HEX_COLUMN_10x20 = W.COLUMN_10x20
 CONCAVE_ABSORBING = B.ParticleConfig(particle_type=10, p=(1.0, 0.7, 43.4114540493), ri_re=1.3116,
                                      ri_im=0.01, absorption=True, wavelength=0.532,
                                      max_reflections=4, cutoff_off=True)
@@ -37,25 +39,9 @@ def sobol_batch(cfg_key: str, n: int, seed: int = 42) -> B.BeamBatch:
 HEX_COLUMN_ABSORBING_10x20 = B.ParticleConfig(particle_type=1, p=(20.0, 10.0), ri_re=1.3116,
                                               ri_im=0.002, absorption=True, wavelength=0.532,
                                               max_reflections=4)
-# Size-scan plate family: length 0.2 x diameter, traced at D = 10 um and
-# scaled (--particle 1 L D).
-PLATE_D10 = B.ParticleConfig(particle_type=1, p=(2.0, 10.0), ri_re=1.3116, ri_im=0.0,
-                             wavelength=0.532, max_reflections=4)
-
 CASES = {"hex40x100": HEX_COLUMN_40x100, "hex10x20": HEX_COLUMN_10x20,
          "concave": CONCAVE_ABSORBING, "hexabs10x20": HEX_COLUMN_ABSORBING_10x20,
          "plate10": PLATE_D10}
-
-
-def size_scan_diameters(n: int = 16, d_min: float = 10.0, d_max: float = 200.0) -> np.ndarray:
-    """Size scan: plate diameters log-spaced from d_min to d_max (um)."""
-    return np.geomspace(d_min, d_max, n)
-
-
-def size_scan_theta_deg() -> np.ndarray:
-    """Size-scan zenith grid: 0.05 deg steps over 0-10 deg (201 rows), then
-    0.5 deg steps over 10.5-180 deg (340 rows)."""
-    return np.concatenate([np.arange(201) * 0.05, 10.5 + np.arange(340) * 0.5])
 
 
 def single_beam_orientations(batch: B.BeamBatch) -> B.BeamBatch:
@@ -98,13 +84,3 @@ def element_errors(M: np.ndarray, Mref: np.ndarray, grid: B.GridTables) -> dict:
         out[name + "/M11_max_abs"] = float(np.max(np.abs(r[:, idx] / r[:, 0] - q[:, idx] / q[:, 0])))
     return out
 
-
-def aggregate_config(path: str, max_reflections: int = 6, profile: str = "fast"):
-    """Non-convex aggregate of 8 hexagonal columns (D=20 um, L=60 um,
-    seed-drawn orientations, touching, written as a reference particle file
-    at `path`), m=1.3116, 6 reflections, cutoff profile `profile`."""
-    from mbs_fast_b200 import particles as PT
-    PT.write_particle_file(path, PT.column_aggregate())
-    return B.ParticleConfig(particle_type=0, particle_file=path, ri_re=1.3116, ri_im=0.0,
-                            wavelength=0.532, max_reflections=max_reflections,
-                            cutoff_profile=profile)

@@ -53,7 +53,24 @@ def test_dropin_matches_reference_cli(tmp_path):
     f32, f32_i, log32 = _run(DROPIN, "gpu", str(tmp_path / "f32"),
                              {"MBS_GPU_TIMING": "1", "MBS_B200_PRECISION": "fp32c"})
     assert "path=b200-fp32c" in log32
-    assert _wl2(f32, ref) < 2e-4
+    assert _wl2(f32, ref) < 2e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFGPU)),
+                    reason="drop-in or the reference's CUDA build not built")
+def test_dropin_matches_reference_cuda_build(tmp_path):
+    """Direct mode (no --fft): the reference's own CUDA FP64 build and the
+    drop-in on the same command line and device, .dat rows and integrals."""
+    ref, ref_i, ref_log = _run(REFGPU, "gpu", str(tmp_path / "ref"))
+    assert "Phase 2 (diffraction, CUDA)" in ref_log
+    gpu, gpu_i, log = _run(DROPIN, "gpu", str(tmp_path / "gpu"), {"MBS_GPU_TIMING": "1"})
+    assert "path=b200-fp64" in log
+    assert gpu.shape == ref.shape
+    np.testing.assert_array_equal(gpu[:, :2], ref[:, :2])
+    assert _wl2(gpu, ref) < 1e-7
+    for k in ("Cext", "Csca"):
+        assert abs(float(gpu_i[k]) / float(ref_i[k]) - 1) < 1e-7, k
 
 
 @pytest.mark.gpu

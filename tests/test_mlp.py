@@ -91,3 +91,25 @@ def test_gpu_training_reduces_loss_and_is_repeatable():
         net.close()
     assert losses[0][1] < 0.05 * losses[0][0]
     np.testing.assert_array_equal(outs[0], outs[1])
+
+
+@pytest.mark.gpu
+def test_gemm_barrier_watchdog_reports_and_recovers():
+    """The tensor-core GEMMs' bounded barrier wait: with the test hook the
+    MMAs and their commit are left out, so the barrier never completes and
+    the wait runs out after a short poll limit.  The call must fail with the
+    timeout error instead of returning output, and the network must stay
+    usable afterwards (its tensor memory freed, the flag cleared): the next
+    normal call returns bitwise the result of the call before."""
+    from mbs_fast_b200.mlp import ProposalNet
+    net = ProposalNet(seed=3)
+    q, _ = _data(300)
+    y0 = net.forward(q)
+    net.set_watchdog(poll_limit=64, skip_mma=True)
+    with pytest.raises(RuntimeError, match="timed out"):
+        net.forward(q)
+    with pytest.raises(RuntimeError, match="timed out"):
+        net.loss_grad(q, np.zeros(len(q), np.float32))
+    net.set_watchdog(0, False)
+    np.testing.assert_array_equal(net.forward(q), y0)
+    net.close()

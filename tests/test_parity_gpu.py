@@ -16,7 +16,8 @@ pytestmark = pytest.mark.gpu
 # path on the same inputs.
 FP64_WL2 = 1e-8          # against the oracle (both evaluate sin/cos to < 1 ulp)
 FP64_REF_WL2 = 1e-7      # against the reference (its own AVX sin/cos polynomial)
-FP32C_WL2 = 2e-4
+FP32C_WL2 = 2e-5         # about 10x what FP32C reaches on these cases
+FP32C_M11_MAX_REL = 2e-3
 
 
 @pytest.fixture(scope="module")
@@ -62,7 +63,62 @@ def test_fp32c_against_fp64(hex_case):
     err = common.element_errors(M32, M64, grid)
     print("FP32C vs FP64 weighted L2", wl2, err)
     assert wl2 < FP32C_WL2
-    assert err["M11_max_rel"] < 1e-2
+    assert err["M11_max_rel"] < FP32C_M11_MAX_REL
+
+
+@pytest.fixture(scope="module")
+def headline_case():
+    """The headline configuration's particle and grid at full size: column
+    D = 40 um, L = 100 um, m = 1.3116 + 1e-9 i, 4 reflections, 64 Sobol
+    orientations, zenith 0-180 deg in 0.1 deg steps x 48 azimuth bins
+    (86,448 directions), with the reference's own CPU result of the same
+    beams."""
+    if not oracle.have_reference():
+        pytest.skip("reference library not built")
+    cfg = common.HEX_COLUMN_40x100
+    batch = common.sobol_batch("hex40x100", 64)
+    spec = (0.0, 180.0, 48, 1800)
+    grid = B.grid(*spec)
+    M_ref, Mns_ref, cext_ref, _ = oracle.ref_batch(cfg, spec, batch)
+    h = GpuHandlerPO(grid, B.wave(cfg), device=0)
+    yield batch, grid, h, M_ref, Mns_ref, cext_ref
+    h.close()
+
+
+def test_headline_grid_fp64_against_reference(headline_case):
+    """FP64 on the headline grid against the reference's CPU double path:
+    the reference's release-gate metric (weighted L2 of the azimuth-averaged
+    rows) at rounding level, pointwise agreement relative to the forward
+    peak, C_ext from the device extinction kernel."""
+    batch, grid, h, M_ref, Mns_ref, cext_ref = headline_case
+    M, Mns = h.new_mueller(), h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M, Mns, precision=abi.FP64)
+    wl2 = common.weighted_l2(M, M_ref, grid)
+    err = common.element_errors(M, M_ref, grid)
+    print("FP64 vs reference, headline grid: weighted L2", wl2, err)
+    assert wl2 < FP64_REF_WL2
+    assert common.weighted_l2(Mns, Mns_ref, grid) < FP64_REF_WL2
+    assert np.max(np.abs(M - M_ref)) < 1e-8 * np.max(np.abs(M_ref[..., 0]))
+    assert err["M11_max_rel"] < 1e-7
+    cext = h.extinction(batch)
+    np.testing.assert_allclose(cext, cext_ref, rtol=1e-9)
+
+
+def test_headline_grid_fp32c_against_reference(headline_case):
+    """FP32C on the headline grid against the reference's CPU double path
+    (the reference's own FP32 CUDA build reports 3.5e-6 weighted L2,
+    docs/releases/v1.0.0.md:30)."""
+    batch, grid, h, M_ref, _, _ = headline_case
+    M = h.new_mueller()
+    assert h.handle_orientations_to_local_gpu(batch, M, precision=abi.FP32C)
+    wl2 = common.weighted_l2(M, M_ref, grid)
+    err = common.element_errors(M, M_ref, grid)
+    print("FP32C vs reference, headline grid: weighted L2", wl2, err)
+    assert wl2 < FP32C_WL2
+    assert err["M11_max_rel"] < FP32C_M11_MAX_REL
+    for k in ("M12/M11_max_abs", "M22/M11_max_abs", "M33/M11_max_abs", "M34/M11_max_abs",
+              "M44/M11_max_abs"):
+        assert err[k] < 1e-3, k
 
 
 def test_accumulates_not_overwrites(hex_case):

@@ -75,3 +75,40 @@ def test_noalloc_accumulates_and_rejects_oversized_grids():
         hb.diffract_staged_noalloc(sb, out.data_ptr(), precision=abi.FP32C)
     sb.free()
     hb.close()
+
+
+def test_noalloc_allocates_nothing_on_a_fresh_handler():
+    """On a handler whose first diffraction is the allocation-free call (no
+    allocating call before it, so the context holds no partial planes), the
+    call leaves the device's free memory unchanged; its result equals the
+    allocating path's afterwards."""
+    import torch
+    cfg = common.HEX_COLUMN_40x100
+    batch = common.sobol_batch("hex40x100", 8)
+    grid = B.grid(0.0, 180.0, 16, 180)
+    # load the library's module (and its fixed array) on this device first
+    warm = GpuHandlerPO(grid, B.wave(cfg))
+    ws = warm.stage(batch.select(0, 1))
+    wacc = torch.zeros(grid.n_dirs * 16, dtype=torch.float64, device="cuda:0")
+    warm.diffract_staged_noalloc(ws, wacc.data_ptr(), precision=abi.FP64)
+    torch.cuda.synchronize()
+    ws.free()
+    warm.close()
+    h = GpuHandlerPO(grid, B.wave(cfg))
+    staged = h.stage(batch)
+    out = torch.zeros(grid.n_dirs * 16, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for precision in (abi.FP64, abi.FP32C):
+        out.zero_()
+        h.diffract_staged_noalloc(staged, out.data_ptr(), precision=precision)
+        torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    ref = torch.zeros_like(out)
+    h.diffract_staged(staged, ref.data_ptr(), precision=abi.FP32C)
+    torch.cuda.synchronize()
+    got, want = out.cpu().numpy(), ref.cpu().numpy()
+    assert np.sqrt(np.sum((got - want) ** 2) / np.sum(want ** 2)) < 1e-12
+    staged.free()
+    h.close()
