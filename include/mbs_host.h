@@ -43,6 +43,10 @@ typedef struct mbs_host_config {
                                     0: the producer's restatement of it (same
                                     result bit for bit, edge tolerance and
                                     facet tracks computed once)               */
+    double      trace_cutoff_importance; /* --trace-cutoff-importance (> 0:
+                                    overrides the profile's, main.cpp:228-229) */
+    double      beam_cutoff_importance;  /* --beam-cutoff-importance (> 0:
+                                    overrides the profile's, main.cpp:152-153) */
 } mbs_host_config;
 
 typedef struct mbs_host_batch mbs_host_batch;

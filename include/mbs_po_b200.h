@@ -188,6 +188,18 @@ int mbs_po_staged_free(mbs_po_ctx *ctx, mbs_po_staged *staged);
  * No counterpart in the reference, which uploads every batch anew
  * (GpuDiffraction.cu:4159-4778). */
 int mbs_po_restage(mbs_po_ctx *ctx, const mbs_po_beams *beams, mbs_po_staged *staged);
+/* A staged batch of n orientations that shares the device records of
+ * `src`: orientation i is src's orientation orient_index[i] with weight
+ * weight[i] (host arrays); only the orientation table is new.  Orientations
+ * may repeat (an orientation set evaluated several times, or re-weighted,
+ * without tracing or staging it again).  `src` must outlive the result and
+ * not be re-filled while it is in use.  Consecutive entries that do not
+ * continue each other's beam range are joined by a weight-0 orientation over
+ * the beams between them: empty for a repeat or a backward jump; a forward
+ * jump costs the skipped beams' work.  No counterpart in the reference. */
+int mbs_po_stage_repeat(mbs_po_ctx *ctx, const mbs_po_staged *src, int n,
+                        const int32_t *orient_index, const double *weight,
+                        mbs_po_staged **out);
 int mbs_po_diffract_staged(mbs_po_ctx *ctx, const mbs_po_staged *staged,
                            int precision, double *M_accum_dev,
                            double *Mns_accum_dev, void *stream,
@@ -288,6 +300,42 @@ int mbs_po_extinction(mbs_po_ctx *ctx, const mbs_po_beams *beams,
 int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams,
                         int start, int max_count, double mem_fraction,
                         int *count_out);
+
+/* mbs_po_diffract_pinned for a batch staged earlier (mbs_po_stage /
+ * mbs_po_restage, one output set): nothing is uploaded.  Serves the
+ * drop-in's packed-beam cache (HandleOrientationsToLocalGpuOnDevice with a
+ * cacheToken, GpuDiffraction.cu:3464-3500 and 4276-4282), which diffracts
+ * the same beams on several grids. */
+int mbs_po_diffract_staged_pinned(mbs_po_ctx *ctx, const mbs_po_staged *staged, int precision,
+                                  const double **M_out, const double **Mns_out,
+                                  mbs_po_stats *stats);
+
+/* Host-side time of the phases of this context's last host-array call
+ * (mbs_po_diffract, _pinned, _staged_pinned, _fft_phi, _multisize), ms:
+ *   [0] growth of the upload area and staged batch, [1] enqueueing the
+ *   host->device copies, [2] record building and its status check,
+ *   [3] enqueueing the diffraction, [4] waiting for the device,
+ *   [5] handing back the result.  n <= 8 entries.  No counterpart in the
+ *   reference (its MBS_GPU_TIMING breakdown, GpuDiffraction.cu:4283-4285). */
+int mbs_po_last_profile(const mbs_po_ctx *ctx, double *ms, int n);
+
+/* Helpers of the drop-in's environment knobs: pure functions, the caller
+ * passes the environment strings (NULL when unset).
+ *   mbs_po_multi_devices  devices one HandleOrientationsToLocalGpu call is
+ *       split over: MBS_GPU_MULTI ("0" off, N a limit), MBS_GPU_MULTI_MAX (a
+ *       cap), off by default under MPI (gpu_multi_device_count,
+ *       GpuDiffraction.cu:595-626).
+ *   mbs_po_device_range   device dev's contiguous orientation range of the
+ *       split (GpuDiffraction.cu:4224-4226).
+ *   mbs_po_eps1_override  the MBS_GPU_EPS1 override of the singular-edge
+ *       threshold eps1 (gpu_effective_eps1, GpuDiffraction.cu:498-512).
+ *   mbs_po_beam_stats     the MBS_GPU_BEAM_STATS line of a batch
+ *       (GpuDiffraction.cu:4354-4443) into buf (MBS_PO_ERANGE if cut). */
+int    mbs_po_multi_devices(int work_count, int device_count, const char *multi,
+                            const char *multi_max, int under_mpi);
+void   mbs_po_device_range(int start, int count, int n_devices, int dev, int *begin, int *sub_count);
+double mbs_po_eps1_override(double eps1, const char *value);
+int    mbs_po_beam_stats(const mbs_po_beams *beams, char *buf, int len);
 
 /* Allocation-free variant of mbs_po_diffract_staged (no counterpart in the
  * reference).  For callers that cannot allocate device memory when they

@@ -84,6 +84,7 @@ class HostConfig(C.Structure):
         ("cutoff_profile", C.c_int32), ("shadow_off", C.c_int32),
         ("legacy_sign", C.c_int32), ("n_threads", C.c_int32),
         ("reference_prepare", C.c_int32),
+        ("trace_cutoff_importance", C.c_double), ("beam_cutoff_importance", C.c_double),
     ]
 
 

@@ -167,6 +167,10 @@ class ParticleConfig:
     # True: the reference's PrepareBeams; False: the producer's bit-identical
     # restatement of it (host/prepare.cpp), several times faster
     reference_prepare: bool = False
+    # individual importance thresholds (> 0) over the profile's:
+    # --trace-cutoff-importance and --beam-cutoff-importance
+    trace_cutoff_importance: float = 0.0
+    beam_cutoff_importance: float = 0.0
 
     PROFILES = ("legacy-default", "off", "safe", "balanced", "fast")
 
@@ -184,7 +188,9 @@ class ParticleConfig:
             absorption=int(self.absorption), wavelength=self.wavelength,
             max_reflections=self.max_reflections, cutoff_profile=self._profile(),
             shadow_off=int(self.shadow_off), legacy_sign=int(self.legacy_sign),
-            n_threads=self.n_threads, reference_prepare=int(self.reference_prepare))
+            n_threads=self.n_threads, reference_prepare=int(self.reference_prepare),
+            trace_cutoff_importance=self.trace_cutoff_importance,
+            beam_cutoff_importance=self.beam_cutoff_importance)
 
 
 def _host():

@@ -16,9 +16,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -114,9 +116,17 @@ struct mbs_po_ctx {
     cudaEvent_t ev[8] = {};
     cudaEvent_t partial_done = nullptr;   // recorded after each launch that used `partial`
     int variant[2] = {0, 0};     // chosen launch shape per precision
+    // host-side phases of the last host call, ms (mbs_po_last_profile)
+    double prof[8] = {};
 };
 
 namespace {
+
+double host_ms()
+{
+    return std::chrono::duration<double, std::milli>(
+        std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 int fail(mbs_po_ctx *ctx, int code, const std::string &msg)
 {
@@ -500,6 +510,7 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     const size_t off_ao = off_raw + align256(scales ? nB * MBS_PO_RAW_STRIDE * 8 : 0);
     const size_t off_ap = off_ao + align256(has_abs ? (nB + 1) * 8 : 0);
     const size_t raw_bytes = off_ap + align256(nAbs * 8);
+    const double tg0 = host_ms();
     if ((rc = grow_arena(ctx, ctx->raw, raw_bytes, "staging", st)))
         return rc;
     unsigned char *raw = (unsigned char *)ctx->raw.base;
@@ -517,6 +528,8 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
     if ((rc = (s == &ctx->host_staged || s->reused ? grow_arena(ctx, s->arena, bytes, "staged batch", st)
                                                    : ensure_arena(ctx, s->arena, bytes, "staged batch"))))
         return rc;
+    const double tg1 = host_ms();
+    ctx->prof[0] = tg1 - tg0;
     unsigned char *base = (unsigned char *)s->arena.base;
     s->beams = (DevBeam *)(base + o_beams);
     s->verts = (DevVert *)(base + o_verts);
@@ -553,6 +566,7 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
             }
         }
         CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st), "memset status");
+        ctx->prof[1] = host_ms() - tg1;
         PackParams P;
         P.n_beams = nB;
         P.n_verts = nV;
@@ -587,6 +601,7 @@ int stage_into(mbs_po_ctx *ctx, const mbs_po_beams *b, mbs_po_staged *s, cudaStr
         int status = 0;
         CK(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H status");
         CK(cudaStreamSynchronize(st), "pack sync");
+        ctx->prof[2] = host_ms() - tg1 - ctx->prof[1];
         if (status)
             return fail(ctx, MBS_PO_EBEAM, "malformed beam in batch");
     }
@@ -905,6 +920,80 @@ extern "C" int mbs_po_staged_free(mbs_po_ctx *ctx, mbs_po_staged *s)
     return MBS_PO_OK;
 }
 
+extern "C" int mbs_po_stage_repeat(mbs_po_ctx *ctx, const mbs_po_staged *src, int n,
+                                   const int32_t *orient_index, const double *weight,
+                                   mbs_po_staged **out)
+{
+    if (out)
+        *out = nullptr;
+    if (!ctx || !src || !out || n < 0 || (n > 0 && (!orient_index || !weight)))
+        return fail(ctx, MBS_PO_EINVAL, "bad arguments");
+    if (src->n_sets != 1)
+        return fail(ctx, MBS_PO_EINVAL, "multi-size staged batches cannot be repeated");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    // the source's orientation offsets, back on the host
+    std::vector<int32_t> soff(src->n_orient + 1);
+    CK(cudaMemcpy(soff.data(), src->beam_off, soff.size() * sizeof(int32_t), cudaMemcpyDeviceToHost),
+       "D2H offsets");
+    // consecutive entries whose ranges do not continue each other are
+    // separated by a weight-0 orientation spanning [end, next begin): empty
+    // when the next range starts at or before the end (a repeat), the
+    // skipped beams (weighted 0) when it starts after it
+    std::vector<int32_t> boff;
+    std::vector<double> w;
+    boff.reserve((size_t)n * 2 + 1);
+    w.reserve((size_t)n * 2);
+    for (int i = 0; i < n; ++i) {
+        const int o = orient_index[i];
+        if (o < 0 || o >= src->n_orient)
+            return fail(ctx, MBS_PO_ERANGE, "orientation index outside the staged batch");
+        if (!boff.empty() && boff.back() != soff[o]) {
+            w.push_back(0.0);
+            boff.push_back(soff[o]);
+        } else if (boff.empty()) {
+            boff.push_back(soff[o]);
+        }
+        w.push_back(weight[i]);
+        boff.push_back(soff[o + 1]);
+    }
+    if (boff.empty())
+        boff.push_back(0);
+    if (w.size() >= ((size_t)1 << 31))
+        return fail(ctx, MBS_PO_ERANGE, "repeated batch exceeds 2^31 orientations");
+    mbs_po_staged *v = new mbs_po_staged();
+    const size_t o_boff = 0, o_w = align256(boff.size() * sizeof(int32_t));
+    int rc = ensure_arena(ctx, v->arena, o_w + std::max<size_t>(w.size(), 1) * sizeof(double), "repeated batch");
+    if (rc) {
+        delete v;
+        return rc;
+    }
+    unsigned char *base = (unsigned char *)v->arena.base;
+    v->beams = src->beams;
+    v->verts = src->verts;
+    v->brec = src->brec;
+    v->vrec = src->vrec;
+    v->moments = src->moments;
+    v->vbeg = src->vbeg;
+    v->beam_off = (int32_t *)(base + o_boff);
+    v->weight = (double *)(base + o_w);
+    v->n_orient = (int)w.size();
+    v->n_beams = src->n_beams;
+    v->n_verts = src->n_verts;
+    v->max_nv = src->max_nv;
+    v->n_sets = 1;
+    v->orient_per_set = v->n_orient;
+    cudaError_t e = cudaMemcpy(v->beam_off, boff.data(), boff.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !w.empty())
+        e = cudaMemcpy(v->weight, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        staged_release(v);
+        delete v;
+        return cuda_fail(ctx, e, "H2D repeated batch");
+    }
+    *out = v;
+    return MBS_PO_OK;
+}
+
 extern "C" int mbs_po_diffract_staged(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision,
                                       double *M_dev, double *Mns_dev, void *stream,
                                       mbs_po_stats *stats)
@@ -1002,24 +1091,30 @@ int run_phi_interp(mbs_po_ctx *ctx, const double *low, int n_low, int n_rows, do
 // view[1] when no-shadow sums are asked for by a non-null Mns_accum) receive
 // pointers to the planes in the page-locked result buffer, or NULL when the
 // batch holds nothing to add.
+// With `pre` set, `beams` is ignored and the already staged batch `pre`
+// (one output set) is diffracted: nothing is uploaded.
 int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scales, int n_scales,
                   double k_rephase, int precision, double *M_accum, double *Mns_accum,
-                  mbs_po_stats *stats, int n_full = 0, const double **view = nullptr)
+                  mbs_po_stats *stats, int n_full = 0, const double **view = nullptr,
+                  const mbs_po_staged *pre = nullptr)
 {
     if (view) {
         view[0] = nullptr;
         view[1] = nullptr;
     }
-    if (!ctx || !beams || !M_accum)
+    if (!ctx || (!beams && !pre) || !M_accum)
         return fail(ctx, MBS_PO_EINVAL, "null argument");
     if (!ctx->has_grid || !ctx->has_wave)
         return fail(ctx, MBS_PO_ESTATE, "grid and wave constants must be set first");
     if (scales && n_scales < 1)
         return fail(ctx, MBS_PO_EINVAL, "no size scale factors");
+    if (pre && pre->n_sets != 1)
+        return fail(ctx, MBS_PO_EINVAL, "multi-size staged batches use mbs_po_diffract_staged");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const int64_t G = (int64_t)ctx->grid.n_az * (ctx->grid.n_zen + 1);
-    if (beams->n_orient == 0 || beams->n_beams == 0 || G == 0)
-        return validate(ctx, beams);
+    if (pre ? (pre->n_orient == 0 || pre->n_beams == 0 || G == 0)
+            : (beams->n_orient == 0 || beams->n_beams == 0 || G == 0))
+        return pre ? MBS_PO_OK : validate(ctx, beams);
     cudaStream_t st = ctx->stream;
     const bool ns = Mns_accum != nullptr;
     const size_t sets = scales ? (size_t)n_scales : 1;
@@ -1039,12 +1134,16 @@ int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scal
         CK(cudaMallocHost((void **)&ctx->hres, n_out * 2 * sizeof(double)), "cudaMallocHost");
         ctx->hres_cap = n_out * 2;
     }
+    for (double &v : ctx->prof)
+        v = 0.0;
     CK(cudaEventRecord(ctx->ev[3], st), "event");
-    if ((rc = stage_into(ctx, beams, &ctx->host_staged, st, scales, n_scales, k_rephase)))
+    if (!pre && (rc = stage_into(ctx, beams, &ctx->host_staged, st, scales, n_scales, k_rephase)))
         return rc;
+    const double td0 = host_ms();
     CK(cudaEventRecord(ctx->ev[4], st), "event");
     CK(cudaMemsetAsync(ctx->macc, 0, n * (ns ? 2 : 1) * sizeof(double), st), "memset acc");
-    rc = run_diffract(ctx, &ctx->host_staged, precision, ctx->macc, ns ? ctx->macc + n : nullptr, st, stats);
+    rc = run_diffract(ctx, pre ? pre : &ctx->host_staged, precision, ctx->macc, ns ? ctx->macc + n : nullptr,
+                      st, stats);
     if (rc)
         return rc;
     const double *dev_out = ctx->macc;
@@ -1060,7 +1159,11 @@ int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scal
     CK(cudaEventRecord(ctx->ev[5], st), "event");
     CK(cudaMemcpyAsync(ctx->hres, dev_out, n_out * (ns ? 2 : 1) * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
     CK(cudaEventRecord(ctx->ev[7], st), "event");
+    const double td1 = host_ms();
     CK(cudaStreamSynchronize(st), "sync");
+    const double td2 = host_ms();
+    ctx->prof[3] = td1 - td0;
+    ctx->prof[4] = td2 - td1;
     float h2d = 0.f, d2h = 0.f;
     cudaEventElapsedTime(&h2d, ctx->ev[3], ctx->ev[4]);
     cudaEventElapsedTime(&d2h, ctx->ev[5], ctx->ev[7]);
@@ -1074,10 +1177,11 @@ int diffract_host(mbs_po_ctx *ctx, const mbs_po_beams *beams, const double *scal
             for (size_t i = 0; i < n_out; ++i)
                 Mns_accum[i] += ctx->hres[n_out + i];
     }
+    ctx->prof[5] = host_ms() - td2;
     if (stats) {
         stats->h2d_ms = h2d;
         stats->d2h_ms = d2h;
-        stats->launches += 1;   // pack kernel
+        stats->launches += pre ? 0 : 1;   // pack kernel
     }
     return MBS_PO_OK;
 }
@@ -1111,6 +1215,137 @@ extern "C" int mbs_po_diffract_pinned(mbs_po_ctx *ctx, const mbs_po_beams *beams
     if (Mns_out)
         *Mns_out = view[1];
     return rc;
+}
+
+extern "C" int mbs_po_last_profile(const mbs_po_ctx *ctx, double *ms, int n)
+{
+    if (!ctx || !ms || n < 0)
+        return MBS_PO_EINVAL;
+    for (int i = 0; i < n && i < 8; ++i)
+        ms[i] = ctx->prof[i];
+    return MBS_PO_OK;
+}
+
+extern "C" int mbs_po_diffract_staged_pinned(mbs_po_ctx *ctx, const mbs_po_staged *staged, int precision,
+                                             const double **M_out, const double **Mns_out,
+                                             mbs_po_stats *stats)
+{
+    if (M_out)
+        *M_out = nullptr;
+    if (Mns_out)
+        *Mns_out = nullptr;
+    if (!ctx)
+        return MBS_PO_EINVAL;
+    if (!M_out || !staged)
+        return fail(ctx, MBS_PO_EINVAL, "null argument");
+    double dummy = 0.0;
+    const double *view[2] = {nullptr, nullptr};
+    const int rc = diffract_host(ctx, nullptr, nullptr, 0, 0.0, precision, &dummy, Mns_out ? &dummy : nullptr,
+                                 stats, 0, view, staged);
+    *M_out = view[0];
+    if (Mns_out)
+        *Mns_out = view[1];
+    return rc;
+}
+
+// ---------------------------------------------- drop-in host helpers --
+// Pure functions behind the drop-in's environment knobs (the caller reads
+// the environment and passes the strings), so their rules are testable on
+// any host.
+
+extern "C" int mbs_po_multi_devices(int work_count, int device_count, const char *multi,
+                                    const char *multi_max, int under_mpi)
+{
+    // gpu_multi_device_count, GpuDiffraction.cu:595-626
+    if (work_count <= 1)
+        return 1;
+    if (multi && multi[0] == '0' && multi[1] == '\0')
+        return 1;
+    if ((!multi || !*multi) && under_mpi)
+        return 1;
+    if (device_count <= 1)
+        return 1;
+    int limit = device_count;
+    if (multi && *multi) {
+        char *end = nullptr;
+        const long v = std::strtol(multi, &end, 10);
+        if (end && *end == '\0' && v > 0)
+            limit = (int)std::min<long>(v, 1 << 20);
+    }
+    if (multi_max) {
+        char *end = nullptr;
+        const long v = std::strtol(multi_max, &end, 10);
+        if (end && *end == '\0' && v > 0)
+            limit = std::min(limit, (int)std::min<long>(v, 1 << 20));
+    }
+    return std::max(1, std::min(std::min(device_count, limit), work_count));
+}
+
+extern "C" void mbs_po_device_range(int start, int count, int n_devices, int dev, int *begin,
+                                    int *sub_count)
+{
+    // GpuDiffraction.cu:4224-4226
+    const int64_t b = start + (int64_t)count * dev / std::max(1, n_devices);
+    const int64_t e = start + (int64_t)count * (dev + 1) / std::max(1, n_devices);
+    if (begin)
+        *begin = (int)b;
+    if (sub_count)
+        *sub_count = (int)(e - b);
+}
+
+extern "C" double mbs_po_eps1_override(double eps1, const char *value)
+{
+    // gpu_effective_eps1, GpuDiffraction.cu:498-512 (the FP32 floor of 3e-5
+    // is applied by the kernels' own threshold)
+    if (value) {
+        char *end = nullptr;
+        const double v = std::strtod(value, &end);
+        if (end && end != value && *end == '\0' && v > 0.0)
+            return v;
+    }
+    return eps1;
+}
+
+extern "C" int mbs_po_beam_stats(const mbs_po_beams *b, char *buf, int len)
+{
+    // the MBS_GPU_BEAM_STATS line of GpuDiffraction.cu:4354-4443
+    if (!b || !buf || len <= 0)
+        return MBS_PO_EINVAL;
+    const int64_t nB = b->n_beams;
+    const int nO = b->n_orient;
+    size_t hist[33] = {};
+    size_t ext = 0, in = 0, ex = 0, ey = 0, mn = (size_t)-1, mx = 0;
+    for (int o = 0; o < nO; ++o) {
+        const size_t c = (size_t)(b->beam_offsets[o + 1] - b->beam_offsets[o]);
+        mn = std::min(mn, c);
+        mx = std::max(mx, c);
+    }
+    for (int64_t i = 0; i < nB; ++i) {
+        const int64_t v0 = b->vert_offsets[i], v1 = b->vert_offsets[i + 1];
+        const int nv = (int)(v1 - v0);
+        if (nv >= 0 && nv <= 32)
+            ++hist[nv];
+        if (b->beam_flags[i] & MBS_PO_BEAM_EXTERNAL) ++ext; else ++in;
+        for (int64_t v = v0; v < v1; ++v) {
+            ex += (b->edge_flags[v] & MBS_PO_EDGE_VALID_X) ? 1 : 0;
+            ey += (b->edge_flags[v] & MBS_PO_EDGE_VALID_Y) ? 1 : 0;
+        }
+    }
+    std::string line = "GPU beam stats orient=" + std::to_string(nO) + " beams=" + std::to_string(nB);
+    char tmp[256];
+    std::snprintf(tmp, sizeof(tmp),
+                  " beams/orient min=%zu mean=%.3f max=%zu external=%zu internal=%zu "
+                  "valid_edges_x/beams=%.3f valid_edges_y/beams=%.3f vertices:",
+                  mn == (size_t)-1 ? 0 : mn, nB == 0 ? 0.0 : (double)nB / (double)nO, mx, ext, in,
+                  nB == 0 ? 0.0 : (double)ex / (double)nB, nB == 0 ? 0.0 : (double)ey / (double)nB);
+    line += tmp;
+    for (int nv = 1; nv <= 32; ++nv)
+        if (hist[nv]) {
+            std::snprintf(tmp, sizeof(tmp), " %d:%zu", nv, hist[nv]);
+            line += tmp;
+        }
+    std::snprintf(buf, (size_t)len, "%s", line.c_str());
+    return (int)line.size() < len ? MBS_PO_OK : MBS_PO_ERANGE;
 }
 
 extern "C" int mbs_po_diffract_fft_phi(mbs_po_ctx *ctx, const mbs_po_beams *beams, int precision,

@@ -43,9 +43,13 @@ def lib() -> C.CDLL:
                                       C.POINTER(abi.Stats)]
         L.mbs_po_diffract_pinned.argtypes = [vp, C.POINTER(abi.Beams), C.c_int,
                                              C.POINTER(abi._dp), C.POINTER(abi._dp), C.POINTER(abi.Stats)]
+        L.mbs_po_diffract_staged_pinned.argtypes = [vp, vp, C.c_int, C.POINTER(abi._dp),
+                                                    C.POINTER(abi._dp), C.POINTER(abi.Stats)]
         L.mbs_po_stage.argtypes = [vp, C.POINTER(abi.Beams), C.POINTER(vp)]
         L.mbs_po_staged_free.argtypes = [vp, vp]
         L.mbs_po_restage.argtypes = [vp, C.POINTER(abi.Beams), vp]
+        L.mbs_po_stage_repeat.argtypes = [vp, vp, C.c_int, C.POINTER(C.c_int32), abi._dp,
+                                          C.POINTER(vp)]
         L.mbs_po_diffract_staged.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.POINTER(abi.Stats)]
         L.mbs_po_extinction.argtypes = [vp, C.POINTER(abi.Beams), abi._dp]
@@ -162,6 +166,22 @@ class GpuHandlerPO:
         rc = lib().mbs_po_diffract_pinned(self.ctx, C.byref(b), precision, C.byref(m),
                                           C.byref(mn) if noshadow else None, C.byref(self.last_stats))
         self._call(rc, "mbs_po_diffract_pinned")
+        shape = (self.grid.n_az, self.grid.n_zen + 1, 16)
+        n = shape[0] * shape[1] * shape[2]
+
+        def grab(ptr):
+            return np.ctypeslib.as_array(ptr, (n,)).reshape(shape).copy() if ptr else None
+        return grab(m), grab(mn)
+
+    def diffract_staged_pinned(self, staged: "Staged", noshadow: bool = False,
+                               precision: int = abi.FP64):
+        """mbs_po_diffract_staged_pinned: diffract_pinned of a batch staged
+        earlier (no upload)."""
+        m, mn = abi._dp(), abi._dp()
+        rc = lib().mbs_po_diffract_staged_pinned(self.ctx, staged.handle, precision, C.byref(m),
+                                                 C.byref(mn) if noshadow else None,
+                                                 C.byref(self.last_stats))
+        self._call(rc, "mbs_po_diffract_staged_pinned")
         shape = (self.grid.n_az, self.grid.n_zen + 1, 16)
         n = shape[0] * shape[1] * shape[2]
 
@@ -371,6 +391,22 @@ class GpuHandlerPO:
         b = batch.as_c(with_raw=False)
         self._call(lib().mbs_po_stage(self.ctx, C.byref(b), C.byref(h)), "mbs_po_stage")
         return Staged(self, h, batch)
+
+    def stage_repeat(self, src: Staged, orient_index, weight) -> Staged:
+        """mbs_po_stage_repeat: orientations orient_index of `src` (which
+        must outlive the result) with the given weights, sharing src's
+        device records."""
+        idx = np.ascontiguousarray(orient_index, dtype=np.int32)
+        w = np.ascontiguousarray(weight, dtype=np.float64)
+        h = C.c_void_p()
+        self._call(lib().mbs_po_stage_repeat(self.ctx, src.handle, len(idx), abi.ptr(idx, C.c_int32),
+                                             abi.ptr(w, C.c_double), C.byref(h)), "mbs_po_stage_repeat")
+        st = Staged.__new__(Staged)
+        st._h, st.handle, st.n_sets = self, h, 1
+        n_out = int(len(idx))
+        st.n_orient, st.n_beams, st.n_verts = n_out, src.n_beams, src.n_verts
+        st._src = src
+        return st
 
     def restage(self, staged: Staged, batch: BeamBatch) -> Staged:
         """mbs_po_restage: re-fill `staged` with `batch` in the device memory

@@ -132,10 +132,11 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
     }
     const int64_t nBeams = ob[nOrient], nVerts = ov[nOrient];
 
-    out.beam_offsets.assign(nOrient + 1, 0);
-    out.orient_weight.assign(nOrient, 0.0);
-    out.extinction_ot.assign(nOrient, 0.0);
-    out.vert_offsets.assign(nBeams + 1, 0);
+    // every element below is written by pass 2 (uninitialised resize)
+    out.beam_offsets.resize(nOrient + 1);
+    out.orient_weight.resize(nOrient);
+    out.extinction_ot.resize(nOrient);
+    out.vert_offsets.resize(nBeams + 1);
     out.vx.resize(nVerts);
     out.vy.resize(nVerts);
     out.slope_yx.resize(nVerts);
@@ -146,7 +147,7 @@ int mbs_pack_prepared(const std::vector<PreparedOrientation> &prepared,
     if (with_raw)
     {
         out.beam_raw.resize((size_t)nBeams * MBS_PO_RAW_STRIDE);
-        out.abs_offsets.assign(nBeams + 1, 0);
+        out.abs_offsets.resize(nBeams + 1);
         out.abs_paths.resize(oa[nOrient]);
     }
     else

@@ -12,22 +12,43 @@
 #include "mbs_po_b200.h"
 #include "HandlerPO.h"
 
+#include <memory>
 #include <string>
 #include <vector>
 
+// Allocator whose resize() leaves new elements uninitialised: every packed
+// array is filled completely by the (parallel) packing pass, so zeroing the
+// new elements first would only add a serial pass that also first-touches
+// every page on one thread.
+template <typename T>
+struct MbsNoInitAlloc : std::allocator<T>
+{
+    template <typename U>
+    struct rebind { using other = MbsNoInitAlloc<U>; };
+    MbsNoInitAlloc() = default;
+    template <typename U>
+    MbsNoInitAlloc(const MbsNoInitAlloc<U> &) noexcept {}
+    template <typename U>
+    void construct(U *p) noexcept { ::new (static_cast<void *>(p)) U; }
+    template <typename U, typename... Args>
+    void construct(U *p, Args &&...args) { ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...); }
+};
+template <typename T>
+using MbsVec = std::vector<T, MbsNoInitAlloc<T>>;
+
 struct MbsPackedBeams
 {
-    std::vector<int64_t> beam_offsets;
-    std::vector<double>  orient_weight;
-    std::vector<int64_t> vert_offsets;
-    std::vector<double>  vx, vy, slope_yx, slope_xy;
-    std::vector<uint8_t> edge_flags;
-    std::vector<double>  beam_geom;
-    std::vector<uint8_t> beam_flags;
-    std::vector<double>  beam_raw;
-    std::vector<int64_t> abs_offsets;
-    std::vector<double>  abs_paths;
-    std::vector<double>  extinction_ot;   // PreparedOrientation::extinctionOt
+    MbsVec<int64_t> beam_offsets;
+    MbsVec<double>  orient_weight;
+    MbsVec<int64_t> vert_offsets;
+    MbsVec<double>  vx, vy, slope_yx, slope_xy;
+    MbsVec<uint8_t> edge_flags;
+    MbsVec<double>  beam_geom;
+    MbsVec<uint8_t> beam_flags;
+    MbsVec<double>  beam_raw;
+    MbsVec<int64_t> abs_offsets;
+    MbsVec<double>  abs_paths;
+    MbsVec<double>  extinction_ot;   // PreparedOrientation::extinctionOt
     int max_vertices = 0;
 
     mbs_po_beams view(bool with_raw) const;

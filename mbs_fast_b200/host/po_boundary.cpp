@@ -15,7 +15,14 @@
 //   - one context per host thread (thread_local, GpuDiffraction.cu:252).
 // Environment knobs: MBS_B200_PRECISION=fp64|fp32c (default fp64, the
 // reference's double build), MBS_GPU_TIMING=1 prints per-call timings,
-// MBS_GPU_MEM_FRACTION bounds batch sizes like the reference.
+// MBS_GPU_MEM_FRACTION bounds batch sizes like the reference; and the
+// reference's own MBS_GPU_MULTI / MBS_GPU_MULTI_MAX (a call split over the
+// visible devices, GpuDiffraction.cu:595-628, 4185-4270), MBS_GPU_EPS1 (the
+// singular-edge threshold, :498-512) and MBS_GPU_BEAM_STATS=1 (per-batch
+// beam statistics, :492-496, 4354-4443).  HandleOrientationsToLocalGpuOnDevice
+// with a nonzero cacheToken keeps the staged beams on the device and reuses
+// them for the next call with the same token and range (:3464-3500,
+// 4276-4282).
 #include "HandlerPO.h"
 #include "FftStatistics.h"
 #include "beam_pack.h"
@@ -25,6 +32,11 @@
 
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -47,15 +59,31 @@ struct BoundaryContext
     // the main path's packed batch, kept between calls so that its pages are
     // not allocated and first touched again on every call
     MbsPackedBeams packed;
+    // packed-beam cache of HandleOrientationsToLocalGpuOnDevice: the staged
+    // batch of (token, start, count) with the wave constants it was staged
+    // under (its records hold them)
+    mbs_po_staged *cached = nullptr;
+    unsigned long long cachedToken = 0;
+    int cachedStart = -1, cachedCount = -1;
+    mbs_po_wave cachedWave{};
 
     ~BoundaryContext()
     {
         if (ctx)
+        {
+            if (cached)
+                mbs_po_staged_free(ctx, cached);
             mbs_po_destroy(ctx);
+        }
     }
 };
 
 thread_local BoundaryContext g_ctx;
+// set on the multi-device split's workers and inside
+// HandleOrientationsToLocalGpuOnDevice: no further split (g_gpuMultiWorker)
+thread_local bool g_multiWorker = false;
+// the OnDevice caller's packed-beam cache token (g_gpuPackCacheToken)
+thread_local unsigned long long g_cacheToken = 0;
 
 bool env_is(const char *name, const char *value)
 {
@@ -88,6 +116,32 @@ bool report(int rc, const char *where)
     return false;
 }
 
+bool under_mpi()
+{
+    // gpu_running_under_mpi, GpuDiffraction.cu:574-592
+    const char *names[] = {"OMPI_COMM_WORLD_SIZE", "PMI_SIZE", "PMIX_SIZE", "MPI_LOCALNRANKS"};
+    for (const char *name : names)
+    {
+        const char *v = std::getenv(name);
+        if (!v || !*v)
+            continue;
+        char *end = nullptr;
+        const long n = std::strtol(v, &end, 10);
+        if (end && *end == '\0' && n > 1)
+            return true;
+    }
+    return false;
+}
+
+int multi_devices(int workCount)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess)
+        count = 1;
+    return mbs_po_multi_devices(workCount, count, std::getenv("MBS_GPU_MULTI"),
+                                std::getenv("MBS_GPU_MULTI_MAX"), under_mpi() ? 1 : 0);
+}
+
 double mem_fraction()
 {
     const char *v = std::getenv("MBS_GPU_MEM_FRACTION");
@@ -110,6 +164,10 @@ public:
         BoundaryContext &c = g_ctx;
         if (c.ctx && c.device != device)
         {
+            if (c.cached)
+                mbs_po_staged_free(c.ctx, c.cached);
+            c.cached = nullptr;
+            c.cachedToken = 0;
             mbs_po_destroy(c.ctx);
             c.ctx = nullptr;
             c.gridNAz = c.gridNZen = -1;
@@ -177,7 +235,7 @@ struct HandlerPOWaveAccess : public HandlerPO
         w.compl_wave_im = imag(cw);
         w.inv_compl_wave_re = real(icw);
         w.inv_compl_wave_im = imag(icw);
-        w.eps1 = h.*(&HandlerPOWaveAccess::m_eps1);
+        w.eps1 = mbs_po_eps1_override(h.*(&HandlerPOWaveAccess::m_eps1), std::getenv("MBS_GPU_EPS1"));
         w.abs_coeff = h.AbsorptionCoefficient();
         w.ot_far_reference_path = h.m_otFarReferencePath;
         w.ot_ping_distance = h.m_otPingDistance;
@@ -216,59 +274,234 @@ static void add_plane(const double *plane, Arr2D &M, int nAz, int nRows)
         }
 }
 
+// One device's share: packs prepared[start, start+count) (or reuses the
+// staged beams of the OnDevice caller's cache token) and diffracts it on this
+// thread's context; *Mv / *Mnv point at the sums in the context's page-locked
+// result buffer (NULL when the range holds no beams), valid until this
+// thread's next call.
+static bool diffract_core(HandlerPO &h, const ScatteringRange &sphere,
+                          const std::vector<PreparedOrientation> &prepared, int start, int count,
+                          bool computeNoShadow, int device, const double **Mv, const double **Mnv)
+{
+    *Mv = *Mnv = nullptr;
+    const bool timing = env_is("MBS_GPU_TIMING", "1");
+    const auto t0 = std::chrono::steady_clock::now();
+    const int nAz = sphere.nAzimuth, nZen = sphere.nZenith;
+    const mbs_po_wave wave = HandlerPOWaveAccess::Get(h, 0.0);
+    BoundaryContext &c = g_ctx;
+    const unsigned long long token = g_cacheToken;
+    const bool hit = token != 0 && c.cached && c.cachedToken == token && c.cachedStart == start
+                     && c.cachedCount == count && c.device == device
+                     && std::memcmp(&c.cachedWave, &wave, sizeof(wave)) == 0;
+    MbsPackedBeams &packed = c.packed;
+    mbs_po_beams view{};
+    if (!hit)
+    {
+        std::string err;
+        const int prc = mbs_pack_prepared(prepared, start, count, false, packed, &err);
+        if (prc == MBS_PO_EBEAM)
+            return false;   // reference: failDirect("bad-edge-data")
+        if (prc != MBS_PO_OK)
+            return false;
+        view = packed.view(false);
+        if (env_is("MBS_GPU_BEAM_STATS", "1"))
+        {
+            char line[1024];
+            mbs_po_beam_stats(&view, line, (int)sizeof(line));
+            std::fprintf(stderr, "%s\n", line);
+        }
+        if (view.n_beams == 0)
+            return true;
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    if (!HandlerPOBoundary::Prepare(h, sphere, wave, device))
+        return false;
+    mbs_po_stats st;
+    std::memset(&st, 0, sizeof(st));
+    const auto t2 = std::chrono::steady_clock::now();
+    int rc;
+    if (token != 0)
+    {
+        if (!hit)
+        {
+            // (re)fill the cache: the staged beams stay on the device
+            rc = c.cached ? mbs_po_restage(c.ctx, &view, c.cached) : mbs_po_stage(c.ctx, &view, &c.cached);
+            if (rc != MBS_PO_OK)
+            {
+                c.cachedToken = 0;
+                if (rc == MBS_PO_EBEAM)
+                    return false;
+                return report(rc, "staging");
+            }
+            c.cachedToken = token;
+            c.cachedStart = start;
+            c.cachedCount = count;
+            c.cachedWave = wave;
+        }
+        rc = mbs_po_diffract_staged_pinned(c.ctx, c.cached, precision_from_env(), Mv,
+                                           computeNoShadow ? Mnv : nullptr, &st);
+    }
+    else
+    {
+        rc = mbs_po_diffract_pinned(c.ctx, &view, precision_from_env(), Mv,
+                                    computeNoShadow ? Mnv : nullptr, &st);
+    }
+    if (rc == MBS_PO_EBEAM)
+        return false;
+    if (!report(rc, "diffraction"))
+        return false;
+    if (timing)
+    {
+        const auto t3 = std::chrono::steady_clock::now();
+        auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        double pr[6] = {};
+        mbs_po_last_profile(c.ctx, pr, 6);
+        std::fprintf(stderr,
+                     "GPU timing diffract path=b200-%s device=%d orient=%d beams=%lld nAz=%d nZen=%d "
+                     "cache=%s pack=%.3fms h2d+stage=%.3fms kernels=%.3fms reduce=%.3fms "
+                     "total=%.3fms setup=%.3fms call=%.3fms "
+                     "[grow=%.3f h2d=%.3f build=%.3f enqueue=%.3f wait=%.3f result=%.3f]\n",
+                     precision_from_env() == MBS_PO_FP32C ? "fp32c" : "fp64", device, count,
+                     hit ? -1LL : (long long)view.n_beams, nAz, nZen,
+                     token == 0 ? "off" : (hit ? "hit" : "fill"), ms(t0, t1), st.h2d_ms,
+                     st.kernel_ms, st.reduce_ms, ms(t0, t3), ms(t1, t2), ms(t2, t3),
+                     pr[0], pr[1], pr[2], pr[3], pr[4], pr[5]);
+    }
+    return true;
+}
+
+// Persistent worker thread per device for the multi-device split.  Each keeps
+// its own BoundaryContext (device context, grid, staged batches) from call to
+// call, where the reference starts std::async threads per call
+// (GpuDiffraction.cu:4214-4250).  Never destroyed: idle workers wait until
+// the process exits.
+class DeviceWorkers
+{
+public:
+    static DeviceWorkers &get()
+    {
+        static DeviceWorkers *w = new DeviceWorkers();
+        return *w;
+    }
+
+    // fns[d] on device d's worker, all at once; true when all succeeded
+    bool run(const std::vector<std::function<bool()>> &fns)
+    {
+        while (workers_.size() < fns.size())
+            workers_.emplace_back(new Worker((int)workers_.size()));
+        for (size_t d = 0; d < fns.size(); ++d)
+        {
+            Worker &w = *workers_[d];
+            std::lock_guard<std::mutex> lk(w.m);
+            w.job = fns[d];
+            w.has = true;
+            w.done = false;
+            w.cv.notify_all();
+        }
+        bool ok = true;
+        for (size_t d = 0; d < fns.size(); ++d)
+        {
+            Worker &w = *workers_[d];
+            std::unique_lock<std::mutex> lk(w.m);
+            w.cv.wait(lk, [&] { return w.done; });
+            ok = w.ok && ok;
+        }
+        return ok;
+    }
+
+private:
+    struct Worker
+    {
+        std::mutex m;
+        std::condition_variable cv;
+        std::function<bool()> job;
+        bool has = false, done = false, ok = false;
+        std::thread th;
+        explicit Worker(int device) : th(&Worker::loop, this, device) { th.detach(); }
+        void loop(int device)
+        {
+            cudaSetDevice(device);
+            g_multiWorker = true;
+            for (;;)
+            {
+                std::function<bool()> f;
+                {
+                    std::unique_lock<std::mutex> lk(m);
+                    cv.wait(lk, [&] { return has; });
+                    f.swap(job);
+                    has = false;
+                }
+                const bool r = f();
+                std::lock_guard<std::mutex> lk(m);
+                ok = r;
+                done = true;
+                cv.notify_all();
+            }
+        }
+    };
+    std::vector<std::unique_ptr<Worker>> workers_;
+};
+
 static bool diffract_range(HandlerPO &h, const ScatteringRange &sphere,
                            const std::vector<PreparedOrientation> &prepared,
                            int start, int count, Arr2D &localM,
                            Arr2D &localM_noshadow, bool computeNoShadow, int device)
 {
+    const int nAz = sphere.nAzimuth, nZen = sphere.nZenith;
+    const int nDev = g_multiWorker ? 1 : multi_devices(count);
+    if (nDev > 1)
+    {
+        // contiguous ranges, one per device, summed into localM in device
+        // order (GpuDiffraction.cu:4185-4270)
+        static bool printed = false;
+        if (!printed || env_is("MBS_GPU_MULTI_DEBUG", "1"))
+        {
+            std::fprintf(stderr,
+                         "GPU multi-device: using %d visible CUDA devices for %d orientations in this batch "
+                         "(disable with MBS_GPU_MULTI=0, cap with MBS_GPU_MULTI_MAX=N).\n",
+                         nDev, count);
+            printed = true;
+        }
+        std::vector<const double *> pm(nDev, nullptr), pn(nDev, nullptr);
+        std::vector<std::function<bool()>> jobs;
+        for (int dev = 0; dev < nDev; ++dev)
+        {
+            int begin = 0, sub = 0;
+            mbs_po_device_range(start, count, nDev, dev, &begin, &sub);
+            jobs.push_back([&h, &sphere, &prepared, &pm, &pn, begin, sub, computeNoShadow, dev]() {
+                if (sub <= 0)
+                    return true;
+                return diffract_core(h, sphere, prepared, begin, sub, computeNoShadow, dev, &pm[dev],
+                                     &pn[dev]);
+            });
+        }
+        if (!DeviceWorkers::get().run(jobs))
+            return false;
+        for (int dev = 0; dev < nDev; ++dev)
+        {
+            if (pm[dev])
+                add_plane(pm[dev], localM, nAz, nZen + 1);
+            if (pn[dev])
+                add_plane(pn[dev], localM_noshadow, nAz, nZen + 1);
+        }
+        return true;
+    }
     const bool timing = env_is("MBS_GPU_TIMING", "1");
     const auto t0 = std::chrono::steady_clock::now();
-    const int nAz = sphere.nAzimuth, nZen = sphere.nZenith;
-    MbsPackedBeams &packed = g_ctx.packed;
-    std::string err;
-    const int prc = mbs_pack_prepared(prepared, start, count, false, packed, &err);
-    if (prc == MBS_PO_EBEAM)
-        return false;   // reference: failDirect("bad-edge-data")
-    if (prc != MBS_PO_OK)
-        return false;
-    const mbs_po_beams view = packed.view(false);
-    if (view.n_beams == 0)
-        return true;
-    const auto t1 = std::chrono::steady_clock::now();
-    if (!HandlerPOBoundary::Prepare(h, sphere, HandlerPOWaveAccess::Get(h, 0.0), device))
-        return false;
-    BoundaryContext &c = g_ctx;
-    mbs_po_stats st;
-    std::memset(&st, 0, sizeof(st));
-    // the sums stay in the library's page-locked buffer and are added into
-    // the Arr2D cells in one pass
     const double *Mv = nullptr, *Mnv = nullptr;
-    const auto t2 = std::chrono::steady_clock::now();
-    const int rc = mbs_po_diffract_pinned(c.ctx, &view, precision_from_env(), &Mv,
-                                          computeNoShadow ? &Mnv : nullptr, &st);
-    if (rc == MBS_PO_EBEAM)
+    if (!diffract_core(h, sphere, prepared, start, count, computeNoShadow, device, &Mv, &Mnv))
         return false;
-    if (!report(rc, "diffraction"))
-        return false;
-    const auto t3 = std::chrono::steady_clock::now();
+    const auto t1 = std::chrono::steady_clock::now();
     if (Mv)
         add_plane(Mv, localM, nAz, nZen + 1);
     if (Mnv)
         add_plane(Mnv, localM_noshadow, nAz, nZen + 1);
-    if (timing)
-    {
-        const auto t4 = std::chrono::steady_clock::now();
-        auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
-            return std::chrono::duration<double, std::milli>(b - a).count();
-        };
-        std::fprintf(stderr,
-                     "GPU timing diffract path=b200-%s orient=%d beams=%lld nAz=%d nZen=%d "
-                     "pack=%.3fms h2d+stage=%.3fms kernels=%.3fms reduce=%.3fms total=%.3fms "
-                     "setup=%.3fms call=%.3fms add=%.3fms\n",
-                     precision_from_env() == MBS_PO_FP32C ? "fp32c" : "fp64",
-                     view.n_orient, (long long)view.n_beams, nAz, nZen, ms(t0, t1), st.h2d_ms,
-                     st.kernel_ms, st.reduce_ms, ms(t0, t4), ms(t1, t2), ms(t2, t3), ms(t3, t4));
-    }
+    if (timing && Mv)
+        std::fprintf(stderr, "GPU timing add path=b200 call=%.3fms add=%.3fms\n",
+                     std::chrono::duration<double, std::milli>(t1 - t0).count(),
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count());
     return true;
 }
 
@@ -355,14 +588,23 @@ bool HandlerPO::HandleOrientationsToLocalGpu(const std::vector<PreparedOrientati
 bool HandlerPO::HandleOrientationsToLocalGpuOnDevice(
     const std::vector<PreparedOrientation> &prepared, int start, int count, int device,
     Arr2D &localM, Arr2D &localM_noshadow, double scale, double waveIndex,
-    unsigned long long /*cacheToken*/)
+    unsigned long long cacheToken)
 {
+    // the call stays on `device` (no further split) and reuses the staged
+    // beams of an earlier call with the same token and range
+    // (GpuDiffraction.cu:3464-3500)
     int saved = 0;
     cudaGetDevice(&saved);
     if (cudaSetDevice(device) != cudaSuccess)
         return false;
+    const bool prevWorker = g_multiWorker;
+    const unsigned long long prevToken = g_cacheToken;
+    g_multiWorker = true;
+    g_cacheToken = std::fabs(scale - 1.0) > 1e-15 ? 0 : cacheToken;   // scaled calls: no cache
     const bool ok = HandleOrientationsToLocalGpu(prepared, start, count, localM,
                                                  localM_noshadow, scale, waveIndex);
+    g_multiWorker = prevWorker;
+    g_cacheToken = prevToken;
     cudaSetDevice(saved);
     return ok;
 }
@@ -649,5 +891,13 @@ int HandlerPO::SelectGpuOrientationBatchSize(const std::vector<PreparedOrientati
     int count = maxCount;
     if (mbs_po_select_batch(g_ctx.ctx, &view, 0, maxCount, mem_fraction(), &count) != MBS_PO_OK)
         return std::max(1, maxCount);
-    return std::max(1, count);
+    int selected = std::max(1, count);
+    if (!g_multiWorker)
+    {
+        // the batch is split over the devices (GpuDiffraction.cu:3021-3027)
+        const int nDev = multi_devices(maxCount);
+        if (nDev > 1)
+            selected = std::min(maxCount, selected * nDev);
+    }
+    return selected;
 }

@@ -171,6 +171,11 @@ struct HostSetup
             handler->m_beamCutoffAreaRel = 0.0;
             handler->m_beamCutoffImportanceRel = profile == 2 ? 1e-10 : (profile == 3 ? 1e-8 : 1e-6);
         }
+        // individual thresholds after the profile, as the CLI applies them
+        if (cfg.trace_cutoff_importance > 0.0)
+            sc->m_traceCutoffImportanceRel = cfg.trace_cutoff_importance;
+        if (cfg.beam_cutoff_importance > 0.0)
+            handler->m_beamCutoffImportanceRel = cfg.beam_cutoff_importance;
         // PrepareBeams does not read the scattering grid; a 1x1 placeholder
         // keeps the per-track matrices of SetTracks small.
         handler->SetScatteringSphere(ScatteringRange(0, M_PI, 1, 1));

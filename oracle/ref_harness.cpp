@@ -61,6 +61,9 @@ typedef struct mbs_ref_config {
     int32_t     shadow_off;
     int32_t     legacy_sign;
     int32_t     n_threads;
+    int32_t     reference_prepare;        /* unused here */
+    double      trace_cutoff_importance;  /* > 0: --trace-cutoff-importance */
+    double      beam_cutoff_importance;   /* > 0: --beam-cutoff-importance */
 } mbs_ref_config;
 
 typedef struct mbs_ref_gridspec {
@@ -158,6 +161,10 @@ struct RefSetup
             range.zenithEnd = range.thetaValues.back();
             range.zenithStep = (range.zenithEnd - range.zenithStart) / gs.n_zen;
         }
+        if (cfg.trace_cutoff_importance > 0.0)
+            sc->m_traceCutoffImportanceRel = cfg.trace_cutoff_importance;
+        if (cfg.beam_cutoff_importance > 0.0)
+            handler->m_beamCutoffImportanceRel = cfg.beam_cutoff_importance;
         handler->SetFullOnly(true);
         handler->SetScatteringSphere(range);
         handler->SetTracks(&tracks);

@@ -19,10 +19,11 @@ ARGS = ["--method", "po", "--particle", "1", "100", "40", "--refractive-index", 
         "--scattering-grid", "0", "180", "48", "180", "--close"]
 
 
-def _run(binary, backend, out, env_extra=None, extra_args=()):
+def _run(binary, backend, out, env_extra=None, extra_args=(), args=None):
     env = dict(os.environ)
     env.update(env_extra or {})
-    r = subprocess.run([binary] + ARGS + list(extra_args) + ["--backend", backend, "--output", out],
+    r = subprocess.run([binary] + (ARGS if args is None else args) + list(extra_args)
+                       + ["--backend", backend, "--output", out],
                        capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
     name = os.path.basename(out)
@@ -90,3 +91,48 @@ def test_dropin_fft_phi_matches_reference_cuda_build(tmp_path):
     assert _wl2(gpu, ref) < 1e-7
     for k in ("Cext", "Csca"):
         assert abs(float(gpu_i[k]) / float(ref_i[k]) - 1) < 1e-7, k
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFGPU)),
+                    reason="drop-in or the reference's CUDA build not built")
+def test_dropin_eps1_and_beam_stats_knobs(tmp_path):
+    """MBS_GPU_EPS1 moves the singular-edge threshold in both builds alike
+    (the drop-in equals the reference's CUDA FP64 build under the same
+    override), and MBS_GPU_BEAM_STATS=1 prints per-batch beam statistics
+    whose beam totals agree with the reference build's."""
+    import re
+    env = {"MBS_GPU_EPS1": "1e-4", "MBS_GPU_BEAM_STATS": "1"}
+    ack = ["--allow-experimental-environment"]   # the CLI's guard for result-affecting knobs
+    ref, ref_i, ref_log = _run(REFGPU, "gpu", str(tmp_path / "ref"), env, extra_args=ack)
+    gpu, gpu_i, log = _run(DROPIN, "gpu", str(tmp_path / "gpu"), dict(env, MBS_GPU_TIMING="1"),
+                           extra_args=ack)
+    assert "path=b200-fp64" in log
+    assert _wl2(gpu, ref) < 1e-7
+    for k in ("Cext", "Csca"):
+        assert abs(float(gpu_i[k]) / float(ref_i[k]) - 1) < 1e-7, k
+
+    def beams(text):
+        return sum(int(m) for m in re.findall(r"GPU beam stats orient=\d+ beams=(\d+)", text))
+    assert beams(log) > 0 and beams(log) == beams(ref_log)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFCLI)),
+                    reason="drop-in or reference CLI not built")
+def test_dropin_theta_groups_reuse_staged_beams(tmp_path):
+    """--so3-quaternion with MBS_GPU_GROUPS=1: the reference's driver
+    diffracts each prepared chunk on several theta-row groups through
+    HandleOrientationsToLocalGpuOnDevice with one packed-beam cache token;
+    the drop-in keeps the staged beams on the device across those calls
+    (cache fill, then hits) and the result equals the reference CLI's CPU
+    result."""
+    args = [a for a in ARGS]
+    i = args.index("--sobol")
+    args[i:i + 2] = ["--so3-quaternion", "32"]
+    ref, ref_i, _ = _run(REFCLI, "cpu", str(tmp_path / "ref"), args=args)
+    gpu, gpu_i, log = _run(DROPIN, "gpu", str(tmp_path / "gpu"),
+                           {"MBS_GPU_TIMING": "1", "MBS_GPU_GROUPS": "1"}, args=args)
+    assert "cache=fill" in log and "cache=hit" in log
+    assert gpu.shape == ref.shape
+    assert _wl2(gpu, ref) < 1e-7
