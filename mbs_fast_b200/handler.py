@@ -82,10 +82,16 @@ def lib() -> C.CDLL:
 class Staged:
     """A batch resident in device memory (mbs_po_stage)."""
 
-    def __init__(self, handler: "GpuHandlerPO", handle: C.c_void_p, batch: BeamBatch):
+    def __init__(self, handler: "GpuHandlerPO", handle: C.c_void_p, batch: BeamBatch | None,
+                 counts: tuple | None = None, source: "Staged | None" = None):
         self._h = handler
         self.handle = handle
-        self._count(batch)
+        self._source = source          # a repeated view keeps its source alive
+        if batch is not None:
+            self._count(batch)
+        else:
+            self.n_sets = 1
+            self.n_orient, self.n_beams, self.n_verts = counts
 
     def _count(self, batch: BeamBatch) -> None:
         self.n_sets = int(lib().mbs_po_staged_sets(self.handle))
@@ -401,12 +407,7 @@ class GpuHandlerPO:
         h = C.c_void_p()
         self._call(lib().mbs_po_stage_repeat(self.ctx, src.handle, len(idx), abi.ptr(idx, C.c_int32),
                                              abi.ptr(w, C.c_double), C.byref(h)), "mbs_po_stage_repeat")
-        st = Staged.__new__(Staged)
-        st._h, st.handle, st.n_sets = self, h, 1
-        n_out = int(len(idx))
-        st.n_orient, st.n_beams, st.n_verts = n_out, src.n_beams, src.n_verts
-        st._src = src
-        return st
+        return Staged(self, h, None, counts=(int(len(idx)), src.n_beams, src.n_verts), source=src)
 
     def restage(self, staged: Staged, batch: BeamBatch) -> Staged:
         """mbs_po_restage: re-fill `staged` with `batch` in the device memory

@@ -22,6 +22,22 @@ import numpy as np
 from . import abi, beams as B
 
 
+def batch_edges(n: int, batch: int) -> list[int]:
+    """Boundaries of the pipeline's batches over n orientations: a quarter
+    batch first, full batches, and the remainder split so that the last
+    batch is at most half a batch."""
+    if n <= batch:
+        return [0, n] if n > 0 else [0]
+    edges = [0, min(n, max(1, batch // 4))]
+    while n - edges[-1] > batch + batch // 2:
+        edges.append(edges[-1] + batch)
+    rest = n - edges[-1]
+    if rest > batch // 2:
+        edges.append(edges[-1] + rest - batch // 2)
+    edges.append(n)
+    return edges
+
+
 def orientation_average(handler, cfg, beta, gamma, weight, precision: int = abi.FP32C,
                         batch: int = 2048, depth: int = 2, noshadow: bool = False):
     """Weighted Mueller sums [n_az, n_zen+1, 16] (and no-shadow sums) of the
@@ -45,10 +61,14 @@ def orientation_average(handler, cfg, beta, gamma, weight, precision: int = abi.
     if cfg.n_threads <= 0:
         cfg = dataclasses.replace(cfg, n_threads=max(1, (os.cpu_count() or 2) - 1))
 
+    # batch boundaries: a short first batch (the device starts sooner) and a
+    # short last one (less device work left once tracing ends), `batch`
+    # orientations in between
+    edges = batch_edges(n, batch)
+
     def producer():
         try:
-            for s in range(0, n, batch):
-                e = min(n, s + batch)
+            for s, e in zip(edges[:-1], edges[1:]):
                 t0 = time.perf_counter()
                 b = B.trace(cfg, beta[s:e], gamma[s:e], weight[s:e])
                 t_trace[0] += time.perf_counter() - t0

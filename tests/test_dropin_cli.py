@@ -120,19 +120,37 @@ def test_dropin_eps1_and_beam_stats_knobs(tmp_path):
 @pytest.mark.gpu
 @pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFCLI)),
                     reason="drop-in or reference CLI not built")
-def test_dropin_theta_groups_reuse_staged_beams(tmp_path):
-    """--so3-quaternion with MBS_GPU_GROUPS=1: the reference's driver
-    diffracts each prepared chunk on several theta-row groups through
-    HandleOrientationsToLocalGpuOnDevice with one packed-beam cache token;
-    the drop-in keeps the staged beams on the device across those calls
-    (cache fill, then hits) and the result equals the reference CLI's CPU
-    result."""
+def test_dropin_variable_phi_so3_matches_reference_cli(tmp_path):
+    """--so3-quaternion: the reference driver's variable-phi averaging, which
+    diffracts each prepared chunk on several theta-row groups with their own
+    azimuth counts (new grids call after call, TracerPOTotal.cpp:6057-6830);
+    the drop-in's result equals the reference CLI's CPU result."""
     args = [a for a in ARGS]
     i = args.index("--sobol")
     args[i:i + 2] = ["--so3-quaternion", "32"]
     ref, ref_i, _ = _run(REFCLI, "cpu", str(tmp_path / "ref"), args=args)
-    gpu, gpu_i, log = _run(DROPIN, "gpu", str(tmp_path / "gpu"),
-                           {"MBS_GPU_TIMING": "1", "MBS_GPU_GROUPS": "1"}, args=args)
-    assert "cache=fill" in log and "cache=hit" in log
+    gpu, gpu_i, log = _run(DROPIN, "gpu", str(tmp_path / "gpu"), {"MBS_GPU_TIMING": "1"}, args=args)
+    assert "path=b200-fp64" in log
     assert gpu.shape == ref.shape
+    np.testing.assert_array_equal(gpu[:, :2], ref[:, :2])
     assert _wl2(gpu, ref) < 1e-7
+    for k in ("Cext", "Csca"):
+        assert abs(float(gpu_i[k]) / float(ref_i[k]) - 1) < 1e-7, k
+
+
+CACHE_CHECK = os.path.join(ROOT, "mbs_fast_b200", "_lib", "mbs_dropin_cache_check")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(CACHE_CHECK), reason="cache check not built")
+def test_dropin_packed_beam_cache():
+    """HandleOrientationsToLocalGpuOnDevice with a cache token (the
+    reference's multi-GPU theta-group path, which a one-GPU CLI run never
+    takes): tests/dropin_cache_check.cpp traces a column with the reference,
+    then fills and hits the cache on two grids and refills it for another
+    range; every result equals the uncached call bit for bit."""
+    env = dict(os.environ, MBS_GPU_TIMING="1")
+    r = subprocess.run([CACHE_CHECK], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
+    assert r.stdout.strip().endswith("OK")
+    assert r.stderr.count("cache=fill") == 2 and r.stderr.count("cache=hit") == 3, r.stderr[-3000:]
