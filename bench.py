@@ -302,7 +302,8 @@ def run_proposal(args):
     the wall time to 1 % is that count times the measured wall time per
     orientation of the whole average with host tracing overlapped (the
     pipeline of the headline line), plus the pilot and the training for the
-    learned estimates.  The network is trained on the rows of --proposal-rows."""
+    learned estimates (16,384 orientations timed per precision).  The network
+    is trained on the rows of --proposal-rows."""
     import torch
     from mbs_fast_b200 import abi, beams as B, proposal as PR, workloads as W
     from mbs_fast_b200.handler import GpuHandlerPO
@@ -326,11 +327,12 @@ def run_proposal(args):
         return PR.averaged_rows(h, b, prec)[0]
 
     # wall time per orientation of the whole average (host tracing
-    # overlapped with the device), per precision, on 4096 orientations
+    # overlapped with the device), per precision, on 16,384 orientations
+    # (the headline line's pipeline)
     per_orient = {}
-    bq, gq, wq = B.sobol_orientations(4096, bs, gs, 7)
+    bq, gq, wq = B.sobol_orientations(16384, bs, gs, 7)
     for prec, name in ((abi.FP64, "fp64"), (abi.FP32C, "fp32c")):
-        orientation_average(h, cfg, bq[:1024], gq[:1024], wq[:1024], precision=prec, batch=1024)
+        orientation_average(h, cfg, bq[:2048], gq[:2048], wq[:2048], precision=prec, batch=1024)
         _, _, tp = orientation_average(h, cfg, bq, gq, wq, precision=prec, batch=1024)
         per_orient[name] = tp["wall_s"] / len(bq)
 

@@ -963,7 +963,8 @@ __device__ __forceinline__ void edge_sums_fixed_f32(const SVertRaw<float> *v, co
 // straight-line code with the beam's A, B and zone tests, so their chains
 // interleave; the tail (the remaining vertices and edges, the closing edge
 // back to vertex 0) follows the warp-uniform switch on the vertex count.
-// Operations and their order are those of edge_sums_fixed_f32.
+// The sums add the edges in edge_sums_fixed_f32's order; consecutive edges
+// share one reciprocal (rcp_pair).
 __device__ __forceinline__ void edge_step_f32(float2 a, float2 b, float slope, float X1, float X2,
                                               float &sr, float &si, float &mn)
 {
@@ -973,6 +974,37 @@ __device__ __forceinline__ void edge_step_f32(float2 a, float2 b, float slope, f
     const float2 df = __ffma2_rn(a, make_float2(-1.f, -1.f), b);
     sr = fmaf(df.x, inv, sr);
     si = fmaf(df.y, inv, si);
+}
+
+// 1/a and 1/b from one reciprocal: r = 1/(a b), 1/a = b r, 1/b = a r (one
+// MUFU instead of two, three more multiplications).  An edge reaches the hot
+// loop's sums only with |a|, |b| > eps (else the pair goes to the FP64 pass),
+// so the product does not underflow.  An invalid edge's coefficient (slope
+// 1e30: about 1e30 |X1|) overflows the product only when the other one
+// exceeds about 3e8; both quotients are then 0 instead of below 1e-30 and
+// 3e-9, terms far below the FP32 rounding of the sum.
+__device__ __forceinline__ void rcp_pair(float a, float b, float &ia, float &ib)
+{
+    const float r = rcp32(a * b);
+    ia = b * r;
+    ib = a * r;
+}
+
+// Two consecutive edges (vertex phasors a -> b -> c, slopes sa, sb) with
+// one reciprocal for both coefficients; otherwise edge_step_f32 twice.
+__device__ __forceinline__ void edge_pair_f32(float2 a, float2 b, float2 c, float sa, float sb, float X1,
+                                              float X2, float &sr, float &si, float &mn)
+{
+    const float ca = fmaf(sa, X1, X2), cb = fmaf(sb, X1, X2);
+    float ia, ib;
+    rcp_pair(ca, cb, ia, ib);
+    mn = fminf(mn, fminf(fabsf(ca), fabsf(cb)));
+    const float2 da = __ffma2_rn(a, make_float2(-1.f, -1.f), b);
+    const float2 db = __ffma2_rn(b, make_float2(-1.f, -1.f), c);
+    sr = fmaf(da.x, ia, sr);
+    si = fmaf(da.y, ia, si);
+    sr = fmaf(db.x, ib, sr);
+    si = fmaf(db.y, ib, si);
 }
 
 template <int DPT>
@@ -1003,8 +1035,8 @@ __device__ __forceinline__ void edge_head_f32(const SVertRaw<float> *v, const do
         mn[d] = 1e30f;
         sr[d] = 0.f;
         si[d] = 0.f;
-        edge_step_f32(h.c0[d], c1[d], useX[d] ? syx0 : sxy0, X1[d], X2[d], sr[d], si[d], mn[d]);
-        edge_step_f32(c1[d], h.c2[d], useX[d] ? syx1 : sxy1, X1[d], X2[d], sr[d], si[d], mn[d]);
+        edge_pair_f32(h.c0[d], c1[d], h.c2[d], useX[d] ? syx0 : sxy0, useX[d] ? syx1 : sxy1, X1[d], X2[d],
+                      sr[d], si[d], mn[d]);
     }
 }
 
@@ -1024,15 +1056,22 @@ __device__ __forceinline__ void edge_tail_fixed_f32(const SVertRaw<float> *v, co
         for (int d = 0; d < DPT; ++d)
             vertex_phasor(st[d], ct[d], w, cs[d][e - 3].y, cs[d][e - 3].x);
     }
+    // edges in pairs (2, 3), (4, 5); an odd last edge alone
 #pragma unroll
-    for (int e = 2; e < NV; ++e) {
+    for (int e = 2; e < NV; e += 2) {
 #pragma unroll
         for (int d = 0; d < DPT; ++d) {
             const float2 a = e == 2 ? h.c2[d] : cs[d][e - 3];
             const float2 b = e + 1 < NV ? cs[d][e - 2] : h.c0[d];
             const float slope = e == 2 ? (useX[d] ? h.syx2 : h.sxy2)
                                        : (useX[d] ? syx[e - 3] : sxy[e - 3]);
-            edge_step_f32(a, b, slope, X1[d], X2[d], sr[d], si[d], mn[d]);
+            if (e + 1 < NV) {
+                const float2 c = e + 2 < NV ? cs[d][e - 1] : h.c0[d];
+                edge_pair_f32(a, b, c, slope, useX[d] ? syx[e - 2] : sxy[e - 2], X1[d], X2[d], sr[d],
+                              si[d], mn[d]);
+            } else {
+                edge_step_f32(a, b, slope, X1[d], X2[d], sr[d], si[d], mn[d]);
+            }
         }
     }
 }
