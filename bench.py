@@ -715,10 +715,10 @@ def run_mlp(args):
 
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) of one
-# full-size FP32C diffraction launch of the headline workload, from the
-# capture summarised in profiles/po_diffract_kernel_f32_traffic_hexcol40x100_16384orient.md
-# (None until measured for the current kernel).
-FP32C_LAUNCH_DRAM_BYTES = None
+# full-size FP32C diffraction launch of the headline workload (16,384
+# orientations), from the capture summarised in
+# profiles/po_diffract_kernel_f32_traffic_hexcol40x100_16384orient.md
+FP32C_LAUNCH_DRAM_BYTES = 2_201_444_096 + 740_194_816
 
 
 def nominal_peaks(clock_mhz: float | None) -> dict:
@@ -904,7 +904,8 @@ def main():
     achieved = flops / kern_s / 1e12
     total_orient = batch.n_orient * world
     value = total_orient / (step_ms * 1e-3)
-    traffic = FP32C_LAUNCH_DRAM_BYTES
+    # the capture's figure holds for the headline batch only
+    traffic = FP32C_LAUNCH_DRAM_BYTES if (batch.n_orient == 16384 and G == 48 * 1801) else None
     roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
                 "traffic": traffic,
