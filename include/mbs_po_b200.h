@@ -383,13 +383,6 @@ int mbs_po_autotune(mbs_po_ctx *ctx, const mbs_po_staged *staged, int precision,
                     int max_orient, int *best, double *ms_out, int ms_len);
 /* Select a launch shape explicitly (0 = default). */
 int mbs_po_set_variant(mbs_po_ctx *ctx, int precision, int variant);
-/* FP32C calls that synchronise (statistics asked for, host-array calls) run
- * the FP64 evaluation of the marked pairs in a second kernel
- * (po_rare_kernel) instead of inside the diffraction kernel; on = 0 keeps it
- * in the kernel (the form every other call uses).  Default on.  The
- * deferred form needs device pools that grow to what a launch asks for (a
- * launch that outgrows them runs again).  No counterpart in the reference. */
-int mbs_po_set_deferred_pass(mbs_po_ctx *ctx, int on);
 
 /* Measured FP32 FMA throughput of the context's device in TFLOP/s (independent
  * FFMA chains on every SM), the denominator of the diffraction kernels'

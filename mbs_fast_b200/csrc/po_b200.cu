@@ -118,16 +118,6 @@ struct mbs_po_ctx {
     int variant[2] = {0, 0};     // chosen launch shape per precision
     // host-side phases of the last host call, ms (mbs_po_last_profile)
     double prof[8] = {};
-    // deferred FP64 pass of the FP32C kernel: pair and cell pools, slot
-    // heads, the 64-bit counters; pools grow to what a launch asked for
-    int2 *rare_pairs = nullptr;
-    size_t pair_cap = 0;
-    double *rare_cells = nullptr;
-    size_t cell_cap = 0;
-    int *rare_heads = nullptr;
-    size_t heads_cap = 0;
-    unsigned long long *rare_count = nullptr;   // [3]
-    bool defer = true;           // mbs_po_set_deferred_pass
 };
 
 namespace {
@@ -349,10 +339,6 @@ extern "C" int mbs_po_destroy(mbs_po_ctx *ctx)
         cudaStreamSynchronize(ctx->side);
     grid_release(ctx->grid);
     cudaFree(ctx->partial);
-    cudaFree(ctx->rare_pairs);
-    cudaFree(ctx->rare_cells);
-    cudaFree(ctx->rare_heads);
-    cudaFree(ctx->rare_count);
     cudaFree(ctx->macc);
     cudaFree(ctx->mfull);
     cudaFree(ctx->phiW);
@@ -666,10 +652,10 @@ LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ct
 
 // Persistent launch: as many CTAs as fit on the device at once (at most one
 // per work item); P.work must be zero on `st` when the kernel starts.
-template <typename T, int TPB, int DPT, bool NS, int MINB, bool DEFER = false>
+template <typename T, int TPB, int DPT, bool NS, int MINB>
 cudaError_t launch_one(const KParams &P, cudaStream_t st)
 {
-    auto kern = po_diffract_kernel<T, TPB, DPT, NS, MINB, DEFER>;
+    auto kern = po_diffract_kernel<T, TPB, DPT, NS, MINB>;
     const size_t smem = diffract_smem_bytes<T, TPB, DPT, NS>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess)
@@ -681,34 +667,13 @@ cudaError_t launch_one(const KParams &P, cudaStream_t st)
         return e;
     const int ctas = std::max(1, std::min(P.n_items, sms * std::max(per_sm, 1)));
     kern<<<ctas, TPB, smem, st>>>(P);
-    if ((e = cudaGetLastError()) != cudaSuccess)
-        return e;
-    if constexpr (DEFER) {
-        // the deferred cells, after the diffraction kernel on the same stream
-        const long long n = (long long)P.n_items * TPB * DPT;
-        const int rb = 128;
-        const int rg = (int)std::max<long long>(1, std::min<long long>((n + rb - 1) / rb, (long long)sms * 16));
-        po_rare_kernel<TPB, DPT><<<rg, rb, 0, st>>>(P);
-        e = cudaGetLastError();
-    }
-    return e;
+    return cudaGetLastError();
 }
 
 // The cases follow kVariantsF64 / kVariantsF32 entry by entry; no-shadow
 // sums use kNoShadowF64 / kNoShadowF32.
-cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &P, cudaStream_t st,
-                            bool defer = false)
+cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &P, cudaStream_t st)
 {
-    if (defer && precision == MBS_PO_FP32C && !ns) {
-        switch (variant) {
-        case 1: return launch_one<float, 64, 3, false, 5, true>(P, st);
-        case 2: return launch_one<float, 128, 3, false, 3, true>(P, st);
-        case 3: return launch_one<float, 96, 2, false, 5, true>(P, st);
-        case 4: return launch_one<float, 128, 2, false, 4, true>(P, st);
-        case 5: return launch_one<float, 64, 3, false, 4, true>(P, st);
-        default: return launch_one<float, 64, 3, false, 6, true>(P, st);
-        }
-    }
     if (precision == MBS_PO_FP64) {
         if (ns)
             return launch_one<double, 128, 1, true, 4>(P, st);
@@ -801,32 +766,6 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     P.partial_ns = ns ? ctx->partial + plane * L.n_chunks : nullptr;
     P.work = ctx->d_status + 1;
     P.n_items = L.n_chunks * nAz * L.tiles_per_row;
-    // The FP32C kernel defers its FP64 pass to po_rare_kernel when the call
-    // synchronises anyway (statistics asked for): the pools' counters are
-    // read back after the two kernels, and a launch that ran out of pool is
-    // run again with pools of the size it asked for.
-    bool defer = ctx->defer && precision == MBS_PO_FP32C && !ns && stats != nullptr;
-    P.rare_pairs = nullptr;
-    P.rare_cells = nullptr;
-    P.rare_heads = nullptr;
-    P.rare_count = nullptr;
-    P.pair_cap = P.cell_cap = 0;
-    if (defer) {
-        const size_t heads = (size_t)P.n_items * V.tpb * V.dpt;
-        if ((rc = ensure(ctx, ctx->rare_heads, ctx->heads_cap, heads, "deferred-pass heads"))
-            || (rc = ensure(ctx, ctx->rare_pairs, ctx->pair_cap, std::max<size_t>(ctx->pair_cap, (size_t)1 << 24),
-                            "deferred-pass pairs"))
-            || (rc = ensure(ctx, ctx->rare_cells, ctx->cell_cap, std::max<size_t>(ctx->cell_cap, (size_t)1 << 24) ,
-                            "deferred-pass cells"))) {
-            cudaGetLastError();
-            defer = false;     // no room: the FP64 pass stays in the kernel
-        }
-        if (defer && !ctx->rare_count) {
-            size_t cap = 0;
-            if (ensure(ctx, ctx->rare_count, cap, 3, "deferred-pass counters"))
-                defer = false;
-        }
-    }
     int launches = 0;
     CK(cudaEventRecord(ctx->ev[0], st), "event");
     // polar rows on the side stream, concurrently with the main kernel
@@ -841,41 +780,11 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
         CK(cudaEventRecord(ctx->ev[6], ctx->side), "event");
         ++launches;
     }
-    for (;;) {
-        if (defer) {
-            P.rare_pairs = ctx->rare_pairs;
-            P.rare_cells = ctx->rare_cells;
-            P.rare_heads = ctx->rare_heads;
-            P.rare_count = ctx->rare_count;
-            P.pair_cap = (long long)std::min<size_t>(ctx->pair_cap, (size_t)INT32_MAX);
-            P.cell_cap = (long long)std::min<size_t>(ctx->cell_cap / kCellWords, (size_t)INT32_MAX);
-            CK(cudaMemsetAsync(ctx->rare_count, 0, 3 * sizeof(unsigned long long), st), "memset counters");
-        }
-        CK(cudaMemsetAsync(P.work, 0, sizeof(int), st), "memset work counter");
-        const cudaError_t e = launch_diffract(precision, variant, ns, P, st, defer);
-        if (e != cudaSuccess)
-            return cuda_fail(ctx, e, "diffraction kernel launch");
-        launches += defer ? 2 : 1;
-        if (!defer)
-            break;
-        unsigned long long cnt[3] = {0, 0, 0};
-        CK(cudaMemcpyAsync(cnt, ctx->rare_count, sizeof(cnt), cudaMemcpyDeviceToHost, st), "D2H counters");
-        CK(cudaStreamSynchronize(st), "deferred-pass sync");
-        if (!cnt[2])
-            break;
-        // out of pool: grow to what the launch asked for (and a quarter
-        // more) and run it again; beyond 2^31 entries, or without the
-        // memory, run it with the FP64 pass in the kernel
-        const size_t want_pairs = (size_t)(cnt[0] + cnt[0] / 4 + 1024);
-        const size_t want_cells = (size_t)(cnt[1] + cnt[1] / 4 + 1024) * kCellWords;
-        if (want_pairs > (size_t)INT32_MAX || want_cells / kCellWords > (size_t)INT32_MAX
-            || ensure(ctx, ctx->rare_pairs, ctx->pair_cap, want_pairs, "deferred-pass pairs")
-            || ensure(ctx, ctx->rare_cells, ctx->cell_cap, want_cells, "deferred-pass cells")) {
-            cudaGetLastError();
-            defer = false;
-        }
-        CK(cudaEventRecord(ctx->ev[0], st), "event");
-    }
+    CK(cudaMemsetAsync(P.work, 0, sizeof(int), st), "memset work counter");
+    const cudaError_t e = launch_diffract(precision, variant, ns, P, st);
+    if (e != cudaSuccess)
+        return cuda_fail(ctx, e, "diffraction kernel launch");
+    ++launches;
     if (ctx->grid.n_pole > 0)
         CK(cudaStreamWaitEvent(st, ctx->ev[6], 0), "join side stream");
     CK(cudaEventRecord(ctx->ev[1], st), "event");
@@ -941,14 +850,6 @@ extern "C" int mbs_po_autotune(mbs_po_ctx *ctx, const mbs_po_staged *s, int prec
     ctx->variant[pi] = bestv;
     if (best)
         *best = bestv;
-    return MBS_PO_OK;
-}
-
-extern "C" int mbs_po_set_deferred_pass(mbs_po_ctx *ctx, int on)
-{
-    if (!ctx)
-        return MBS_PO_EINVAL;
-    ctx->defer = on != 0;
     return MBS_PO_OK;
 }
 

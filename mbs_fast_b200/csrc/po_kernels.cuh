@@ -140,21 +140,7 @@ struct KParams {
     WaveConst wc;
     double *partial;           // [n_chunks][16][G]
     double *partial_ns;        // [n_chunks][16][G] or null
-    // Deferred FP64 pass (FP32C kernels with DEFER): the marked pairs and the
-    // Jones sums of their (orientation, direction) cells, handed to
-    // po_rare_kernel.  rare_count: [0] pairs taken, [1] cells taken, [2] set
-    // when either pool ran out (nothing was written past its end).
-    int2 *rare_pairs;          // [pair_cap] (global beam index, next pair of the cell or -1)
-    double *rare_cells;        // [cell_cap][kCellWords]
-    int *rare_heads;           // [n_items * directions per item] last cell of the slot, -1: none
-    unsigned long long *rare_count;   // [3], 64-bit so that requests past the pools never wrap
-    long long pair_cap, cell_cap;
 };
-
-// A deferred cell (orientation o, direction of one slot): word 0 holds
-// (o, previous cell of the slot or -1), word 1 (first pair or -1, 0), words
-// 2-9 the hot loop's Jones sum (Kahan sum minus compensation, FP64).
-constexpr int kCellWords = 10;
 
 // Orientation range [o0, o1) of an orientation chunk; chunks never span
 // two output sets.
@@ -1324,20 +1310,13 @@ struct JonesAcc {
 // (orientation chunk, azimuth bin, zenith tile) from a global counter.  Each
 // thread owns DPT directions of an item (zenith rows t0 + d*TPB of the
 // item's azimuth).  T = float selects FP32C.
-// DEFER (FP32C without no-shadow sums only): the marked pairs are not
-// evaluated here; each thread lists them per (orientation, direction) cell
-// in P.rare_pairs, a cell with marked pairs adds no Mueller matrix to the
-// partial plane (its first orientation stores zero instead) and leaves its
-// hot-loop Jones sum in P.rare_cells, and po_rare_kernel completes the cells
-// in FP64 afterwards.  The kernel then holds none of the FP64 pass's code.
-template <typename T, int TPB, int DPT, bool NS, int MINB, bool DEFER = false>
+template <typename T, int TPB, int DPT, bool NS, int MINB>
 __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
 {
     using Cfg = StageCfg<T, TPB>;
     constexpr int kDirs = TPB * DPT;
     constexpr bool kF32 = sizeof(T) == 4;
     constexpr int kSets = NS ? 2 : 1;        // full and no-shadow sums
-    static_assert(!DEFER || (kF32 && !NS), "the deferred pass serves FP32C without no-shadow sums");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SBeamRaw<T> *sb = reinterpret_cast<SBeamRaw<T> *>(smem_raw);
     SVertRaw<T> *sv = reinterpret_cast<SVertRaw<T> *>(smem_raw + Cfg::kBeams * sizeof(SBeamRaw<T>));
@@ -1355,7 +1334,6 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
     __shared__ int s_item;
     __shared__ double s_zdel[TPB / 32];
     __shared__ int s_rwarp[TPB / 32], s_rbase[TPB], s_rok[TPB];   // the spread FP64 pass
-    __shared__ unsigned long long s_take, s_ctake;                  // DEFER: first pool slots taken
 
     // Persistent: take work items until none are left, so CTAs of uneven
     // cost (rare FP64 pairs, ragged beam counts) balance across the SMs.
@@ -1414,19 +1392,8 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
             s_zdel[threadIdx.x >> 5] = dd;
     }
 
-    // DEFER: the slot's last deferred cell (item-wide) and, per orientation,
-    // the cell's last listed pair
-    int hcell[DEFER ? DPT : 1];
-#pragma unroll
-    for (int d = 0; d < (DEFER ? DPT : 1); ++d)
-        hcell[d] = -1;
-
     for (int o = o0; o < o1; ++o) {
         JonesAcc<T> J[DPT], Jn[NS ? DPT : 1];
-        int hpair[DEFER ? DPT : 1];
-#pragma unroll
-        for (int d = 0; d < (DEFER ? DPT : 1); ++d)
-            hpair[d] = -1;
 #pragma unroll
         for (int d = 0; d < DPT; ++d) {
             J[d].zero();
@@ -1611,57 +1578,6 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                 }
             }
             }
-            if constexpr (DEFER) {
-                // list the stage's marked pairs: each thread's pairs take
-                // consecutive slots of the pair pool (one reservation per
-                // stage for the CTA, numbered owner by owner), each pair
-                // linked to the previous one of its cell
-                const int words = (nb + 31) >> 5;
-                const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-                int cnt = 0;
-#pragma unroll
-                for (int d = 0; d < DPT; ++d)
-                    for (int w = 0; w < words; ++w)
-                        cnt += __popc(rmask[(d * kMaskWords + w) * TPB + threadIdx.x]);
-                int incl = cnt;
-#pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const int v = __shfl_up_sync(0xffffffffu, incl, off);
-                    if (lane >= off)
-                        incl += v;
-                }
-                if (lane == 31)
-                    s_rwarp[warp] = incl;
-                __syncthreads();   // warp totals visible
-                int base = incl - cnt, total = 0;
-#pragma unroll
-                for (int w2 = 0; w2 < TPB / 32; ++w2) {
-                    const int v = s_rwarp[w2];
-                    base += w2 < warp ? v : 0;
-                    total += v;
-                }
-                if (threadIdx.x == 0)
-                    s_take = total > 0 ? atomicAdd(P.rare_count, (unsigned long long)total) : 0ull;
-                __syncthreads();   // s_take visible; s_rwarp free again
-                const unsigned long long take = s_take;
-                if (total > 0 && take + (unsigned long long)total > (unsigned long long)P.pair_cap) {
-                    if (threadIdx.x == 0)
-                        atomicExch(P.rare_count + 2, 1ull);   // pool exhausted: nothing written
-                } else if (cnt > 0) {
-                    int k = (int)take + base;   // < pair_cap <= INT_MAX
-#pragma unroll
-                    for (int d = 0; d < DPT; ++d)
-                        for (int w = 0; w < words; ++w) {
-                            uint32_t m = rmask[(d * kMaskWords + w) * TPB + threadIdx.x];
-                            while (m) {
-                                const int j = w * 32 + __ffs(m) - 1;
-                                m &= m - 1;
-                                P.rare_pairs[k] = make_int2(bs + j, hpair[d]);
-                                hpair[d] = k++;
-                            }
-                        }
-                }
-            } else {
             // FP64 pass over the stage's marked pairs, spread over all the
             // CTA's threads: a pair's owner (the thread whose direction it
             // is) seldom has company in its warp, so per-owner loops left most
@@ -1777,7 +1693,6 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                     __syncthreads();   // the slots are read before the next round
                 }
             }
-            }   // DEFER
             if (kF32) {
 #pragma unroll
                 for (int d = 0; d < DPT; ++d) {
@@ -1795,64 +1710,10 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
         // The adds are reductions performed in L2 (no load on the thread's
         // path); each partial element has a single owner thread, whose adds
         // reach it in program order, so the sums are deterministic.
-        if constexpr (DEFER) {
-            // the cells with listed pairs go to po_rare_kernel: their Jones
-            // sums and pair lists, one cell slot each (CTA-wide reservation)
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-            int cnt = 0;
-#pragma unroll
-            for (int d = 0; d < DPT; ++d)
-                cnt += hpair[d] >= 0 ? 1 : 0;
-            int incl = cnt;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, incl, off);
-                if (lane >= off)
-                    incl += v;
-            }
-            if (lane == 31)
-                s_rwarp[warp] = incl;
-            __syncthreads();
-            int base = incl - cnt, total = 0;
-#pragma unroll
-            for (int w2 = 0; w2 < TPB / 32; ++w2) {
-                const int v = s_rwarp[w2];
-                base += w2 < warp ? v : 0;
-                total += v;
-            }
-            if (threadIdx.x == 0)
-                s_ctake = total > 0 ? atomicAdd(P.rare_count + 1, (unsigned long long)total) : 0ull;
-            __syncthreads();
-            const unsigned long long take = s_ctake;
-            const bool room = total == 0 || take + (unsigned long long)total <= (unsigned long long)P.cell_cap;
-            if (!room && threadIdx.x == 0)
-                atomicExch(P.rare_count + 2, 1ull);   // pool exhausted: nothing written
-            if (room && cnt > 0) {
-                int k = (int)take + base;   // < cell_cap <= INT_MAX
-#pragma unroll
-                for (int d = 0; d < DPT; ++d) {
-                    if (hpair[d] < 0)
-                        continue;
-                    double *c = P.rare_cells + (size_t)k * kCellWords;
-                    const float *sk = Ksm + d * TPB + threadIdx.x;
-                    c[0] = __hiloint2double(hcell[d], o);
-                    c[1] = __hiloint2double(0, hpair[d]);
-#pragma unroll
-                    for (int i = 0; i < 8; ++i)
-                        c[2 + i] = (double)sk[i * kDirs] - (double)sk[(8 + i) * kDirs];
-                    hcell[d] = k++;
-                }
-            }
-        }
         const double wgt = P.weight[o] * 0.25;
 #pragma unroll
         for (int d = 0; d < DPT; ++d) {
             if (!active[d])
-                continue;
-            // DEFER: a cell with listed pairs adds nothing here (po_rare_kernel
-            // adds it); as the chunk's first orientation it stores zero
-            const bool deferred = DEFER && hpair[DEFER ? d : 0] >= 0;
-            if (deferred && o != o0)
                 continue;
             const int slot = d * TPB + threadIdx.x;
             const size_t g = (size_t)p * P.n_t + t[d];
@@ -1872,8 +1733,7 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
 #pragma unroll
                 for (int i = 0; i < 16; ++i)
                     m[i] = 0.0;
-                if (!deferred)
-                    mueller_add(j, wgt, m);
+                mueller_add(j, wgt, m);
                 double *out = (set == 0 ? P.partial : P.partial_ns) + (size_t)chunk * 16 * G + g;
                 if (o == o0) {
 #pragma unroll
@@ -1887,106 +1747,7 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
             }
         }
     }
-    if constexpr (DEFER) {
-        // the slots' last deferred cells, every slot of the item (-1: none)
-#pragma unroll
-        for (int d = 0; d < DPT; ++d)
-            P.rare_heads[(size_t)item * kDirs + d * TPB + threadIdx.x] = hcell[d];
-    }
     }   // work items
-}
-
-// Completes the cells that the FP32C kernel deferred (DEFER).  One thread per
-// (work item, direction slot) walks the slot's cells (its orientations in
-// reverse order): each listed pair's FP64 contribution (beam_rare /
-// beam_sing, on the beam and vertex records built as the stage fill builds
-// them, in local memory) is added to the cell's Jones sum, which becomes the
-// cell's weighted Mueller matrix; the slot's sum over its cells is then added
-// to the chunk's partial plane.  Each partial element has this one owner,
-// after the diffraction kernel, so the sums are deterministic.
-template <int TPB, int DPT>
-__global__ void __launch_bounds__(128) po_rare_kernel(KParams P)
-{
-    constexpr int kDirs = TPB * DPT;
-    const int items_per_chunk = P.n_az * P.tiles_per_row;
-    const size_t G = (size_t)P.n_az * P.n_t;
-    const long long n = (long long)P.n_items * kDirs;
-    SVertRaw<float> sv[kMaxNv + 1];
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
-         idx += (long long)gridDim.x * blockDim.x) {
-        int c = P.rare_heads[idx];
-        if (c < 0)
-            continue;
-        const int item = (int)(idx / kDirs), slot = (int)(idx - (long long)item * kDirs);
-        const int chunk = item / items_per_chunk;
-        const int pt = item - chunk * items_per_chunk;
-        const int p = pt / P.tiles_per_row;
-        const int tile = pt - p * P.tiles_per_row;
-        const int d = slot / TPB;
-        const int t = tile * kDirs + d * TPB + (slot - d * TPB);   // < n_t: only active slots have cells
-        const double cp = P.cphi[p], sp = P.sphi[p];
-        const double st = P.st[t], ct = P.ct[t];
-        const float stT = (float)st, ctT = (float)ct;
-        const bool gen = P.row_kind[t] == 2;
-        const TileZone tz = {st, ct, 0.0};
-        double acc[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-            acc[i] = 0.0;
-        while (c >= 0) {
-            const double *cell = P.rare_cells + (size_t)c * kCellWords;
-            const int o = __double2loint(cell[0]);
-            const int prev = __double2hiint(cell[0]);
-            int q = __double2loint(cell[1]);
-            double j[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-                j[i] = cell[2 + i];
-            while (q >= 0) {
-                const int2 pr = P.rare_pairs[q];
-                const int gb = pr.x;
-                SBeamRaw<float> rec;
-                fill_beam(BrecRef{P.brec + gb, P.brec_stride}, cp, sp, 0, gb, tz, rec);
-                BeamRegs<float> b;
-                load_beam(rec, b);
-                // the tests of the kernel's FP64 pass, on the same FP32 values
-                const float A = fmaf(stT, b.a[0], fmaf(ctT, b.a[1], b.a[2]));
-                const float B = fmaf(stT, b.a[3], fmaf(ctT, b.a[4], b.a[5]));
-                const bool near = !gen && (float)(A * A + B * B) <= b.nearr2;
-                const bool cand = fabsf(fmaf(A, b.slab[0], B * b.slab[1])) <= 1.f
-                               && fabsf(fmaf(A, b.slab[2], B * b.slab[3])) <= 1.f;
-                float out[8];
-                bool ok;
-                if (gen || near || cand) {
-                    ok = beam_rare<float>(P, gb, &rec, p, t, near, out, 1);
-                } else {
-                    const int vg = P.vbeg[gb];
-                    for (int v = 0; v < b.nv; ++v)
-                        fill_vert(VrecRef{P.vrec + vg + v, P.vrec_stride}, cp, sp, sv[v]);
-                    ok = beam_sing<float>(P, &rec, sv, vg, st, ct, out, 1);
-                }
-                if (ok) {
-#pragma unroll
-                    for (int i = 0; i < 8; ++i)
-                        j[i] += (double)out[i];
-                }
-                q = pr.y;
-            }
-            double m[16];
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-                m[i] = 0.0;
-            mueller_add(j, P.weight[o] * 0.25, m);
-#pragma unroll
-            for (int i = 0; i < 16; ++i)
-                acc[i] += m[i];
-            c = prev;
-        }
-        double *outp = P.partial + (size_t)chunk * 16 * G + (size_t)p * P.n_t + t;
-#pragma unroll
-        for (int i = 0; i < 16; ++i)
-            outp[i * G] += acc[i];
-    }
 }
 
 template <typename T, int TPB, int DPT, bool NS>

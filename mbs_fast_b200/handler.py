@@ -59,7 +59,6 @@ def lib() -> C.CDLL:
         L.mbs_po_probe_fp64_peak.argtypes = [vp, abi._dp]
         L.mbs_po_autotune.argtypes = [vp, vp, C.c_int, C.c_int, C.POINTER(C.c_int), abi._dp, C.c_int]
         L.mbs_po_set_variant.argtypes = [vp, C.c_int, C.c_int]
-        L.mbs_po_set_deferred_pass.argtypes = [vp, C.c_int]
         L.mbs_po_diffract_staged_noalloc.argtypes = [vp, vp, C.c_int, C.c_void_p, C.c_void_p,
                                                      C.c_void_p]
         L.mbs_po_diffract_multisize.argtypes = [vp, C.POINTER(abi.Beams), abi._dp, C.c_int,
@@ -391,11 +390,6 @@ class GpuHandlerPO:
 
     def set_variant(self, precision: int, variant: int) -> None:
         self._call(lib().mbs_po_set_variant(self.ctx, precision, variant), "mbs_po_set_variant")
-
-    def set_deferred_pass(self, on: bool) -> None:
-        """mbs_po_set_deferred_pass: FP32C's FP64 pass in a second kernel
-        (synchronising calls) or inside the diffraction kernel."""
-        self._call(lib().mbs_po_set_deferred_pass(self.ctx, int(on)), "mbs_po_set_deferred_pass")
 
     # -- device-resident path -------------------------------------------------
     def stage(self, batch: BeamBatch) -> Staged:

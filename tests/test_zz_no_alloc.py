@@ -106,9 +106,6 @@ def test_noalloc_allocates_nothing_on_a_fresh_handler():
     free1, _ = torch.cuda.mem_get_info()
     assert free1 == free0
     ref = torch.zeros_like(out)
-    # like for like: the allocating path with its FP64 pass inside the
-    # kernel, as the allocation-free path runs it
-    h.set_deferred_pass(False)
     h.diffract_staged(staged, ref.data_ptr(), precision=abi.FP32C)
     torch.cuda.synchronize()
     got, want = out.cpu().numpy(), ref.cpu().numpy()
