@@ -14,7 +14,7 @@ square, and sampled by a 2-D inverse transform of scrambled Sobol points.
 Every sample carries the importance weight p0 / g / N, so the weighted sum
 (which the diffraction kernels compute with these weights as orientation
 weights) is an unbiased estimate of the same average.  The plain Sobol
-average remains the fallback (used when the fit is poor) and the judge of the
+average remains the fallback (used when the fit is poor) and the measure of the
 error.
 """
 from __future__ import annotations
@@ -125,7 +125,7 @@ def uniform_proposal(cells: int = 128) -> Proposal:
 
 
 def plain_sobol(n: int, seed: int = 0):
-    """Plain quasi-random points with equal weights (the fallback and judge)."""
+    """Plain quasi-random points with equal weights (the fallback and the error reference)."""
     from scipy.stats import qmc
     s = qmc.Sobol(d=2, scramble=True, seed=seed).random(n)
     return s[:, 0], s[:, 1], np.full(n, 1.0 / n)
