@@ -393,20 +393,6 @@ __global__ void k_refresh(const float *params, bf16 *w1p, bf16 *w2, bf16 *w3)
     }
 }
 
-__global__ void k_adam(float *p, const float *g, float *m, float *v, int n, float lr, float bc1,
-                       float bc2)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    const float gi = g[i];
-    const float mi = 0.9f * m[i] + 0.1f * gi;
-    const float vi = 0.999f * v[i] + 0.001f * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
-}
-
 // Mean-squared loss of n samples, one CTA, fixed-order tree sum.
 __global__ void __launch_bounds__(256) k_loss(const float *y, const float *t, int n, float *out)
 {
@@ -427,16 +413,45 @@ __global__ void __launch_bounds__(256) k_loss(const float *y, const float *t, in
         *out = red[0] / (float)max(n, 1);
 }
 
-// q_b[i] = q[idx[i]], t_b[i] = t[idx[i]].
-__global__ void k_gather(const float *q, const float *t, const int *idx, int n, float *qb, float *tb)
+// q_b[i] = q[idx[*cursor + i]], t_b[i] = t[idx[*cursor + i]]: the training
+// step's minibatch, at the position in the shuffled order that the device
+// cursor holds (so one captured epoch replays over every epoch's order).
+__global__ void k_gather(const float *q, const float *t, const int *idx, const int *cursor, int n,
+                         float *qb, float *tb)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    const int s = idx[i];
+    const int s = idx[*cursor + i];
     for (int c = 0; c < kIn; ++c)
         qb[i * kIn + c] = q[s * kIn + c];
     tb[i] = t[s];
+}
+
+// Adam with the bias corrections of the step the device counter holds
+// (bc[2 k], bc[2 k + 1] for the call's k-th step).
+__global__ void k_adam_step(float *p, const float *g, float *m, float *v, int n, float lr,
+                            const float *bc, const int *stepc)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int k = *stepc;
+    const float bc1 = bc[2 * k], bc2 = bc[2 * k + 1];
+    const float gi = g[i];
+    const float mi = 0.9f * m[i] + 0.1f * gi;
+    const float vi = 0.999f * v[i] + 0.001f * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
+}
+
+// End of a training step: the cursor moves past the minibatch, the step
+// counter by one.
+__global__ void k_advance(int *cursor, int *stepc, int nb)
+{
+    *cursor += nb;
+    *stepc += 1;
 }
 
 inline int pad_rows(int n) { return (n + kTile - 1) / kTile * kTile; }
@@ -535,14 +550,23 @@ int check_err(mbs_mlp *net)
     return 0;
 }
 
+// The GEMM kernels' dynamic shared-memory limit, set once per process
+// (before any graph capture: the training epoch is captured).
+void gemm_attrs()
+{
+    static bool done = false;
+    if (!done) {
+        cudaFuncSetAttribute(k_gemm<kModeFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+        cudaFuncSetAttribute(k_gemm<kModeBwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+        cudaFuncSetAttribute(k_gemm<kModeF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
+        done = true;
+    }
+}
+
 template <int MODE>
 void gemm(cudaStream_t s, int M, int N, int K, Mat A, Mat B, GemmOut o, Watch w)
 {
-    static bool attr = false;   // the dynamic shared-memory limit, once per instantiation
-    if (!attr) {
-        cudaFuncSetAttribute(k_gemm<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
-        attr = true;
-    }
+    gemm_attrs();
     k_gemm<MODE><<<tiles(M, N), kGemmThreads, kGemmSmem, s>>>(M, N, K, A, B, o, w);
 }
 
@@ -761,15 +785,30 @@ extern "C" int mbs_mlp_train(mbs_mlp *net, const float *q, const float *t, int n
     if (rc)
         return rc;
     cudaStream_t s = net->stream;
-    float *dq = nullptr, *dt = nullptr;
-    int *didx = nullptr;
-    auto cleanup = [&]() { cudaFree(dq); cudaFree(dt); cudaFree(didx); };
+    // one epoch's steps: minibatches of `batch`, the last one shorter
+    std::vector<int> sizes;
+    for (int b0 = 0; b0 < n; b0 += batch)
+        sizes.push_back(std::min(batch, n - b0));
+    const size_t steps = (size_t)epochs * sizes.size();
+    float *dq = nullptr, *dt = nullptr, *dbc = nullptr;
+    int *didx = nullptr, *dstate = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto cleanup = [&]() {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (graph)
+            cudaGraphDestroy(graph);
+        cudaFree(dq); cudaFree(dt); cudaFree(didx); cudaFree(dbc); cudaFree(dstate);
+    };
     if (cudaMalloc((void **)&dq, (size_t)n * kIn * 4) || cudaMalloc((void **)&dt, (size_t)n * 4)
-        || cudaMalloc((void **)&didx, (size_t)epochs * n * 4 + 4)) {
+        || cudaMalloc((void **)&didx, (size_t)epochs * n * 4 + 4)
+        || cudaMalloc((void **)&dbc, steps * 2 * 4 + 8) || cudaMalloc((void **)&dstate, 8)) {
         cleanup();
         return mfail(net, -4, "cudaMalloc training set");
     }
-    // the shuffled order of every epoch, uploaded once
+    // the shuffled order of every epoch and every step's Adam bias
+    // corrections, uploaded once
     std::vector<int> order((size_t)epochs * n);
     std::mt19937_64 rng(seed);
     std::vector<int> perm(n);
@@ -779,28 +818,63 @@ extern "C" int mbs_mlp_train(mbs_mlp *net, const float *q, const float *t, int n
         std::shuffle(perm.begin(), perm.end(), rng);
         std::copy(perm.begin(), perm.end(), order.begin() + (size_t)e * n);
     }
+    std::vector<float> bc(steps * 2 + 2);
+    for (size_t k = 0; k < steps; ++k) {
+        const float step = (float)(net->step + 1 + (long long)k);
+        bc[2 * k] = 1.f - std::pow(0.9f, step);
+        bc[2 * k + 1] = 1.f - std::pow(0.999f, step);
+    }
+    const int zero2[2] = {0, 0};
     cudaError_t e = cudaMemcpyAsync(dq, q, (size_t)n * kIn * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(dt, t, (size_t)n * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess && epochs > 0)
         e = cudaMemcpyAsync(didx, order.data(), order.size() * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && epochs > 0)
+        e = cudaMemcpyAsync(dbc, bc.data(), steps * 2 * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dstate, zero2, 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);   // the host arrays are read before they go
     if (e != cudaSuccess) {
         cleanup();
         return mfail(net, -3, std::string("training upload: ") + cudaGetErrorString(e));
     }
-    for (int ep = 0; ep < epochs && rc == 0; ++ep) {
-        for (int b0 = 0; b0 < n && rc == 0; b0 += batch) {
-            const int nb = std::min(batch, n - b0);
-            k_gather<<<(nb + 127) / 128, 128, 0, s>>>(dq, dt, didx + (size_t)ep * n + b0, nb, net->q, net->t);
-            if ((rc = forward_dev(net, nb)) || (rc = backward_dev(net, nb)))
-                break;
-            ++net->step;
-            const float bc1 = 1.f - std::pow(0.9f, (float)net->step);
-            const float bc2 = 1.f - std::pow(0.999f, (float)net->step);
-            k_adam<<<(kNParams + 255) / 256, 256, 0, s>>>(net->params, net->grad, net->m, net->v,
-                                                          kNParams, lr, bc1, bc2);
-            rc = refresh(net);
+    // One epoch (every minibatch: gather, forward, backward, Adam, BF16
+    // weight copies, cursor advance) captured once as a graph and replayed
+    // per epoch: about twenty small launches per step would otherwise bound
+    // the training by launch latency.
+    if (epochs > 0) {
+        gemm_attrs();
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            for (const int nb : sizes) {
+                k_gather<<<(nb + 127) / 128, 128, 0, s>>>(dq, dt, didx, dstate, nb, net->q, net->t);
+                if ((rc = forward_dev(net, nb)) || (rc = backward_dev(net, nb)))
+                    break;
+                k_adam_step<<<(kNParams + 255) / 256, 256, 0, s>>>(net->params, net->grad, net->m,
+                                                                   net->v, kNParams, lr, dbc,
+                                                                   dstate + 1);
+                if ((rc = refresh(net)))
+                    break;
+                k_advance<<<1, 1, 0, s>>>(dstate, dstate + 1, nb);
+            }
+            const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+            if (e == cudaSuccess)
+                e = ec;
         }
+        if (e == cudaSuccess && rc == 0)
+            e = cudaGraphInstantiate(&exec, graph, 0);
+        for (int ep = 0; ep < epochs && e == cudaSuccess && rc == 0; ++ep)
+            e = cudaGraphLaunch(exec, s);
+        if (e != cudaSuccess || rc) {
+            cudaGetLastError();
+            cleanup();
+            if (rc)
+                return rc;
+            return mfail(net, -3, std::string("training graph: ") + cudaGetErrorString(e));
+        }
+        net->step += (int)steps;
     }
     if (rc == 0 && final_loss) {
         // loss over the whole set with the trained parameters

@@ -874,6 +874,45 @@ __device__ __forceinline__ void vertex_phasor(double st, double ct, const VertRe
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
 }
 
+// The same for two directions of one vertex: the two reductions to the
+// angle in one FFMA2 (each lane rounds as the FFMA above, so the phasors are
+// bitwise those of two single calls).
+__device__ __forceinline__ void vertex_phasor2(double st0, double ct0, double st1, double ct1,
+                                               const VertRegs &w, float2 &cs0, float2 &cs1)
+{
+    const double t0 = fma(st0, w.ps, fma(ct0, w.pc, w.p0));
+    const double t1 = fma(st1, w.ps, fma(ct1, w.pc, w.p0));
+    const unsigned lo0 = (unsigned)__double2loint(t0), lo1 = (unsigned)__double2loint(t1);
+    const float2 y = make_float2(__int_as_float(0x3F800000u | (lo0 & 0x007FFFFFu)),
+                                 __int_as_float(0x3F800000u | (lo1 & 0x007FFFFFu)));
+    const float2 x = __ffma2_rn(y, make_float2(6.28318530717958647f, 6.28318530717958647f),
+                                make_float2(-9.42477796076937972f, -9.42477796076937972f));
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(cs0.y) : "f"(x.x));
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(cs0.x) : "f"(x.x));
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(cs1.y) : "f"(x.y));
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(cs1.x) : "f"(x.y));
+}
+
+// Phasors (cos, sin) of one vertex for a thread's DPT directions, handed to
+// out(d, phasor): directions in pairs, an odd last one alone.
+template <int DPT, typename Out>
+__device__ __forceinline__ void vertex_phasors(const double *st, const double *ct, const VertRegs &w,
+                                               Out &&out)
+{
+#pragma unroll
+    for (int d = 0; d + 1 < DPT; d += 2) {
+        float2 a, b;
+        vertex_phasor2(st[d], ct[d], st[d + 1], ct[d + 1], w, a, b);
+        out(d, a);
+        out(d + 1, b);
+    }
+    if (DPT & 1) {
+        float2 c;
+        vertex_phasor(st[DPT - 1], ct[DPT - 1], w, c.y, c.x);
+        out(DPT - 1, c);
+    }
+}
+
 __device__ __forceinline__ double rcp_t(double x) { return rcp64(x); }
 __device__ __forceinline__ float rcp_t(float x) { return rcp32(x); }
 
@@ -1024,12 +1063,11 @@ __device__ __forceinline__ void edge_head_f32(const SVertRaw<float> *v, const do
     load_vert(v[0], w0, syx0, sxy0);
     load_vert(v[1], w1, syx1, sxy1);
     load_vert(v[2], w2, h.syx2, h.sxy2);
-#pragma unroll
-    for (int d = 0; d < DPT; ++d) {
-        vertex_phasor(st[d], ct[d], w0, h.c0[d].y, h.c0[d].x);
-        vertex_phasor(st[d], ct[d], w1, c1[d].y, c1[d].x);
-        vertex_phasor(st[d], ct[d], w2, h.c2[d].y, h.c2[d].x);
-    }
+    // the head's phasors with the reductions of two directions paired (the
+    // tail keeps single ones: pairing there too made the step 3 % longer)
+    vertex_phasors<DPT>(st, ct, w0, [&](int d, float2 p) { h.c0[d] = p; });
+    vertex_phasors<DPT>(st, ct, w1, [&](int d, float2 p) { c1[d] = p; });
+    vertex_phasors<DPT>(st, ct, w2, [&](int d, float2 p) { h.c2[d] = p; });
 #pragma unroll
     for (int d = 0; d < DPT; ++d) {
         mn[d] = 1e30f;

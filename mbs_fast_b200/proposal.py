@@ -230,39 +230,77 @@ def orientation_sample_batch(cfg, u, v, w, beta_sym: float, gamma_sym: float):
 class TrainedProposal:
     """A proposal with its pilot run: the pilot's points (u, v) and
     per-orientation rows [n_pilot, n_t, 16] (orientation weight 1), which
-    balance_weights lets the final estimate reuse, and the seconds spent in
-    the pilot (tracing and device rows) and in the network fit."""
+    balance_weights lets the final estimate reuse when the pilot ran on the
+    handler's grid (pilot_rows is None when it ran on a row subset), and the
+    seconds spent in the pilot (tracing and device rows) and in the network
+    fit."""
     proposal: Proposal
     fit_r2: float
     pilot_u: np.ndarray
     pilot_v: np.ndarray
-    pilot_rows: np.ndarray
+    pilot_rows: np.ndarray | None
     pilot_s: float
     fit_s: float
+    parts: dict | None = None    # seconds per part of the pilot and the fit
+
+
+def pilot_theta_rows(theta_deg: np.ndarray, rows_mask=None, every: int = 1) -> np.ndarray:
+    """Zenith angles (degrees) of a pilot grid: the rows of rows_mask (all
+    rows when None), every `every`-th of them.  The importance target is an
+    RMS over rows, so a pilot on these rows alone gives the same targets (all
+    the chosen rows) or nearly (a thinned set) at a fraction of the cost."""
+    th = np.asarray(theta_deg, dtype=np.float64)
+    if rows_mask is not None:
+        th = th[np.asarray(rows_mask, dtype=bool)]
+    return np.ascontiguousarray(th[::max(1, int(every))])
 
 
 def train_proposal_with_pilot(handler, cfg, n_pilot: int, rows_mask=None, pilot_seed: int = 777,
                               cells: int = 128, mix: float = 0.8, epochs: int = 400,
                               batch: int = 256, min_r2: float = 0.2, device: int = 0,
-                              precision: int = 1) -> TrainedProposal:
-    """Pilot run (plain Sobol, per-orientation rows on the handler's grid),
-    network training on the log importance, proposal table."""
+                              precision: int = 1, pilot_theta_deg=None,
+                              lr: float = 2e-3) -> TrainedProposal:
+    """Pilot run (plain Sobol, per-orientation rows), network training on the
+    log importance, proposal table.  The pilot's rows are the handler's grid
+    (and rows_mask selects the target rows among them), or, with
+    pilot_theta_deg, only those zenith rows (same azimuth bins): then every
+    pilot row is a target row."""
     import time
     from . import beams as B
     t0 = time.perf_counter()
+    parts = {}
     bs, gs, _ = B.symmetry(cfg)
     u, v, _ = plain_sobol(n_pilot, seed=pilot_seed)
     pb = orientation_sample_batch(cfg, u, v, np.ones(n_pilot), bs, gs)
-    rows = handler.orientation_rows(pb, precision=precision)
+    parts["trace_s"] = time.perf_counter() - t0
+    if pilot_theta_deg is None:
+        rows = handler.orientation_rows(pb, precision=precision)
+        keep = rows
+    else:
+        from .handler import GpuHandlerPO
+        th = np.asarray(pilot_theta_deg, dtype=np.float64)
+        ph = GpuHandlerPO(B.grid(float(th[0]), float(th[-1]), handler.grid.n_az, len(th) - 1,
+                                 theta_deg=th), handler.wave, device=device)
+        try:
+            rows = ph.orientation_rows(pb, precision=precision)
+        finally:
+            ph.close()
+        rows_mask, keep = None, None
     t1 = time.perf_counter()
+    parts["rows_s"] = t1 - t0 - parts["trace_s"]
     logh = variance_targets(rows, rows_mask)
     lp = LearnedProposal(bs, gs, device=device)
+    t2 = time.perf_counter()
+    parts["targets_and_net_s"] = t2 - t1
     try:
-        r2 = lp.fit(u, v, logh, epochs=epochs, batch=batch)
+        r2 = lp.fit(u, v, logh, epochs=epochs, batch=batch, lr=lr)
+        t3 = time.perf_counter()
+        parts["train_s"] = t3 - t2
         prop = lp.proposal(cells=cells, mix=mix, min_r2=min_r2)
+        parts["table_s"] = time.perf_counter() - t3
     finally:
         lp.close()
-    return TrainedProposal(prop, r2, u, v, rows, t1 - t0, time.perf_counter() - t1)
+    return TrainedProposal(prop, r2, u, v, keep, t1 - t0, time.perf_counter() - t1, parts)
 
 
 def train_proposal(handler, cfg, n_pilot: int, rows_mask=None, pilot_seed: int = 777,

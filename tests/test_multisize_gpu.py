@@ -52,8 +52,9 @@ def test_multisize_fp32c_against_fp64(absorbing):
     for s, a, b in zip(SCALES, m32, m64):
         wl2, err = common.weighted_l2(a, b, grid), common.element_errors(a, b, grid)
         print("scale", s, "FP32C vs FP64 weighted L2", wl2, err)
-        assert wl2 < 5e-5
-        assert err["M11_max_rel"] < 5e-3
+        # about ten times the measured 1.2e-6 and 1.4e-4
+        assert wl2 < 1.5e-5
+        assert err["M11_max_rel"] < 1.5e-3
 
 
 def test_multisize_accumulates_and_scale_one_matches_direct(absorbing):
@@ -124,7 +125,7 @@ def test_size_scan_plates_nonuniform_grid():
     for i in range(len(scales)):
         wl2 = common.weighted_l2(m32[i], ms[i], grid)
         print("size", i, "FP32C vs FP64 weighted L2", wl2)
-        assert wl2 < 1e-4, i
+        assert wl2 < 1.5e-5, i      # about ten times the measured 1.6e-6
     # the forward peak grows about as D^4 (shadow area squared; beam
     # interference makes it non-monotonic over three orientations)
     f = np.array([m[0, 0, 0] for m in ms])
