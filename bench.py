@@ -71,7 +71,7 @@ def parse():
                     help="orientations of the same-box comparison with the reference's CUDA build")
     ap.add_argument("--launch-selftest", action="store_true",
                     help="ranks only exchange one gloo all-reduce (tests the --gpus N launcher on the CPU)")
-    ap.add_argument("--proposal-epochs", type=int, default=400,
+    ap.add_argument("--proposal-epochs", type=int, default=200,
                     help="training epochs of the proposal network (workload proposal)")
     ap.add_argument("--proposal-pilot", type=int, default=2048,
                     help="plain Sobol pilot orientations of the proposal (workload proposal)")

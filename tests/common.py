@@ -39,9 +39,19 @@ def sobol_batch(cfg_key: str, n: int, seed: int = 42) -> B.BeamBatch:
 HEX_COLUMN_ABSORBING_10x20 = B.ParticleConfig(particle_type=1, p=(20.0, 10.0), ri_re=1.3116,
                                               ri_im=0.002, absorption=True, wavelength=0.532,
                                               max_reflections=4)
+# The reference's other particle shapes (its main.cpp --particle 2, 4, 12):
+# apertures of 7-12 vertices.
+BULLET_30x10 = B.ParticleConfig(particle_type=2, p=(30.0, 10.0), ri_re=1.3116, ri_im=0.0,
+                                wavelength=0.532, max_reflections=4)
+DROXTAL_20 = B.ParticleConfig(particle_type=4, p=(20.0,), ri_re=1.3116, ri_im=0.0,
+                              wavelength=0.532, max_reflections=4)
+HEXAGG_20x10x3 = B.ParticleConfig(particle_type=12, p=(20.0, 10.0, 3), ri_re=1.3116, ri_im=0.0,
+                                  wavelength=0.532, max_reflections=4)
 CASES = {"hex40x100": HEX_COLUMN_40x100, "hex10x20": HEX_COLUMN_10x20,
          "concave": CONCAVE_ABSORBING, "hexabs10x20": HEX_COLUMN_ABSORBING_10x20,
-         "plate10": PLATE_D10}
+         "plate10": PLATE_D10, "bullet30x10": BULLET_30x10, "droxtal20": DROXTAL_20,
+         "hexagg20x10x3": HEXAGG_20x10x3}
+SHAPE_CASES = ("bullet30x10", "droxtal20", "hexagg20x10x3")
 
 
 def single_beam_orientations(batch: B.BeamBatch) -> B.BeamBatch:

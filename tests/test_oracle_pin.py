@@ -35,7 +35,10 @@ def test_jones_to_mueller_kat():
 
 @pytest.mark.parametrize("case,n,grid", [("hex40x100", 6, (0.0, 180.0, 16, 90)),
                                          ("concave", 8, (0.0, 180.0, 24, 60)),
-                                         ("hex10x20", 4, (0.0, 180.0, 12, 180))])
+                                         ("hex10x20", 4, (0.0, 180.0, 12, 180)),
+                                         ("bullet30x10", 6, (0.0, 180.0, 16, 180)),
+                                         ("droxtal20", 6, (0.0, 180.0, 16, 180)),
+                                         ("hexagg20x10x3", 6, (0.0, 180.0, 16, 180))])
 def test_oracle_matches_reference(case, n, grid):
     cfg = common.CASES[case]
     batch = common.sobol_batch(case, n)
