@@ -874,6 +874,18 @@ __device__ __forceinline__ void vertex_phasor(double st, double ct, const VertRe
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
 }
 
+// FP64 phasor through the kernel's sine table; the FP32C form ignores it.
+__device__ __forceinline__ void vertex_phasor_t(double st, double ct, const VertRegs &w,
+                                                const double2 *tab, double &s, double &c)
+{
+    sincos_turns_tab(fma(st, w.ps, fma(ct, w.pc, w.p0)), tab, s, c);
+}
+__device__ __forceinline__ void vertex_phasor_t(double st, double ct, const VertRegs &w,
+                                                const double2 *, float &s, float &c)
+{
+    vertex_phasor(st, ct, w, s, c);
+}
+
 // The same for two directions of one vertex: the two reductions to the
 // angle in one FFMA2 (each lane rounds as the FFMA above, so the phasors are
 // bitwise those of two single calls).
@@ -925,7 +937,7 @@ __device__ __forceinline__ float rcp_t(float x) { return rcp32(x); }
 template <typename T, int DPT, int NV>
 __device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const double *st, const double *ct,
                                                 const T *X1, const T *X2, const bool *useX,
-                                                T *sr, T *si, T *mn)
+                                                T *sr, T *si, T *mn, const double2 *tab)
 {
     T c[DPT][NV], s[DPT][NV], syx[NV], sxy[NV];
 #pragma unroll
@@ -934,7 +946,7 @@ __device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const doub
         load_vert(v[e], w, syx[e], sxy[e]);
 #pragma unroll
         for (int d = 0; d < DPT; ++d)
-            vertex_phasor(st[d], ct[d], w, s[d][e], c[d][e]);
+            vertex_phasor_t(st[d], ct[d], w, tab, s[d][e], c[d][e]);
     }
 #pragma unroll
     for (int d = 0; d < DPT; ++d) {
@@ -942,16 +954,32 @@ __device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const doub
         sr[d] = T(0);
         si[d] = T(0);
     }
+    // consecutive edges share one reciprocal: 1/a = b/(ab), 1/b = a/(ab)
+    // (FP64 here: coefficients between eps1 and about 1e30 |X1| keep the
+    // product far from overflow and underflow; a pair with a smaller one is
+    // marked and its sums discarded)
 #pragma unroll
-    for (int e = 0; e < NV; ++e) {
-        const int en = (e + 1 < NV) ? e + 1 : 0;
+    for (int e = 0; e < NV; e += 2) {
 #pragma unroll
         for (int d = 0; d < DPT; ++d) {
-            const T coef = fma(useX[d] ? syx[e] : sxy[e], X1[d], X2[d]);
-            const T inv = rcp_t(coef);
-            mn[d] = fmin(mn[d], fabs(coef));
-            sr[d] = fma(c[d][en] - c[d][e], inv, sr[d]);
-            si[d] = fma(s[d][en] - s[d][e], inv, si[d]);
+            const T ca = fma(useX[d] ? syx[e] : sxy[e], X1[d], X2[d]);
+            const int e1 = (e + 1 < NV) ? e + 1 : 0;
+            if (e + 1 < NV) {
+                const T cb = fma(useX[d] ? syx[e1] : sxy[e1], X1[d], X2[d]);
+                const T r = rcp_t(ca * cb);
+                const T ia = cb * r, ib = ca * r;
+                const int e2 = (e + 2 < NV) ? e + 2 : 0;
+                mn[d] = fmin(mn[d], fmin(fabs(ca), fabs(cb)));
+                sr[d] = fma(c[d][e1] - c[d][e], ia, sr[d]);
+                si[d] = fma(s[d][e1] - s[d][e], ia, si[d]);
+                sr[d] = fma(c[d][e2] - c[d][e1], ib, sr[d]);
+                si[d] = fma(s[d][e2] - s[d][e1], ib, si[d]);
+            } else {
+                const T inv = rcp_t(ca);
+                mn[d] = fmin(mn[d], fabs(ca));
+                sr[d] = fma(c[d][0] - c[d][e], inv, sr[d]);
+                si[d] = fma(s[d][0] - s[d][e], inv, si[d]);
+            }
         }
     }
 }
@@ -1145,7 +1173,8 @@ __device__ __forceinline__ void edge_tail_loop_f32(const SVertRaw<float> *v, int
 template <typename T, int DPT>
 __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, const double *st,
                                                const double *ct, const T *X1, const T *X2,
-                                               const bool *useX, T *sr, T *si, T *mn)
+                                               const bool *useX, T *sr, T *si, T *mn,
+                                               const double2 *tab)
 {
     T c0[DPT], s0[DPT], cp_[DPT], sp_[DPT];
     T syx, sxy;
@@ -1153,7 +1182,7 @@ __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, con
     load_vert(v[0], w, syx, sxy);
 #pragma unroll
     for (int d = 0; d < DPT; ++d) {
-        vertex_phasor(st[d], ct[d], w, s0[d], c0[d]);
+        vertex_phasor_t(st[d], ct[d], w, tab, s0[d], c0[d]);
         cp_[d] = c0[d];
         sp_[d] = s0[d];
         mn[d] = T(1e30);
@@ -1169,7 +1198,7 @@ __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, con
         for (int d = 0; d < DPT; ++d) {
             T cn = c0[d], sn = s0[d];
             if (!last)
-                vertex_phasor(st[d], ct[d], w, sn, cn);
+                vertex_phasor_t(st[d], ct[d], w, tab, sn, cn);
             const T coef = fma(useX[d] ? syx_e : sxy_e, X1[d], X2[d]);
             const T inv = rcp_t(coef);
             mn[d] = fmin(mn[d], fabs(coef));
@@ -1184,7 +1213,8 @@ __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, con
 template <typename T, int DPT>
 __device__ __forceinline__ void edge_sums(const SVertRaw<T> *v, int nv, const double *st,
                                           const double *ct, const T *X1, const T *X2,
-                                          const bool *useX, T *sr, T *si, T *mn)
+                                          const bool *useX, T *sr, T *si, T *mn,
+                                          const double2 *tab)
 {
     if constexpr (sizeof(T) == 4) {
         switch (nv) {   // warp-uniform: every lane evaluates the same beam
@@ -1192,15 +1222,15 @@ __device__ __forceinline__ void edge_sums(const SVertRaw<T> *v, int nv, const do
         case 4: edge_sums_fixed_f32<DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn); break;
         case 5: edge_sums_fixed_f32<DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn); break;
         case 6: edge_sums_fixed_f32<DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-        default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn); break;
+        default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn, tab); break;
         }
     } else {
         switch (nv) {
-        case 3: edge_sums_fixed<T, DPT, 3>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-        case 4: edge_sums_fixed<T, DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-        case 5: edge_sums_fixed<T, DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-        case 6: edge_sums_fixed<T, DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-        default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn); break;
+        case 3: edge_sums_fixed<T, DPT, 3>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
+        case 4: edge_sums_fixed<T, DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
+        case 5: edge_sums_fixed<T, DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
+        case 6: edge_sums_fixed<T, DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
+        default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn, tab); break;
         }
     }
 }
@@ -1372,6 +1402,15 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
     __shared__ int s_item;
     __shared__ double s_zdel[TPB / 32];
     __shared__ int s_rwarp[TPB / 32], s_rbase[TPB], s_rok[TPB];   // the spread FP64 pass
+    // FP64: sin and cos of the 128 angles 2 pi k / 128 for the vertex phasors
+    __shared__ double2 s_sincos[kF32 ? 1 : 128];
+    if constexpr (!kF32) {
+        for (int i = threadIdx.x; i < 128; i += TPB) {
+            double sv_, cv_;
+            sincos_turns(i * 0.0078125, sv_, cv_);
+            s_sincos[i] = make_double2(sv_, cv_);
+        }
+    }
 
     // Persistent: take work items until none are left, so CTAs of uneven
     // cost (rare FP64 pairs, ragged beam counts) balance across the SMs.
@@ -1537,7 +1576,7 @@ __global__ void __launch_bounds__(TPB, MINB) po_diffract_kernel(KParams P)
                     default: edge_tail_loop_f32<DPT>(vb, b.nv, st, ct, X1, X2, useX, eh, sr, si, mn); break;
                     }
                 } else {
-                    edge_sums<T, DPT>(sv + b.vs, b.nv, st, ct, X1, X2, useX, sr, si, mn);
+                    edge_sums<T, DPT>(sv + b.vs, b.nv, st, ct, X1, X2, useX, sr, si, mn, s_sincos);
                 }
                 T s_r[DPT], s_i[DPT];
 #pragma unroll
