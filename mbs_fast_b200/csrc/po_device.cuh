@@ -105,29 +105,30 @@ __device__ __forceinline__ void sincos_turns(double u, double &s, double &c)
 // sin and cos of 2*pi*u from a table of the 128 angles 2*pi*k/128 (tab[k] =
 // (sin, cos), filled by sincos_turns): u = k/128 + r exactly (|r| <= 1/256
 // turn, the reduction is exact as in sincos_turns), then the angle-addition
-// formulas with Taylor polynomials of sin x (to x^7) and cos x (to x^6) on
-// |x| = 2 pi |r| <= pi/128, whose truncation errors are below 1e-20 and
-// 4e-18.  About 14 FP64 operations and one shared-memory load against about
-// 22 operations and 8 selects of the quadrant form.
+// formulas with the Taylor polynomials of sin(2 pi r) (to r^7) and cos(2 pi r)
+// (to r^6) in r itself (coefficients (2 pi)^n / n!, rounded to double), whose
+// truncation errors are below 1e-20 and 4e-18.  15 FP64 operations and one
+// shared-memory load against about 22 operations and 8 selects of the
+// quadrant form.
 __device__ __forceinline__ void sincos_turns_tab(double u, const double2 *tab, double &s, double &c)
 {
     const double t = fma(u, 128.0, kMagic52);
     const double n = t - kMagic52;
     const int k = __double2loint(t) & 127;
-    const double x = fma(n, -0.0078125, u) * kTwoPi;
-    const double x2 = x * x;
-    double ps = -1.9841269841269841e-04;         // -1/7!
-    ps = fma(ps, x2, 8.3333333333333333e-03);    // 1/5!
-    ps = fma(ps, x2, -1.6666666666666666e-01);   // -1/3!
-    const double sx = fma(x * x2, ps, x);
-    double pc = -1.3888888888888889e-03;         // -1/6!
-    pc = fma(pc, x2, 4.1666666666666664e-02);    // 1/4!
-    pc = fma(pc, x2, -0.5);                      // -1/2!
-    const double cm1 = x2 * pc;                  // cos x - 1
+    const double r = fma(n, -0.0078125, u);          // exact, |r| <= 1/256 turn
+    const double r2 = r * r;
+    double ps = -76.70585975306139;                  // -(2 pi)^7 / 7!
+    ps = fma(ps, r2, 81.60524927607506);             //  (2 pi)^5 / 5!
+    ps = fma(ps, r2, -41.34170224039976);            // -(2 pi)^3 / 3!
+    ps = fma(ps, r2, 6.283185307179586);             //   2 pi
+    const double sx = r * ps;                        // sin(2 pi r)
+    double pc = -85.45681720669373;                  // -(2 pi)^6 / 6!
+    pc = fma(pc, r2, 64.9393940226683);              //  (2 pi)^4 / 4!
+    pc = fma(pc, r2, -19.739208802178716);           // -(2 pi)^2 / 2!
+    const double cx = fma(r2, pc, 1.0);              // cos(2 pi r)
     const double2 sc = tab[k];
-    // sin(a + x) = S + (S (cos x - 1) + C sin x), cos(a + x) = C + (C (cos x - 1) - S sin x)
-    s = sc.x + fma(sc.x, cm1, sc.y * sx);
-    c = sc.y + fma(sc.y, cm1, -(sc.x * sx));
+    s = fma(sc.x, cx, sc.y * sx);
+    c = fma(sc.y, cx, -(sc.x * sx));
 }
 
 __device__ __forceinline__ void sincos_rad(double x, double &s, double &c)
