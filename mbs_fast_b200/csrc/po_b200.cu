@@ -44,13 +44,14 @@ struct GridDev {
 // Launch shapes of the diffraction kernel: threads per CTA, directions per
 // thread and the minimum resident CTAs per SM the register budget is cut
 // for.  mbs_po_autotune times them on the caller's batch and keeps the
-// fastest per precision; variant 0 is the default.
+// fastest per precision; variant 0, the default (the drop-in does not
+// autotune), is the fastest on the column and aggregate workloads.
 struct Variant {
     int tpb, dpt, minb;
 };
-constexpr Variant kVariantsF32[] = {{64, 3, 6}, {64, 3, 5}, {128, 3, 3},
+constexpr Variant kVariantsF32[] = {{128, 3, 3}, {64, 3, 5}, {64, 3, 6},
                                     {96, 2, 5}, {128, 2, 4}, {64, 3, 4}};
-constexpr Variant kVariantsF64[] = {{64, 2, 6}, {128, 1, 3}, {96, 2, 4}, {128, 1, 4}, {64, 3, 4}};
+constexpr Variant kVariantsF64[] = {{64, 3, 4}, {128, 1, 3}, {96, 2, 4}, {128, 1, 4}, {64, 2, 6}};
 // Shapes of the kernels that also accumulate the no-shadow sums.
 constexpr Variant kNoShadowF32 = {128, 2, 4};
 constexpr Variant kNoShadowF64 = {128, 1, 4};
@@ -681,19 +682,19 @@ cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &
         case 1: return launch_one<double, 128, 1, false, 3>(P, st);
         case 2: return launch_one<double, 96, 2, false, 4>(P, st);
         case 3: return launch_one<double, 128, 1, false, 4>(P, st);
-        case 4: return launch_one<double, 64, 3, false, 4>(P, st);
-        default: return launch_one<double, 64, 2, false, 6>(P, st);
+        case 4: return launch_one<double, 64, 2, false, 6>(P, st);
+        default: return launch_one<double, 64, 3, false, 4>(P, st);
         }
     }
     if (ns)
         return launch_one<float, 128, 2, true, 4>(P, st);
     switch (variant) {
     case 1: return launch_one<float, 64, 3, false, 5>(P, st);
-    case 2: return launch_one<float, 128, 3, false, 3>(P, st);
+    case 2: return launch_one<float, 64, 3, false, 6>(P, st);
     case 3: return launch_one<float, 96, 2, false, 5>(P, st);
     case 4: return launch_one<float, 128, 2, false, 4>(P, st);
     case 5: return launch_one<float, 64, 3, false, 4>(P, st);
-    default: return launch_one<float, 64, 3, false, 6>(P, st);
+    default: return launch_one<float, 128, 3, false, 3>(P, st);
     }
 }
 

@@ -66,6 +66,38 @@ def test_fp32c_against_fp64(hex_case):
     assert err["M11_max_rel"] < FP32C_M11_MAX_REL
 
 
+def _n_variants(h, precision):
+    """Launch shapes the library offers for a precision (set_variant refuses
+    the first index past them)."""
+    n = 0
+    while True:
+        try:
+            h.set_variant(precision, n)
+        except RuntimeError:
+            return n
+        n += 1
+
+
+def test_every_launch_shape_matches_oracle(hex_case):
+    """The autotuner may pick any launch shape (threads per CTA, directions
+    per thread, CTAs per SM; each also sets the orientation chunking): every
+    one of them against the oracle."""
+    cfg, batch, grid, wave, h, M_ref, _ = hex_case
+    try:
+        for prec, gate in ((abi.FP64, FP64_WL2), (abi.FP32C, FP32C_WL2)):
+            nv = _n_variants(h, prec)
+            assert nv >= 5
+            for v in range(nv):
+                h.set_variant(prec, v)
+                M = h.new_mueller()
+                assert h.handle_orientations_to_local_gpu(batch, M, precision=prec)
+                wl2 = common.weighted_l2(M, M_ref, grid)
+                assert wl2 < gate, (prec, v, wl2)
+    finally:
+        h.set_variant(abi.FP64, 0)
+        h.set_variant(abi.FP32C, 0)
+
+
 @pytest.fixture(scope="module")
 def headline_case():
     """The headline configuration's particle and grid at full size: column
