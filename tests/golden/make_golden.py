@@ -3,7 +3,10 @@
 Run here, where the reference sources are mounted and oracle/_ref holds the
 reference compiled from them (make -C oracle):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py [REFERENCE_DIR]
+
+(default: $MBS_REFERENCE_DIR, else the directory `reference` beside this
+repository)
 
 Fixtures (small, committed):
   extinction_reference.json  the reference's extinction known answers
@@ -90,4 +93,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MBS_REFERENCE_DIR", "/root/reference"))
+    default = os.environ.get("MBS_REFERENCE_DIR") or os.path.join(
+        os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else default)
