@@ -112,11 +112,12 @@ def build_inputs(args, rank, world):
         import dataclasses
         cfg = dataclasses.replace(cfg, n_threads=max(1, (os.cpu_count() or 1) // world))
     bs, gs, _ = B.symmetry(cfg)
-    beta, gamma, w = B.sobol_orientations(args.orient, bs, gs, 42)
-    # weak scaling: every rank owns its own contiguous orientation shard of
-    # the same size (TracerPOTotal.cpp:5715-5718 splits ranks the same way)
+    # weak scaling: the job averages args.orient x world Sobol orientations
+    # and every rank owns a contiguous shard of args.orient of them
+    # (TracerPOTotal.cpp:5715-5718 splits ranks the same way); rank 0's
+    # shard is the one-GPU workload
+    beta, gamma, w = B.sobol_orientations(args.orient * world, bs, gs, 42)
     if world > 1:
-        beta, gamma, w = np.tile(beta, world), np.tile(gamma, world), np.tile(w, world)
         n = args.orient
         beta, gamma, w = beta[rank * n:(rank + 1) * n], gamma[rank * n:(rank + 1) * n], w[rank * n:(rank + 1) * n]
     batch = B.trace(cfg, beta, gamma, w)
@@ -842,6 +843,8 @@ def main():
         ref = torch.zeros_like(acc)
         st = abi.Stats()
         h.diffract_staged(staged, ref.data_ptr(), precision=abi.FP64, stream=stream, stats=st)
+        if world > 1:        # the whole job's sums, like the FP32C steps'
+            torch.distributed.all_reduce(ref)
         torch.cuda.synchronize()
         fp64_ms = st.kernel_ms + st.reduce_ms
         fp64_kernel_ms = st.kernel_ms
@@ -870,6 +873,9 @@ def main():
         h.diffract_staged(staged, acc.data_ptr(), precision=abi.FP32C, stream=stream, stats=stats)
         kernel_ms.append(stats.kernel_ms)
         launches += stats.launches + 1      # diffraction + reduce (+ pole rows), + the accumulator clear
+        if world > 1:
+            # the path's one exchange: the sum of the ranks' Mueller accumulators
+            torch.distributed.all_reduce(acc)
     ev1.record()
     torch.cuda.synchronize()
     step_ms = ev0.elapsed_time(ev1) / args.steps
@@ -892,6 +898,11 @@ def main():
         Mh[:] = 0.0
         t1 = time.perf_counter()
         h.handle_orientations_to_local_gpu(pinned, Mh, precision=abi.FP32C)
+        if world > 1:
+            # the ranks' host sums, added over NCCL (up and back down)
+            red = torch.from_numpy(Mh).to(f"cuda:{local}")
+            torch.distributed.all_reduce(red)
+            Mh[...] = red.cpu().numpy()
         e2e_t.append(time.perf_counter() - t1)
     e2e_s = float(np.mean(e2e_t))
     if world > 1:
@@ -903,6 +914,9 @@ def main():
                                           pinned.slope_yx, pinned.slope_xy, pinned.edge_flags,
                                           pinned.beam_geom, pinned.beam_flags)))
     d2h_bytes = G * 16 * 8
+    if world > 1:              # the reduction's round trip
+        h2d_bytes += G * 16 * 8
+        d2h_bytes += G * 16 * 8
 
     # ---- the whole orientation average: host tracing overlapped with the device ----
     from mbs_fast_b200.pipeline import orientation_average
@@ -912,6 +926,11 @@ def main():
     orientation_average(h, cfg, beta_o[:2048], gamma_o[:2048], w_o[:2048], precision=abi.FP32C,
                         batch=1024)
     _, _, tp = orientation_average(h, cfg, beta_o, gamma_o, w_o, precision=abi.FP32C, batch=1024)
+    trace_wall = tp["wall_s"]
+    if world > 1:
+        t = torch.tensor([trace_wall], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        trace_wall = float(t.item())
 
     # ---- error of FP32C against the plain FP64 path on the same orientations ----
     m11_err = metrics.compare(h, M32, M64) if M64 is not None else None
@@ -959,8 +978,8 @@ def main():
         "e2e": {"value": total_orient / e2e_s, "unit": "orientations/s",
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "timed_calls": len(e2e_t)},
-        "e2e_with_tracing": {"value": batch.n_orient / tp["wall_s"], "unit": "orientations/s",
-                             "wall_s": tp["wall_s"], "host_trace_s": tp["trace_s"],
+        "e2e_with_tracing": {"value": total_orient / trace_wall, "unit": "orientations/s",
+                             "wall_s": trace_wall, "host_trace_s": tp["trace_s"],
                              "what": "reference tracer and restated PrepareBeams on all host "
                                      "cores but one (which stages the batches), batches of 1024, "
                                      "overlapped with FP32C diffraction on the device"},
