@@ -424,6 +424,8 @@ def run_proposal(args):
                       "launch_shapes": st_best},
            "fit_r2": r2, "proposal_train_s": t_train, "pilot_s": tp.pilot_s, "fit_s": tp.fit_s,
            "proposal_parts_s": tp.parts,
+           "proposal_learned": bool(prop.learned),
+           "predicted_variance_ratio": tp.variance_ratio,
            "reference_s": t_ref,
            "wall_s_per_orientation_with_tracing": per_orient,
            "errors": err, "to_1pct": proj}

@@ -14,7 +14,8 @@ square, and sampled by a 2-D inverse transform of scrambled Sobol points.
 Every sample carries the importance weight p0 / g / N, so the weighted sum
 (which the diffraction kernels compute with these weights as orientation
 weights) is an unbiased estimate of the same average.  The plain Sobol
-average remains the fallback (used when the fit is poor) and the measure of the
+average remains the fallback (used when the fit is poor, or when the held-out
+pilot orientations predict no clear variance reduction) and the measure of the
 error.
 """
 from __future__ import annotations
@@ -159,6 +160,7 @@ class LearnedProposal:
         perm = rng.permutation(n)
         nh = max(1, int(holdout * n))
         te, tr = perm[:nh], perm[nh:]
+        self.holdout = te
         self.net.train(q[tr], t[tr], epochs=epochs, batch=batch, lr=lr, seed=seed)
         pred = self.net.forward(q[te])
         ss_res = float(np.sum((pred - t[te]) ** 2))
@@ -181,6 +183,31 @@ class LearnedProposal:
 
     def close(self) -> None:
         self.net.close()
+
+
+def predicted_variance_ratio(rows: np.ndarray, g: np.ndarray, rows_mask=None,
+                             eps: float = 1e-12) -> float:
+    """Variance of the importance-sampled estimate against plain sampling,
+    predicted from uniformly drawn pilot orientations (rows [n, n_t, 16],
+    orientation weight 1) and the proposal density g at them: summed over
+    the rows of rows_mask, for the relative M11 error and the -M12/M11 error
+    (the quantities variance_targets weighs),
+        plain:      mean_i x_i^2 - (mean_i x_i)^2
+        importance: mean_i x_i^2 / g_i - (mean_i x_i)^2
+    for x = a_i(t) and b_i(t).  Below 1 the proposal should help."""
+    if rows_mask is not None:
+        rows = rows[:, np.asarray(rows_mask, dtype=bool), :]
+    f11, f12 = rows[:, :, 0], rows[:, :, 1]
+    m11 = f11.mean(axis=0)
+    ok = np.abs(m11) > eps * np.max(np.abs(m11))
+    m11 = np.where(ok, m11, 1.0)
+    R = np.where(ok, f12.mean(axis=0) / m11, 0.0)
+    a = (f11 / m11)[:, ok]
+    b = ((f12 - R * f11) / m11)[:, ok]
+    g = np.asarray(g, dtype=np.float64)[:, None]
+    plain = sum(float(np.sum(np.mean(x * x, axis=0) - np.mean(x, axis=0) ** 2)) for x in (a, b))
+    imp = sum(float(np.sum(np.mean(x * x / g, axis=0) - np.mean(x, axis=0) ** 2)) for x in (a, b))
+    return imp / plain if plain > 0 else 1.0
 
 
 def row_errors(rows: np.ndarray, ref: np.ndarray, rows_mask=None, eps: float = 1e-12) -> dict:
@@ -226,6 +253,11 @@ def orientation_sample_batch(cfg, u, v, w, beta_sym: float, gamma_sym: float):
     return B.trace(cfg, beta, gamma, w)
 
 
+# A learned proposal is kept only when the held-out pilot orientations predict
+# at most this fraction of plain sampling's variance (else plain Sobol).
+MAX_VARIANCE_RATIO = 0.8
+
+
 @dataclass
 class TrainedProposal:
     """A proposal with its pilot run: the pilot's points (u, v) and
@@ -242,6 +274,7 @@ class TrainedProposal:
     pilot_s: float
     fit_s: float
     parts: dict | None = None    # seconds per part of the pilot and the fit
+    variance_ratio: float | None = None   # predicted on the held-out pilot points
 
 
 def pilot_theta_rows(theta_deg: np.ndarray, rows_mask=None, every: int = 1) -> np.ndarray:
@@ -259,7 +292,8 @@ def train_proposal_with_pilot(handler, cfg, n_pilot: int, rows_mask=None, pilot_
                               cells: int = 128, mix: float = 0.8, epochs: int = 400,
                               batch: int = 256, min_r2: float = 0.2, device: int = 0,
                               precision: int = 1, pilot_theta_deg=None,
-                              lr: float = 2e-3) -> TrainedProposal:
+                              lr: float = 2e-3,
+                              max_variance_ratio: float = MAX_VARIANCE_RATIO) -> TrainedProposal:
     """Pilot run (plain Sobol, per-orientation rows), network training on the
     log importance, proposal table.  The pilot's rows are the handler's grid
     (and rows_mask selects the target rows among them), or, with
@@ -297,10 +331,17 @@ def train_proposal_with_pilot(handler, cfg, n_pilot: int, rows_mask=None, pilot_
         t3 = time.perf_counter()
         parts["train_s"] = t3 - t2
         prop = lp.proposal(cells=cells, mix=mix, min_r2=min_r2)
+        # the fit may rank orientations well and still not pay: keep the
+        # learned density only where the held-out pilot points predict a
+        # clear variance reduction
+        te = lp.holdout
+        ratio = predicted_variance_ratio(rows[te], proposal_density(prop, u[te], v[te]), rows_mask)
+        if prop.learned and ratio > max_variance_ratio:
+            prop = uniform_proposal(cells)
         parts["table_s"] = time.perf_counter() - t3
     finally:
         lp.close()
-    return TrainedProposal(prop, r2, u, v, keep, t1 - t0, time.perf_counter() - t1, parts)
+    return TrainedProposal(prop, r2, u, v, keep, t1 - t0, time.perf_counter() - t1, parts, ratio)
 
 
 def train_proposal(handler, cfg, n_pilot: int, rows_mask=None, pilot_seed: int = 777,

@@ -94,6 +94,51 @@ def test_variance_targets_prefer_influential_orientations():
     assert t_reg[7] - np.median(t_reg) > t_all[7] - np.median(t_all)
 
 
+def test_predicted_variance_ratio():
+    """Uniform density: the ratio is 1.  A density that follows where the
+    rows vary predicts a reduction; one that avoids it predicts an increase.
+    The prediction matches the variances of the two estimators measured by
+    repeated sampling."""
+    rng = np.random.default_rng(11)
+    n, nt = 4000, 12
+    x = rng.random(n)
+    # rows: a smooth part plus a spike over x > 0.9 that carries the variance
+    f11 = 1.0 + 0.05 * np.sin(6 * x)[:, None] + np.where(x > 0.9, 8.0, 0.0)[:, None] * rng.random((n, nt))
+    rows = np.zeros((n, nt, 16))
+    rows[:, :, 0] = f11
+    rows[:, :, 1] = -0.3 * f11 + 0.01 * rng.normal(size=(n, nt))
+    assert PR.predicted_variance_ratio(rows, np.ones(n)) == pytest.approx(1.0, rel=1e-12)
+    g_good = np.where(x > 0.9, 5.0, 0.5 / 0.9 * 1.0)        # integrates to 1 over [0, 1]
+    g_bad = np.where(x > 0.9, 0.2, (1 - 0.02) / 0.9)
+    r_good = PR.predicted_variance_ratio(rows, g_good)
+    r_bad = PR.predicted_variance_ratio(rows, g_bad)
+    assert r_good < 0.5 < 1.0 < r_bad
+    # against sampling: the per-row M11 mean estimated with 200 points drawn
+    # from g, weights 1/g, over many repetitions
+    def f(xs):
+        return 1.0 + 0.05 * np.sin(6 * xs) + np.where(xs > 0.9, 4.0, 0.0)
+
+    def draw(m, good):
+        if not good:
+            return rng.random(m), np.ones(m)
+        hi = rng.random(m) < 0.5                              # mass 0.5 on (0.9, 1]
+        xs = np.where(hi, 0.9 + 0.1 * rng.random(m), 0.9 * rng.random(m))
+        return xs, np.where(xs > 0.9, 5.0, 0.5 / 0.9)
+    est = {k: [] for k in (True, False)}
+    for _ in range(3000):
+        for k in est:
+            xs, gs = draw(200, k)
+            est[k].append(np.mean(f(xs) / gs))
+    measured = np.var(est[True]) / np.var(est[False])
+    xs = rng.random(20000)
+    rows1 = np.zeros((20000, 1, 16))
+    rows1[:, 0, 0] = f(xs)
+    rows1[:, 0, 1] = -0.3 * f(xs)
+    predicted = PR.predicted_variance_ratio(rows1[:, :, :], np.where(xs > 0.9, 5.0, 0.5 / 0.9))
+    # the ratio counts M11 and -M12/M11 (zero here: f12 is proportional)
+    assert predicted == pytest.approx(measured, rel=0.15)
+
+
 @pytest.mark.gpu
 def test_learned_proposal_gains_on_backscatter():
     """The learned proposal at test size: the network trained on a
@@ -163,8 +208,9 @@ def test_learned_proposal_on_all_rows_no_worse_than_plain_sobol():
         return PR.averaged_rows(h, PR.orientation_sample_batch(cfg, u, v, w, bs, gs), prec)[0]
 
     ref = rows_of(*PR.plain_sobol(32768, seed=4242), abi.FP64)
-    prop, r2, _ = PR.train_proposal(h, cfg, 2048, rows_mask=inner)
-    print("fit R^2", r2, "learned", prop.learned)
+    tp = PR.train_proposal_with_pilot(h, cfg, 2048, rows_mask=inner)
+    prop, r2 = tp.proposal, tp.fit_r2
+    print("fit R^2", r2, "learned", prop.learned, "predicted variance ratio", tp.variance_ratio)
     for N in (1024, 2048):
         e = {"is": {"M11_rms_rel": [], "P_rms_abs": []}, "pl": {"M11_rms_rel": [], "P_rms_abs": []}}
         for seed in (1, 2, 3, 4):
