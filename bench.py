@@ -354,10 +354,16 @@ def run_proposal(args):
     # launches are not part of a proposal's cost
     PR.train_proposal_with_pilot(h, cfg, 256, rows_mask=target, epochs=2,
                                  batch=args.proposal_batch, pilot_theta_deg=pilot_th)
-    tp = PR.train_proposal_with_pilot(h, cfg, n_pilot, rows_mask=target, epochs=args.proposal_epochs,
-                                      batch=args.proposal_batch, pilot_theta_deg=pilot_th)
+    # the pilot and fit three times (same seeds, the same proposal): the
+    # median time, as the shared host's load shows in single runs
+    runs = [PR.train_proposal_with_pilot(h, cfg, n_pilot, rows_mask=target,
+                                         epochs=args.proposal_epochs, batch=args.proposal_batch,
+                                         pilot_theta_deg=pilot_th) for _ in range(3)]
+    order = sorted(range(3), key=lambda i: runs[i].pilot_s + runs[i].fit_s)
+    tp = runs[order[1]]
     prop, r2 = tp.proposal, tp.fit_r2
     t_train = tp.pilot_s + tp.fit_s
+    train_runs_s = [round(r.pilot_s + r.fit_s, 4) for r in runs]
     Ns = [1024, 2048, 4096, 8192]
     modes = ("plain_fp64", "plain_fp32c", "learned_fp32c", "learned_fp32c_with_pilot")
     if tp.pilot_rows is None:      # the pilot's rows are not the grid's: nothing to reuse
@@ -424,6 +430,7 @@ def run_proposal(args):
                       "launch_shapes": st_best},
            "fit_r2": r2, "proposal_train_s": t_train, "pilot_s": tp.pilot_s, "fit_s": tp.fit_s,
            "proposal_parts_s": tp.parts,
+           "proposal_train_runs_s": train_runs_s,
            "proposal_learned": bool(prop.learned),
            "predicted_variance_ratio": tp.variance_ratio,
            "reference_s": t_ref,

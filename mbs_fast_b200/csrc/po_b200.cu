@@ -1469,19 +1469,24 @@ extern "C" int mbs_po_orientation_rows(mbs_po_ctx *ctx, const mbs_po_beams *beam
     std::memset(rows_out, 0, sizeof(double) * nrow * nO);
     if (nO == 0 || beams->n_beams == 0)
         return MBS_PO_OK;
-    // orientation groups: one Mueller grid per orientation, about 1 GiB of
-    // grids per group
+    // orientation groups: one Mueller grid per orientation, at most 256 MiB
+    // of grids per group, from the context's pool (stream-ordered: a later
+    // call reuses the blocks without mapping new pages or synchronising)
     const int group = (int)std::max<size_t>(
-        1, std::min<size_t>(std::min<size_t>(nO, 16384), ((size_t)1 << 27) / plane));
+        1, std::min<size_t>(std::min<size_t>(nO, 16384), ((size_t)1 << 25) / plane));
     double *grids = nullptr, *drows = nullptr;
-    size_t gcap = 0, rcap = 0;
-    if ((rc = ensure(ctx, grids, gcap, plane * group, "orientation grids")))
-        return rc;
-    if ((rc = ensure(ctx, drows, rcap, nrow * group, "orientation rows"))) {
-        cudaFree(grids);
-        return rc;
-    }
     cudaStream_t st = ctx->stream;
+    {
+        cudaError_t e = cudaMallocFromPoolAsync((void **)&grids, plane * group * sizeof(double),
+                                                ctx->pool, st);
+        if (e == cudaSuccess)
+            e = cudaMallocFromPoolAsync((void **)&drows, nrow * group * sizeof(double), ctx->pool, st);
+        if (e != cudaSuccess) {
+            if (grids)
+                cudaFreeAsync(grids, st);
+            return fail(ctx, MBS_PO_ENOMEM, std::string("orientation grids: ") + cudaGetErrorString(e));
+        }
+    }
     std::vector<int64_t> boff, voff;
     for (int o0 = 0; o0 < nO && rc == 0; o0 += group) {
         const int n = std::min(group, nO - o0);
@@ -1537,8 +1542,8 @@ extern "C" int mbs_po_orientation_rows(mbs_po_ctx *ctx, const mbs_po_beams *beam
             rc = cuda_fail(ctx, e, "orientation rows");
     }
     ctx->host_staged.n_sets = 1;
-    cudaFree(grids);
-    cudaFree(drows);
+    cudaFreeAsync(grids, st);
+    cudaFreeAsync(drows, st);
     return rc;
 }
 
