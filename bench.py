@@ -673,10 +673,10 @@ def reference_gpu_compare(n: int, n_phi: int, n_theta: int, warm: bool = True) -
     (its GpuDiffraction.cu for sm_100, FP64 and FP32) against the drop-in
     binary (the same CLI with this library underneath, FP64 and FP32C), on
     the D=40 um, L=100 um column with n Sobol orientations.  Per binary: the
-    sums of the "GPU timing diffract" lines (MBS_GPU_TIMING=1) of one run,
+    sums of the "GPU timing diffract" lines (MBS_GPU_TIMING=1) of a run,
     kernels and whole calls (packing, copies, kernels, accumulation), and the
-    process wall time; with `warm`, after one untimed run (the first
-    process on a fresh device pays one-off costs)."""
+    process wall time, each the median of three runs; with `warm`, after one
+    untimed run (the first process on a fresh device pays one-off costs)."""
     import re
     import tempfile
     cli = ["--method", "po", "--particle", "1", "100", "40", "--refractive-index", "1.3116", "1e-9",
@@ -693,17 +693,25 @@ def reference_gpu_compare(n: int, n_phi: int, n_theta: int, warm: bool = True) -
         if warm:
             subprocess.run([binary] + cli + ["--output", os.path.join(tempfile.mkdtemp(), "w")],
                            capture_output=True, text=True, env=env, timeout=1800)
-        d = tempfile.mkdtemp()
-        t0 = time.perf_counter()
-        r = subprocess.run([binary] + cli + ["--output", os.path.join(d, "o")], capture_output=True,
-                           text=True, env=env, timeout=1800)
-        wall = time.perf_counter() - t0
-        text = r.stdout + r.stderr
-        lines = [ln for ln in text.splitlines() if "GPU timing diffract" in ln]
-        kern = sum(float(m) for ln in lines for m in re.findall(r"kernels=([0-9.]+)ms", ln))
-        tot = sum(float(m) for ln in lines for m in re.findall(r"total=([0-9.]+)ms", ln))
-        out[name] = {"rc": r.returncode, "calls": len(lines), "kernel_ms": kern, "call_ms": tot,
-                     "process_wall_s": wall}
+        # three timed runs, the median of each figure: single runs on the
+        # shared host show stalls of hundreds of ms in either binary
+        runs = []
+        for _ in range(3):
+            d = tempfile.mkdtemp()
+            t0 = time.perf_counter()
+            r = subprocess.run([binary] + cli + ["--output", os.path.join(d, "o")], capture_output=True,
+                               text=True, env=env, timeout=1800)
+            wall = time.perf_counter() - t0
+            text = r.stdout + r.stderr
+            lines = [ln for ln in text.splitlines() if "GPU timing diffract" in ln]
+            kern = sum(float(m) for ln in lines for m in re.findall(r"kernels=([0-9.]+)ms", ln))
+            tot = sum(float(m) for ln in lines for m in re.findall(r"total=([0-9.]+)ms", ln))
+            runs.append((r.returncode, len(lines), kern, tot, wall))
+        out[name] = {"rc": max(x[0] for x in runs), "calls": runs[0][1],
+                     "kernel_ms": float(np.median([x[2] for x in runs])),
+                     "call_ms": float(np.median([x[3] for x in runs])),
+                     "process_wall_s": float(np.median([x[4] for x in runs])),
+                     "runs": 3}
     for prec, ref, mine in (("fp64", "reference_fp64", "b200_fp64"), ("fp32", "reference_fp32", "b200_fp32c")):
         a, b = out.get(ref, {}), out.get(mine, {})
         if a.get("kernel_ms") and b.get("kernel_ms"):
