@@ -52,9 +52,11 @@ struct Variant {
 constexpr Variant kVariantsF32[] = {{128, 3, 3}, {64, 3, 5}, {64, 3, 6},
                                     {96, 2, 5}, {128, 2, 4}, {64, 3, 4}};
 constexpr Variant kVariantsF64[] = {{64, 3, 4}, {128, 1, 3}, {96, 2, 4}, {128, 1, 4}, {64, 2, 6}};
-// Shapes of the kernels that also accumulate the no-shadow sums.
-constexpr Variant kNoShadowF32 = {128, 2, 4};
-constexpr Variant kNoShadowF64 = {128, 1, 4};
+// Shapes of the kernels that also accumulate the no-shadow sums (the
+// fastest of 128x2x4 / 128x3x3 / 64x2x6 / 128x2x3 for FP32C and 128x1x4 /
+// 128x1x3 / 64x2x4 / 64x1x6 for FP64 on the column).
+constexpr Variant kNoShadowF32 = {128, 3, 3};
+constexpr Variant kNoShadowF64 = {128, 1, 3};
 constexpr int kNumVariantsF32 = sizeof(kVariantsF32) / sizeof(Variant);
 constexpr int kNumVariantsF64 = sizeof(kVariantsF64) / sizeof(Variant);
 
@@ -677,7 +679,7 @@ cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &
 {
     if (precision == MBS_PO_FP64) {
         if (ns)
-            return launch_one<double, 128, 1, true, 4>(P, st);
+            return launch_one<double, 128, 1, true, 3>(P, st);
         switch (variant) {
         case 1: return launch_one<double, 128, 1, false, 3>(P, st);
         case 2: return launch_one<double, 96, 2, false, 4>(P, st);
@@ -687,7 +689,7 @@ cudaError_t launch_diffract(int precision, int variant, bool ns, const KParams &
         }
     }
     if (ns)
-        return launch_one<float, 128, 2, true, 4>(P, st);
+        return launch_one<float, 128, 3, true, 3>(P, st);
     switch (variant) {
     case 1: return launch_one<float, 64, 3, false, 5>(P, st);
     case 2: return launch_one<float, 64, 3, false, 6>(P, st);
