@@ -413,45 +413,64 @@ __global__ void __launch_bounds__(256) k_loss(const float *y, const float *t, in
         *out = red[0] / (float)max(n, 1);
 }
 
-// q_b[i] = q[idx[*cursor + i]], t_b[i] = t[idx[*cursor + i]]: the training
-// step's minibatch, at the position in the shuffled order that the device
-// cursor holds (so one captured epoch replays over every epoch's order).
-__global__ void k_gather(const float *q, const float *t, const int *idx, const int *cursor, int n,
-                         float *qb, float *tb)
+// The training step's minibatch at offset b0 of the epoch the device counter
+// holds (so one captured epoch replays over every epoch's shuffled order):
+// t_b[i] = t[s], X0[i] = the BF16 quaternion of s padded to kInPad columns,
+// s = idx[epoch n + b0 + i]; rows n_b .. bpad-1 of X0 are zeros (k_input's
+// layout, without the FP32 copy of the quaternions).
+__global__ void k_gather_input(const float *q, const float *t, const int *idx, const int *epoch,
+                               int n, int b0, int nb, int bpad, bf16 *x0, float *tb)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
+    if (i >= bpad)
         return;
-    const int s = idx[*cursor + i];
-    for (int c = 0; c < kIn; ++c)
-        qb[i * kIn + c] = q[s * kIn + c];
-    tb[i] = t[s];
+    if (i < nb) {
+        const int s = idx[(size_t)(*epoch) * n + b0 + i];
+#pragma unroll
+        for (int c = 0; c < kInPad; ++c)
+            x0[i * kInPad + c] = __float2bfloat16(c < kIn ? q[s * kIn + c] : 0.f);
+        tb[i] = t[s];
+    } else {
+#pragma unroll
+        for (int c = 0; c < kInPad; ++c)
+            x0[i * kInPad + c] = __float2bfloat16(0.f);
+    }
 }
 
-// Adam with the bias corrections of the step the device counter holds
-// (bc[2 k], bc[2 k + 1] for the call's k-th step).
-__global__ void k_adam_step(float *p, const float *g, float *m, float *v, int n, float lr,
-                            const float *bc, const int *stepc)
+// Adam with the bias corrections of step epoch * steps_per_epoch + k (bc[2 j],
+// bc[2 j + 1] for the call's j-th step), and the BF16 copies of the updated
+// weights (k_refresh's layout; W1's padding columns stay the zeros that
+// k_refresh wrote).
+__global__ void k_adam_refresh(float *p, const float *g, float *m, float *v, int n, float lr,
+                               const float *bc, const int *epoch, int steps_per_epoch, int k,
+                               bf16 *w1p, bf16 *w2, bf16 *w3)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    const int k = *stepc;
-    const float bc1 = bc[2 * k], bc2 = bc[2 * k + 1];
+    const int j = (*epoch) * steps_per_epoch + k;
+    const float bc1 = bc[2 * j], bc2 = bc[2 * j + 1];
     const float gi = g[i];
     const float mi = 0.9f * m[i] + 0.1f * gi;
     const float vi = 0.999f * v[i] + 0.001f * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    p[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
+    const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + 1e-8f);
+    p[i] = pi;
+    if (i < ob1) {
+        const int r = (i - oW1) / kIn, c = (i - oW1) - r * kIn;
+        w1p[r * kInPad + c] = __float2bfloat16(pi);
+    } else if (i >= oW2 && i < ob2) {
+        w2[i - oW2] = __float2bfloat16(pi);
+    } else if (i >= oW3 && i < ob3) {
+        w3[i - oW3] = __float2bfloat16(pi);
+    }
 }
 
-// End of a training step: the cursor moves past the minibatch, the step
-// counter by one.
-__global__ void k_advance(int *cursor, int *stepc, int nb)
+// End of a captured epoch: the epoch counter moves on.
+__global__ void k_next_epoch(int *epoch)
 {
-    *cursor += nb;
-    *stepc += 1;
+    *epoch += 1;
 }
 
 inline int pad_rows(int n) { return (n + kTile - 1) / kTile * kTile; }
@@ -572,11 +591,12 @@ void gemm(cudaStream_t s, int M, int N, int K, Mat A, Mat B, GemmOut o, Watch w)
 
 // Forward pass of n samples already in net->q (device); train keeps the
 // pre-activations for the backward pass.
-int forward_dev(mbs_mlp *net, int n)
+int forward_dev(mbs_mlp *net, int n, bool x0_ready = false)
 {
     const int bp = pad_rows(n);
     cudaStream_t s = net->stream;
-    k_input<<<(bp * kInPad + 255) / 256, 256, 0, s>>>(net->q, n, bp, net->x0);
+    if (!x0_ready)
+        k_input<<<(bp * kInPad + 255) / 256, 256, 0, s>>>(net->q, n, bp, net->x0);
     GemmOut o{};
     o.ldo = kH;
     o.bias = net->params + ob1; o.z = net->z1; o.h = net->h1;
@@ -848,17 +868,19 @@ extern "C" int mbs_mlp_train(mbs_mlp *net, const float *q, const float *t, int n
         gemm_attrs();
         e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            for (const int nb : sizes) {
-                k_gather<<<(nb + 127) / 128, 128, 0, s>>>(dq, dt, didx, dstate, nb, net->q, net->t);
-                if ((rc = forward_dev(net, nb)) || (rc = backward_dev(net, nb)))
+            const int spe = (int)sizes.size();
+            for (int k = 0, b0 = 0; k < spe; b0 += sizes[k], ++k) {
+                const int nb = sizes[k], bp = pad_rows(nb);
+                k_gather_input<<<(bp + 127) / 128, 128, 0, s>>>(dq, dt, didx, dstate, n, b0, nb, bp,
+                                                                net->x0, net->t);
+                if ((rc = forward_dev(net, nb, true)) || (rc = backward_dev(net, nb)))
                     break;
-                k_adam_step<<<(kNParams + 255) / 256, 256, 0, s>>>(net->params, net->grad, net->m,
-                                                                   net->v, kNParams, lr, dbc,
-                                                                   dstate + 1);
-                if ((rc = refresh(net)))
-                    break;
-                k_advance<<<1, 1, 0, s>>>(dstate, dstate + 1, nb);
+                k_adam_refresh<<<(kNParams + 255) / 256, 256, 0, s>>>(
+                    net->params, net->grad, net->m, net->v, kNParams, lr, dbc, dstate, spe, k,
+                    net->w1p, net->w2, net->w3);
             }
+            if (rc == 0)
+                k_next_epoch<<<1, 1, 0, s>>>(dstate);
             const cudaError_t ec = cudaStreamEndCapture(s, &graph);
             if (e == cudaSuccess)
                 e = ec;
