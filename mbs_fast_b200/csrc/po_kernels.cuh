@@ -874,16 +874,11 @@ __device__ __forceinline__ void vertex_phasor(double st, double ct, const VertRe
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
 }
 
-// FP64 phasor through the kernel's sine table; the FP32C form ignores it.
+// FP64 phasor through the kernel's sine table.
 __device__ __forceinline__ void vertex_phasor_t(double st, double ct, const VertRegs &w,
                                                 const double2 *tab, double &s, double &c)
 {
     sincos_turns_tab(fma(st, w.ps, fma(ct, w.pc, w.p0)), tab, s, c);
-}
-__device__ __forceinline__ void vertex_phasor_t(double st, double ct, const VertRegs &w,
-                                                const double2 *, float &s, float &c)
-{
-    vertex_phasor(st, ct, w, s, c);
 }
 
 // The same for two directions of one vertex: the two reductions to the
@@ -984,54 +979,16 @@ __device__ __forceinline__ void edge_sums_fixed(const SVertRaw<T> *v, const doub
     }
 }
 
-// FP32C form of edge_sums_fixed: the phasors of a vertex as (cos, sin)
-// pairs, the edge differences as one packed FP32x2 operation (the same
-// rounding as two subtractions: (-1) c_e + c_{e+1} is exact before its
-// single rounding).
-template <int DPT, int NV>
-__device__ __forceinline__ void edge_sums_fixed_f32(const SVertRaw<float> *v, const double *st,
-                                                    const double *ct, const float *X1, const float *X2,
-                                                    const bool *useX, float *sr, float *si, float *mn)
-{
-    float2 cs[DPT][NV];
-    float syx[NV], sxy[NV];
-#pragma unroll
-    for (int e = 0; e < NV; ++e) {
-        VertRegs w;
-        load_vert(v[e], w, syx[e], sxy[e]);
-#pragma unroll
-        for (int d = 0; d < DPT; ++d)
-            vertex_phasor(st[d], ct[d], w, cs[d][e].y, cs[d][e].x);
-    }
-    const float2 m1 = make_float2(-1.f, -1.f);
-#pragma unroll
-    for (int d = 0; d < DPT; ++d) {
-        mn[d] = 1e30f;
-        sr[d] = 0.f;
-        si[d] = 0.f;
-    }
-#pragma unroll
-    for (int e = 0; e < NV; ++e) {
-        const int en = (e + 1 < NV) ? e + 1 : 0;
-#pragma unroll
-        for (int d = 0; d < DPT; ++d) {
-            const float coef = fmaf(useX[d] ? syx[e] : sxy[e], X1[d], X2[d]);
-            const float inv = rcp32(coef);
-            mn[d] = fminf(mn[d], fabsf(coef));
-            const float2 df = __ffma2_rn(cs[d][e], m1, cs[d][en]);
-            sr[d] = fmaf(df.x, inv, sr[d]);
-            si[d] = fmaf(df.y, inv, si[d]);
-        }
-    }
-}
-
 // FP32C edge sums in two parts.  The head (vertices 0-2, edges 0 and 1:
 // every aperture has at least three vertices) sits in the beam loop's
 // straight-line code with the beam's A, B and zone tests, so their chains
 // interleave; the tail (the remaining vertices and edges, the closing edge
 // back to vertex 0) follows the warp-uniform switch on the vertex count.
-// The sums add the edges in edge_sums_fixed_f32's order; consecutive edges
-// share one reciprocal (rcp_pair).
+// The sums add the edges in order (edge e from vertex e to e + 1, the last
+// back to vertex 0); consecutive edges share one reciprocal (rcp_pair).  The
+// edge differences are one packed FP32x2 operation each (the same rounding
+// as two subtractions: (-1) c_e + c_{e+1} is exact before its single
+// rounding).
 __device__ __forceinline__ void edge_step_f32(float2 a, float2 b, float slope, float X1, float X2,
                                               float &sr, float &si, float &mn)
 {
@@ -1210,28 +1167,21 @@ __device__ __forceinline__ void edge_sums_loop(const SVertRaw<T> *v, int nv, con
     }
 }
 
+// FP64 edge sums of one beam (the FP32C path uses edge_head_f32 and the
+// tails above): fixed vertex counts unrolled, longer apertures in a loop.
 template <typename T, int DPT>
 __device__ __forceinline__ void edge_sums(const SVertRaw<T> *v, int nv, const double *st,
                                           const double *ct, const T *X1, const T *X2,
                                           const bool *useX, T *sr, T *si, T *mn,
                                           const double2 *tab)
 {
-    if constexpr (sizeof(T) == 4) {
-        switch (nv) {   // warp-uniform: every lane evaluates the same beam
-        case 3: edge_sums_fixed_f32<DPT, 3>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-        case 4: edge_sums_fixed_f32<DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-        case 5: edge_sums_fixed_f32<DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-        case 6: edge_sums_fixed_f32<DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn); break;
-        default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn, tab); break;
-        }
-    } else {
-        switch (nv) {
-        case 3: edge_sums_fixed<T, DPT, 3>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
-        case 4: edge_sums_fixed<T, DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
-        case 5: edge_sums_fixed<T, DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
-        case 6: edge_sums_fixed<T, DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
-        default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn, tab); break;
-        }
+    static_assert(sizeof(T) == 8, "FP64 path");
+    switch (nv) {   // warp-uniform: every lane evaluates the same beam
+    case 3: edge_sums_fixed<T, DPT, 3>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
+    case 4: edge_sums_fixed<T, DPT, 4>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
+    case 5: edge_sums_fixed<T, DPT, 5>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
+    case 6: edge_sums_fixed<T, DPT, 6>(v, st, ct, X1, X2, useX, sr, si, mn, tab); break;
+    default: edge_sums_loop<T, DPT>(v, nv, st, ct, X1, X2, useX, sr, si, mn, tab); break;
     }
 }
 
