@@ -94,6 +94,17 @@ def test_variance_targets_prefer_influential_orientations():
     assert t_reg[7] - np.median(t_reg) > t_all[7] - np.median(t_all)
 
 
+def test_pilot_theta_rows():
+    th = np.linspace(0.0, 180.0, 1801)
+    back = (th >= 170) & (th < 179.5)
+    rows = PR.pilot_theta_rows(th, back)
+    np.testing.assert_array_equal(rows, th[back])
+    thin = PR.pilot_theta_rows(th, (th > 0.5) & (th < 179.5), every=9)
+    assert len(thin) == len(range(0, int(((th > 0.5) & (th < 179.5)).sum()), 9))
+    assert thin[0] == th[(th > 0.5)][0] and np.all(np.diff(thin) > 0)
+    np.testing.assert_array_equal(PR.pilot_theta_rows(th), th)
+
+
 def test_predicted_variance_ratio():
     """Uniform density: the ratio is 1.  A density that follows where the
     rows vary predicts a reduction; one that avoids it predicts an increase.
