@@ -352,9 +352,10 @@ int    mbs_po_beam_stats(const mbs_po_beams *beams, char *buf, int len);
  *     Mns_accum_dev) exceeds the array are rejected with MBS_PO_ERANGE; when
  *     the array holds fewer orientation chunks than the default plan uses,
  *     the call runs fewer, larger chunks.
- *   - Throughput: the default plan uses up to 64 orientation chunks (about
- *     32 work items per resident CTA); when fewer chunk planes fit in the
- *     array the call runs fewer, larger chunks and fewer work items.  On the
+ *   - Throughput: this call uses up to 64 orientation chunks (about 32 work
+ *     items per resident CTA; the allocating calls use up to 256, about
+ *     128); when fewer chunk planes fit in the array the call runs fewer,
+ *     larger chunks and fewer work items.  On the
  *     48 x 1801 grid (11 MB per plane) one chunk fits with no-shadow sums
  *     (240 work items for about 444 resident CTAs: under half the device
  *     busy) and three without.  Grids get the full 64 chunks only up to

@@ -624,10 +624,18 @@ struct LaunchPlan {
     int tiles_per_row, n_chunks, orient_per_chunk, chunks_per_set;
 };
 
+// At most this many orientation chunks (partial Mueller planes) per set.
+// The persistent kernel's last wave of work items leaves SMs idle; about 128
+// items per resident CTA keep that tail near 0.5 % of the step (64 chunks:
+// 1 % longer FP32C and FP64 steps on the column; 32: 3 %), at 256 planes of
+// 11 MB on the headline grid.
+constexpr int kMaxChunks = 256;
+
 // Orientation chunks per output set: enough work items (chunk x azimuth x
-// zenith tile) for about 32 per resident CTA of the persistent kernel, so
-// the last items leave little tail; at most 64 chunks per set (each chunk
-// owns a partial plane).  n_orient is per set; n_chunks counts all sets.
+// zenith tile) for about kMaxChunks / 2 per resident CTA of the persistent
+// kernel, at most kMaxChunks chunks per set (each chunk owns a partial
+// plane).  n_orient is per set; n_chunks counts all sets.
+
 LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ctas_per_sm,
                        int n_sets = 1)
 {
@@ -642,10 +650,10 @@ LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ct
             sms = v;
     }
     n_sets = std::max(1, n_sets);
-    const long long target = (long long)sms * ctas_per_sm * 32;
+    const long long target = (long long)sms * ctas_per_sm * (kMaxChunks / 2);
     long long chunks = (target + ctas_per_chunk * n_sets - 1) / (ctas_per_chunk * n_sets);
     chunks = std::max<long long>(1, std::min<long long>(chunks, std::max(1, n_orient)));
-    chunks = std::min<long long>(chunks, 64);
+    chunks = std::min<long long>(chunks, kMaxChunks);
     L.orient_per_chunk = (int)((n_orient + chunks - 1) / chunks);
     L.chunks_per_set = (int)((n_orient + L.orient_per_chunk - 1) / std::max(1, L.orient_per_chunk));
     if (L.chunks_per_set < 1) L.chunks_per_set = 1;
@@ -1656,8 +1664,8 @@ extern "C" int mbs_po_select_batch(mbs_po_ctx *ctx, const mbs_po_beams *beams, i
     if (!(mem_fraction > 0.1 && mem_fraction <= 0.98))
         mem_fraction = 0.88;   // MBS_GPU_MEM_FRACTION default (GpuDiffraction.cu:391-401)
     const int64_t G = ctx->has_grid ? (int64_t)ctx->grid.n_az * (ctx->grid.n_zen + 1) : 0;
-    // fixed: partials (up to 64 chunks x 2 planes) + accumulators + 128 MiB slack
-    const double fixed = (double)G * 16 * 8 * (64 * 2 + 2) + (128.0 * (1 << 20));
+    // fixed: partials (up to kMaxChunks chunks x 2 planes) + accumulators + 128 MiB slack
+    const double fixed = (double)G * 16 * 8 * (kMaxChunks * 2 + 2) + (128.0 * (1 << 20));
     double budget = freeB * mem_fraction - fixed;
     int count = 0;
     const int end = std::min(beams->n_orient, start + std::max(0, max_count));
