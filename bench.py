@@ -760,7 +760,7 @@ def run_mlp(args):
 # full-size FP32C diffraction launch of the headline workload (16,384
 # orientations), from the capture summarised in
 # profiles/po_diffract_kernel_f32_traffic_hexcol40x100_16384orient.md
-FP32C_LAUNCH_DRAM_BYTES = 2_201_444_096 + 740_194_816
+FP32C_LAUNCH_DRAM_BYTES = 1_571_426_560 + 2_719_601_664
 
 
 def nominal_peaks(clock_mhz: float | None) -> dict:
