@@ -154,3 +154,33 @@ def test_dropin_packed_beam_cache():
     assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
     assert r.stdout.strip().endswith("OK")
     assert r.stderr.count("cache=fill") == 2 and r.stderr.count("cache=hit") == 3, r.stderr[-3000:]
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (os.path.exists(DROPIN) and os.path.exists(REFCLI)),
+                    reason="drop-in or reference CLI not built")
+def test_dropin_noshadow_output_matches_reference_cli(tmp_path):
+    """--no-shadow-output (HandlerPO::ComputeNoShadow, the kernels that also
+    accumulate the sums over internal beams): the full and the no-shadow .dat
+    rows and integrals of the drop-in against the reference CLI, FP64 and
+    FP32C."""
+    def run(binary, backend, out, env=None):
+        rows, integ, log = _run(binary, backend, out, env, ["--no-shadow-output"])
+        name = os.path.basename(out)
+        ns = np.loadtxt(os.path.join(out, name + "_noshadow.dat"), skiprows=1)
+        with open(os.path.join(out, name + "_noshadow_integrals.tsv")) as f:
+            lines = [ln.rstrip("\n").split("\t") for ln in f if ln.strip()]
+        return rows, integ, ns, dict(zip(lines[0], lines[1])), log
+
+    ref, ref_i, ref_ns, ref_nsi, _ = run(REFCLI, "cpu", str(tmp_path / "ref"))
+    for prec, gate in (("fp64", 1e-7), ("fp32c", 1e-4)):
+        gpu, gpu_i, ns, nsi, log = run(DROPIN, "gpu", str(tmp_path / prec),
+                                       {"MBS_GPU_TIMING": "1", "MBS_B200_PRECISION": prec})
+        assert "path=b200-" + prec in log
+        assert gpu.shape == ref.shape and ns.shape == ref_ns.shape
+        np.testing.assert_array_equal(ns[:, :2], ref_ns[:, :2])
+        assert _wl2(gpu, ref) < gate, prec
+        assert _wl2(ns, ref_ns) < gate, prec
+        if prec == "fp64":
+            for k in ("Csca",):
+                assert abs(float(nsi[k]) / float(ref_nsi[k]) - 1) < 1e-7, k
