@@ -188,7 +188,12 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // after each use on whatever stream that was), and the new one taken in
 // stream order, at least twice the old size: a cudaFree here waits for all
 // work on the device, in the reference's CLI the tracer threads' kernels too.
-int grow_partial(mbs_po_ctx *ctx, size_t n, cudaStream_t st)
+// The chunk partials grow to at least `min_doubles` at once: a first
+// allocation sized for 64 chunk planes serves every call up to that many
+// chunks (the drop-in's growing first batches among them) with one
+// allocation instead of one per doubling (large device allocations on a
+// busy host have taken up to 0.4 s each).
+int grow_partial(mbs_po_ctx *ctx, size_t n, cudaStream_t st, size_t min_doubles = 0)
 {
     if (n <= ctx->partial_cap && ctx->partial)
         return MBS_PO_OK;
@@ -201,7 +206,7 @@ int grow_partial(mbs_po_ctx *ctx, size_t n, cudaStream_t st)
             return fail(ctx, MBS_PO_ECUDA, std::string("releasing the partials: ") + cudaGetErrorString(e));
     }
     ctx->partial = nullptr;
-    const size_t want = std::max<size_t>(n, 2 * ctx->partial_cap);
+    const size_t want = std::max<size_t>(std::max<size_t>(n, 2 * ctx->partial_cap), min_doubles);
     ctx->partial_cap = 0;
     e = cudaMallocFromPoolAsync((void **)&ctx->partial, want * sizeof(double), ctx->pool, st);
     if (e != cudaSuccess) {
@@ -652,7 +657,10 @@ LaunchPlan plan_launch(int n_az, int n_t, int n_orient, int dirs_per_cta, int ct
     n_sets = std::max(1, n_sets);
     const long long target = (long long)sms * ctas_per_sm * (kMaxChunks / 2);
     long long chunks = (target + ctas_per_chunk * n_sets - 1) / (ctas_per_chunk * n_sets);
-    chunks = std::max<long long>(1, std::min<long long>(chunks, std::max(1, n_orient)));
+    // at least 8 orientations per chunk: small calls (the drop-in's first,
+    // growing batches) keep few partial planes, so the context's partial
+    // buffer does not grow through many large allocations
+    chunks = std::max<long long>(1, std::min<long long>(chunks, std::max(1, n_orient / 8)));
     chunks = std::min<long long>(chunks, kMaxChunks);
     L.orient_per_chunk = (int)((n_orient + chunks - 1) / chunks);
     L.chunks_per_set = (int)((n_orient + L.orient_per_chunk - 1) / std::max(1, L.orient_per_chunk));
@@ -746,7 +754,7 @@ int run_diffract(mbs_po_ctx *ctx, const mbs_po_staged *s, int precision, double 
     const LaunchPlan L = plan_launch(nAz, nT, per_set, V.tpb * V.dpt, V.minb, n_sets);
     const size_t plane = (size_t)16 * G;
     int rc;
-    if ((rc = grow_partial(ctx, plane * L.n_chunks * (ns ? 2 : 1), st)))
+    if ((rc = grow_partial(ctx, plane * L.n_chunks * (ns ? 2 : 1), st, plane * 64 * (ns ? 2 : 1))))
         return rc;
     KParams P;
     P.beams = s->beams;
