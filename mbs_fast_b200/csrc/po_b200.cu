@@ -224,8 +224,10 @@ int grow_partial(mbs_po_ctx *ctx, size_t n, cudaStream_t st, size_t min_doubles 
 // taken in stream order on `st`: unlike cudaFree, that waits for no other
 // work on the device -- in the reference's CLI, tracer threads run their own
 // kernels while a diffraction call stages its batch.  They grow to at least
-// twice the request and four times the old size, so batches that grow call
-// by call (SelectGpuOrientationBatchSize doubles them) reallocate rarely.
+// twice the request, four times the old size and 32 MiB, so batches that
+// grow call by call (SelectGpuOrientationBatchSize doubles them) reallocate
+// rarely: an allocation that has to grow the pool can wait for the device
+// (up to 0.2 s in the reference CLI while its tracer threads run kernels).
 int grow_arena(mbs_po_ctx *ctx, Arena &a, size_t bytes, const char *what, cudaStream_t st)
 {
     if (bytes <= a.cap && a.base)
@@ -236,7 +238,7 @@ int grow_arena(mbs_po_ctx *ctx, Arena &a, size_t bytes, const char *what, cudaSt
             return fail(ctx, MBS_PO_ECUDA, std::string("cudaFreeAsync ") + what + ": " + cudaGetErrorString(e));
     }
     a.base = nullptr;
-    const size_t want = std::max<size_t>({(size_t)2 * bytes, (size_t)4 * a.cap, (size_t)1 << 20});
+    const size_t want = std::max<size_t>({(size_t)2 * bytes, (size_t)4 * a.cap, (size_t)32 << 20});
     const size_t cap = (want + ((size_t)1 << 21) - 1) & ~(((size_t)1 << 21) - 1);
     a.cap = 0;
     cudaError_t e = cudaMallocFromPoolAsync(&a.base, cap, ctx->pool, st);
