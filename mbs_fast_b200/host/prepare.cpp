@@ -3,7 +3,8 @@
 // HandlerPO::ComputeBeamInfo (:824-878), HandlerPO::ComputeOpticalLengths
 // (:1075-1083), Handler::PrecomputeEdgeData (Handler.cpp:641-693),
 // Handler::ApplyAbsorption (:220-260) and Tracks::RecoverTrack
-// (Tracks.cpp:152-181), so that every field of the result is the same double.
+// (Tracks.cpp:152-181), so that every field of the result is the same double
+// (in batch-only mode, every field the flat batch and the extinction read).
 #include "prepare.h"
 
 #include "HandlerPO_fast.h"
@@ -64,7 +65,7 @@ BeamInfo PrepareHandler::BeamInfoWithTrack(Beam &beam, const std::vector<int> &t
     info.center = beam.Center();
     info.projectedCenter = ChangeCoordinateSystem(info.horAxis, info.verAxis,
                                                   info.normald, info.center);
-    if (internal)
+    if (internal && !m_batchOnly)
     {
         for (int i = 0; i < 3; ++i)
             info.opticalLengths[i] = m_scattering->ComputeInternalOpticalPath(beam, beam.arr[i], track);
@@ -178,7 +179,19 @@ void PrepareHandler::Prepare(std::vector<Beam> &beams, double sinZenith, Prepare
         if (info.isBad)
             continue;
 
-        Beam originalBeam = beam;
+        // the unabsorbed beam: all of it, or (batch-only) the fields the
+        // batch reads, its Jones matrix, optical path and act count
+        Beam originalBeam;
+        if (m_batchOnly)
+        {
+            originalBeam.J = beam.J;
+            originalBeam.opticalPath = beam.opticalPath;
+            originalBeam.nActs = beam.nActs;
+        }
+        else
+        {
+            originalBeam = beam;
+        }
         std::vector<double> absorptionPaths;
         if (internal)
         {
@@ -206,8 +219,11 @@ void PrepareHandler::Prepare(std::vector<Beam> &beams, double sinZenith, Prepare
         if (beam.lastFacetId != __INT_MAX__)
         {
             ++candidates;
-            matrix mm = Mueller(beam.J);
-            energy += BeamCrossSection(beam) * mm[0][0] * sinZenith;
+            if (!m_batchOnly)
+            {
+                matrix mm = Mueller(beam.J);
+                energy += BeamCrossSection(beam) * mm[0][0] * sinZenith;
+            }
             const double jn = beam.J.Norm();
             const double ar = info.area;
             const double imp = jn * ar;
@@ -231,7 +247,7 @@ void PrepareHandler::Prepare(std::vector<Beam> &beams, double sinZenith, Prepare
         PreparedBeam &pb = out.beams.back();
         pb.info = info;
         pb.absorptionPaths = absorptionPaths;
-        if (beam.lastFacetId != __INT_MAX__)
+        if (beam.lastFacetId != __INT_MAX__ && !m_batchOnly)
         {
             pb.outputCrossSection = BeamCrossSection(originalBeam);
             matrix unabsorbed = Mueller(originalBeam.J);
@@ -264,7 +280,16 @@ void PrepareHandler::Prepare(std::vector<Beam> &beams, double sinZenith, Prepare
         pb.jp01r = real(j01); pb.jp01i = imag(j01);
         pb.jp10r = real(j10); pb.jp10i = imag(j10);
         pb.jp11r = real(j11); pb.jp11i = imag(j11);
-        pb.origBeam = originalBeam;
+        if (m_batchOnly)
+        {
+            pb.origBeam.J = originalBeam.J;
+            pb.origBeam.opticalPath = originalBeam.opticalPath;
+            pb.origBeam.nActs = originalBeam.nActs;
+        }
+        else
+        {
+            pb.origBeam = originalBeam;
+        }
     }
 
     out.extinctionOt = ComputeForwardExtinctionOt(out);

@@ -36,10 +36,20 @@ public:
     // the id does not decode for the particle.
     static void DecodeTrack(const Beam &beam, int nFacets, std::vector<int> &track);
 
+    // Batch-only preparation (the host producer's): only what the flat batch
+    // (beam_pack.cpp) and ComputeForwardExtinctionOt read is computed, bit
+    // for bit as above.  Left out: BeamInfo::opticalLengths and the length
+    // indices (three internal optical paths per internal beam), the output
+    // cross section and M00 of the unabsorbed beam, the original beam's
+    // polygon (origBeam keeps J, opticalPath and nActs) and the handler's
+    // output-energy statistic.
+    void SetBatchOnly(bool on) { m_batchOnly = on; }
+
 private:
     double EdgeTolerance();
     BeamInfo BeamInfoWithTrack(Beam &beam, const std::vector<int> &track, bool internal);
     void EdgeData(const BeamInfo &info, const Beam &beam, BeamEdgeData &ed);
 
     double m_edgeTolerance = -1.0;
+    bool m_batchOnly = false;
 };

@@ -232,6 +232,8 @@ extern "C" int mbs_host_trace(const mbs_host_config *cfg, int n_orient,
                                         setup.handler->nTheta, master->m_wave);
             const bool referencePrepare = cfg->reference_prepare != 0;
             localHandler.ConfigureForThreadLocalPrepare(*setup.handler, localScatter);
+            // the producer packs the prepared beams: only what the batch reads
+            localHandler.SetBatchOnly(true);
             std::vector<Beam> localBeams;
             PreparedOrientation po;
             double tScatter = 0.0, tPrepare = 0.0, tPack = 0.0;
